@@ -1,0 +1,360 @@
+"""Benchmark: signed triangle counting on B200, one JSON line on rank 0.
+
+A step is one pass of the whole counting path over one synthetic signed graph
+resident in HBM: dedup, (degree, id) orientation, forward CSR with int8 signs
+and the intersection engine, ending in the four per-type counts.  The default
+workload is the power-law one: RMAT scale 24, edge factor 16,
+(a, b, c, d) = (.57, .19, .19, .05), p(+) = .5, generated on the device
+(268,435,456 samples, about 250M undirected edges after dedup).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload 3]
+    python bench.py --impl reference ...      # the reference's CPU code
+
+Metric: undirected edges (after dedup) counted per second, whole job.  With
+N > 1 every rank counts its own instance of the workload (seed + rank): weak
+scaling, no data-path collective.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "edges/s (undirected edges after dedup, whole counting path)"
+UNIT = "edges/s"
+CPU_SAMPLE_SCALE = 20  # RMAT scale of the bounded CPU sample
+
+WORKLOADS = {
+    1: "ER G(n=10,000, m=100,000), p(+)=0.7",
+    2: "Delaunay of 1,000,000 uniform points, 20% of edges deleted, p(+)=0.6",
+    3: "RMAT scale 24, edge factor 16, (.57,.19,.19,.05), symmetrised + deduped, p(+)=0.5",
+    5: "skew: 64Mi vertices, 128Mi samples, backbone + 32 hubs deg in [1e5,1e7], p(+)=0.8",
+}
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-i", str(self.gpu), "-lms", "200"], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def load_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d["hbm_gbs"], "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def load_traffic(workload: int):
+    """Per-launch DRAM bytes of the counting kernel from the committed ncu summary."""
+    p = ROOT / "profiles" / "ncu_traffic.json"
+    if not p.exists():
+        return None
+    d = json.loads(p.read_text())
+    return d.get(str(workload))
+
+
+def golden_counts(workload: int):
+    p = ROOT / "tests" / "golden" / "golden.json"
+    if not p.exists():
+        return None
+    w = json.loads(p.read_text()).get("workloads", {}).get(f"{workload}/0")
+    return tuple(w["t"]) if w else None
+
+
+def make_device_workload(ctx, workload: int, seed_offset: int, torch):
+    """Synthetic graph resident in HBM as (src, dst, sign) tensors."""
+    from signed_triangle_counting_b200 import synth
+    if workload == 3:
+        scale = 24
+        n = 1 << scale
+        samples = 16 << scale
+        seed = synth.workload_seed(3) + seed_offset
+        dev = torch.device("cuda", ctx.device)
+        src = torch.empty(samples, dtype=torch.int32, device=dev)
+        dst = torch.empty(samples, dtype=torch.int32, device=dev)
+        sign = torch.empty(samples, dtype=torch.int8, device=dev)
+        ctx.synth_rmat_device(seed, scale, n, samples, 0.57, 0.19, 0.19, 0.5, src, dst, sign)
+        return src, dst, sign
+    el = synth.workload(workload)
+    if seed_offset:
+        raise SystemExit("only the RMAT workload has per-rank instances")
+    dev = torch.device("cuda", ctx.device)
+    return (torch.from_numpy(el.src.view("int32")).to(dev), torch.from_numpy(el.dst.view("int32")).to(dev),
+            torch.from_numpy(el.sign).to(dev))
+
+
+def cpu_reference_sample(threads: int | None = None) -> dict:
+    """The reference's own CPU path (oracle/_ref harness around tc_serial.cpp:
+    build_forward_csr + sort_adj_lists + count_triangles, OpenMP on all host
+    threads) on RMAT scale CPU_SAMPLE_SCALE with the workload's parameters."""
+    import oracle
+    from signed_triangle_counting_b200 import synth
+    if not oracle.ref_available():
+        return None
+    el = synth.rmat(synth.workload_seed(3), CPU_SAMPLE_SCALE, 1 << CPU_SAMPLE_SCALE,
+                    16 << CPU_SAMPLE_SCALE, p_pos=0.5)
+    t, sec, fwd = oracle.ref_count_arrays(el.src, el.dst, el.sign, with_edges=True)
+    total = sum(sec)
+    return dict(edges=fwd, seconds=total, value=fwd / total, counts=t, stage_seconds=sec,
+                sample=f"RMAT scale {CPU_SAMPLE_SCALE} (2^{CPU_SAMPLE_SCALE} vertices, "
+                       f"{16 << CPU_SAMPLE_SCALE} samples, {fwd} unique edges), same (a,b,c) and "
+                       f"p(+); timed: build_forward_csr + sort_adj_lists + count_triangles")
+
+
+def run_reference(args) -> None:
+    world, rank, _ = _dist()
+    if rank != 0:
+        return
+    import oracle
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref (the reference compiled from its sources) is missing"}))
+        return
+    cores = os.cpu_count()
+    vals = []
+    r = None
+    for i in range(args.warmup + args.steps):
+        r = cpu_reference_sample()
+        if i >= args.warmup:
+            vals.append(r["value"])
+    value = statistics.median(vals)
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["seconds"] * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32/i8",
+        "data": "synthetic",
+        "config": {"workload": WORKLOADS[3], "parallelism": "host OpenMP",
+                   "cpu_sample": r["sample"]},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": r["sample"]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "counts": list(r["counts"]),
+    }
+    print(json.dumps(out))
+
+
+def run_gpu(args) -> None:
+    import torch
+    import signed_triangle_counting_b200 as stc
+
+    world, rank, local = _dist()
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(local)
+    ctx = stc.Context(local)
+    stream = torch.cuda.current_stream(local)
+    src, dst, sign = make_device_workload(ctx, args.workload, rank, torch)
+    torch.cuda.synchronize()
+    m_input = src.numel()
+
+    def step():
+        c = ctx.count(src, dst, sign, strategy=args.strategy, dispatch=args.dispatch,
+                      stream=stream.cuda_stream)
+        return c, ctx.last_stats()
+
+    counts, st = None, None
+    for _ in range(args.warmup):
+        counts, st = step()
+    # Exact-count check of rank 0's instance against the reference's counts.
+    want = golden_counts(args.workload) if rank == 0 else None
+    exact = (counts.as_tuple() == want) if want is not None else None
+
+    # ---- timed region: inputs resident in HBM (2.4 GB > 126 MB L2)
+    sampler = ClockSampler(local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    count_ms, launches, alg_bytes = [], 0, 0
+    for _ in range(args.steps):
+        counts, st = step()
+        count_ms.append(st.ms_count)
+        launches += st.kernel_launches
+        alg_bytes = st.alg_bytes
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    edges = st.m_unique
+    value = world * edges * args.steps / (ms / 1e3)
+
+    # ---- end to end through the C ABI from pinned host memory
+    h_src = torch.empty(m_input, dtype=torch.int32, pin_memory=True)
+    h_dst = torch.empty(m_input, dtype=torch.int32, pin_memory=True)
+    h_sign = torch.empty(m_input, dtype=torch.int8, pin_memory=True)
+    h_src.copy_(src)
+    h_dst.copy_(dst)
+    h_sign.copy_(sign)
+    torch.cuda.synchronize()
+    import ctypes as C
+    from signed_triangle_counting_b200 import _capi
+    out = _capi.stc_counts()
+    o = stc.Context._opts(args.strategy, args.dispatch, False, True, stream.cuda_stream)
+
+    def e2e_step():
+        s_ = _capi.lib().stc_count(ctx._h, C.c_void_p(h_src.data_ptr()), C.c_void_p(h_dst.data_ptr()),
+                                   C.c_void_p(h_sign.data_ptr()), m_input, C.byref(o), C.byref(out))
+        assert s_ == 0, stc.StcError(s_)
+
+    e2e_step()
+    e2e_steps = max(1, min(args.steps, 5))
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    f1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = f0.elapsed_time(f1)
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * edges * e2e_steps / (e2e_ms / 1e3)
+
+    if rank == 0:
+        peaks = load_peaks()
+        cms = statistics.mean(count_ms)
+        achieved = alg_bytes / (cms / 1e3) / 1e9
+        traffic = load_traffic(args.workload)
+        cpu = None
+        if world == 1 and not args.skip_cpu:
+            r = cpu_reference_sample()
+            if r:
+                cpu = {"value": r["value"], "unit": UNIT, "cores": os.cpu_count(),
+                       "kind": "reference", "sample": r["sample"]}
+        res = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32/i8 (ids/signs), u64 counters",
+            "data": "synthetic (seeded, generated on the device)",
+            "config": {"workload": WORKLOADS[args.workload], "m_input": m_input,
+                       "m_unique": edges, "n": st.n, "strategy": args.strategy,
+                       "dispatch": args.dispatch, "l2": "inputs 2.4 GB > 126 MB L2, no flush",
+                       "parallelism": f"{world} rank(s), one graph instance each"},
+            "exact": exact, "counts": list(counts.as_tuple()),
+            "stage_ms": {"dedup": st.ms_dedup, "orient": st.ms_orient, "csr": st.ms_csr,
+                         "count": st.ms_count, "device_total": st.ms_total},
+            "roofline": {"bound": "hbm", "kernel": "intersection engine (count)",
+                         "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
+                         "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
+                         "count_ms": cms},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": m_input * 9,
+                    "d2h_bytes_per_step": 32, "steps": e2e_steps},
+            "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        print(json.dumps(res))
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["mine", "reference"], default="mine")
+    ap.add_argument("--workload", type=int, default=3, choices=[1, 2, 3, 5])
+    ap.add_argument("--strategy", default="auto", choices=["auto", "merge", "hash", "search"])
+    ap.add_argument("--dispatch", default="fixed", choices=["fixed", "learned"])
+    ap.add_argument("--skip-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

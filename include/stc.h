@@ -1,0 +1,203 @@
+/* stc — signed triangle counting on NVIDIA B200 (sm_100a), C ABI.
+ *
+ * Drop-in boundary for the counting path of NikhilBisht2/Signed_Triangle_Counting
+ * ("Signed_TC/Multicore Implementations/", abbreviated MC/ below, and the
+ * Gunrock plug-ins under "Signed_TC/GPU Implementations/", abbreviated GM/).
+ *
+ * Rules of the ABI: plain C types only, no exceptions cross it, every call
+ * returns an stc_status, and buffers passed in are owned by the caller.
+ * Buffers the library returns (edge lists, forward CSRs) are released with
+ * the matching stc_free_* call.  Device memory is owned by an stc_ctx; use
+ * one context per host thread (a context is not thread-safe).
+ *
+ * Semantics follow the reference CPU code:
+ *  - an edge line/element (u, v, s) with u == v is dropped (MC/graph_io.h:191);
+ *  - s < 0 means a negative edge, anything else positive (MC/graph_io.h:84-97);
+ *  - (u, v) and (v, u) are the same undirected edge; duplicates keep their
+ *    first occurrence (MC/graph_io.h:221-259);
+ *  - vertices are ordered by (degree, id) and every edge is oriented from the
+ *    lower to the higher vertex of that order (MC/graph_io.h:261-330);
+ *  - a triangle's type is its number of negative edges: 0 -> T3 (+++),
+ *    1 -> T2 (++-), 2 -> T1 (+--), 3 -> T0 (---) (MC/tc_serial.cpp:95-112).
+ * Vertex ids must be below 2^31 and an edge list below 2^32 elements.
+ */
+#ifndef STC_H
+#define STC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define STC_ABI_VERSION 1
+
+typedef enum stc_status {
+  STC_OK = 0,
+  STC_ERR_INVALID_ARGUMENT = 1, /* null pointer, bad option, malformed CSR */
+  STC_ERR_IO = 2,               /* file cannot be opened / read (MC/graph_io.h:40-59) */
+  STC_ERR_CUDA = 3,             /* a CUDA call failed; see stc_ctx_last_error */
+  STC_ERR_OUT_OF_MEMORY = 4,    /* host or device allocation failed */
+  STC_ERR_LIMIT = 5,            /* id >= 2^31 or list >= 2^32 elements */
+  STC_ERR_DEVICE_TIMEOUT = 6,   /* a bounded device-side wait expired */
+  STC_ERR_NO_DEVICE = 7,        /* no CUDA device, or not an sm_100 part */
+  STC_ERR_INTERNAL = 8          /* a self-check failed (e.g. strategies disagree) */
+} stc_status;
+
+/* GlobalTriCounts (MC/tc_serial.cpp:11-31). */
+typedef struct stc_counts {
+  uint64_t t0; /* --- unbalanced */
+  uint64_t t1; /* +-- balanced   */
+  uint64_t t2; /* ++- unbalanced */
+  uint64_t t3; /* +++ balanced   */
+} stc_counts;
+
+static inline uint64_t stc_balanced(const stc_counts* c) { return c->t1 + c->t3; }
+static inline uint64_t stc_unbalanced(const stc_counts* c) { return c->t0 + c->t2; }
+static inline uint64_t stc_total(const stc_counts* c) { return c->t0 + c->t1 + c->t2 + c->t3; }
+
+/* EdgeList (MC/graph_io.h:14-20) plus the reference's `raw_edges` line count. */
+typedef struct stc_edge_list {
+  uint32_t n;      /* max kept id + 1 */
+  uint64_t lines;  /* non-blank, non-comment lines (printed as raw_edges) */
+  uint64_t m;      /* kept edges */
+  uint32_t* src;   /* min endpoint */
+  uint32_t* dst;   /* max endpoint */
+  int8_t* sign;    /* +1 / -1 */
+} stc_edge_list;
+
+/* ForwardCSR (MC/graph_io.h:22-30) with every list sorted by neighbour id,
+ * i.e. as MC/tc_serial.cpp:33-93 (sort_adj_lists) leaves it. */
+typedef struct stc_forward_csr {
+  uint32_t n;
+  uint64_t m;        /* forward edges */
+  uint64_t* offsets; /* n + 1 */
+  uint32_t* edges;   /* m */
+  int8_t* signs;     /* m */
+  uint32_t* fdeg;    /* n */
+  uint32_t* rank;    /* n: position of each vertex in (degree, id) order */
+} stc_forward_csr;
+
+/* One graph of a batch (host or device arrays, see STC_F_DEVICE_INPUT). */
+typedef struct stc_graph {
+  const uint32_t* src;
+  const uint32_t* dst;
+  const int8_t* sign;
+  uint64_t m;
+} stc_graph;
+
+/* Intersection strategy selection. */
+typedef enum stc_strategy {
+  STC_STRATEGY_AUTO = 0,   /* dispatcher picks per edge bucket (default) */
+  STC_STRATEGY_MERGE = 1,  /* force the warp-cooperative sorted merge */
+  STC_STRATEGY_HASH = 2,   /* force the shared-memory hash probe */
+  STC_STRATEGY_SEARCH = 3  /* force binary search / galloping */
+} stc_strategy;
+
+typedef enum stc_dispatch {
+  STC_DISPATCH_FIXED = 0,   /* fixed degree thresholds (fallback) */
+  STC_DISPATCH_LEARNED = 1  /* learned per-bucket choice, when a model is loaded */
+} stc_dispatch;
+
+/* Option flags. */
+#define STC_F_DEVICE_INPUT 0x1u /* input pointers are device pointers */
+#define STC_F_TIMING 0x2u       /* record per-stage device times (stc_ctx_last_stats) */
+#define STC_F_NO_SYNC 0x4u      /* leave results on device; stc_ctx_counts_device */
+
+typedef struct stc_opts {
+  uint32_t strategy; /* stc_strategy */
+  uint32_t dispatch; /* stc_dispatch */
+  uint32_t flags;    /* STC_F_* */
+  uint32_t reserved;
+  void* stream;      /* cudaStream_t to run on; NULL = the context's own stream */
+} stc_opts;
+
+/* Per-call statistics of the last call on a context. */
+typedef struct stc_stats {
+  uint64_t n;             /* vertices */
+  uint64_t m_input;       /* input edges */
+  uint64_t m_unique;      /* undirected edges after dedup */
+  uint64_t m_forward;     /* forward edges (arcs) */
+  uint64_t alg_bytes;     /* merge-model bytes: sum over arcs of 5 (d+(u) + d+(v)) + 25 */
+  uint64_t triangles;     /* total */
+  double ms_h2d;          /* host -> device copy of the input */
+  double ms_dedup;        /* ingest, sort, unique */
+  double ms_orient;       /* degree, (degree, id) rank, orientation */
+  double ms_csr;          /* forward CSR build (arc sort, offsets) */
+  double ms_count;        /* intersection engine */
+  double ms_total;        /* whole call on the device */
+  uint32_t kernel_launches;
+  uint32_t reserved;
+} stc_stats;
+
+typedef struct stc_ctx stc_ctx;
+
+/* ------------------------------------------------------------ context ---- */
+/* Opens a context on CUDA device `device`.  Fails with STC_ERR_NO_DEVICE when
+ * the device is missing or not compute capability 10.x. */
+stc_status stc_ctx_create(int device, stc_ctx** out);
+void stc_ctx_destroy(stc_ctx* ctx);
+/* Message of the last failure on this context ("" when none). */
+const char* stc_ctx_last_error(const stc_ctx* ctx);
+stc_status stc_ctx_last_stats(const stc_ctx* ctx, stc_stats* out);
+/* Releases the context's cached device buffers. */
+stc_status stc_ctx_trim(stc_ctx* ctx);
+const char* stc_status_string(stc_status s);
+int stc_abi_version(void);
+
+/* --------------------------------------------------------------- ingest ---- */
+/* load_graph / free_edge_list (MC/graph_io.h:100-219): parses a `u v sign`
+ * text file on the host ('#'/'%' lines are comments) with all host threads. */
+stc_status stc_load_edge_list(const char* path, stc_edge_list* out);
+/* Same parse over an in-memory buffer. */
+stc_status stc_parse_edge_text(const char* data, uint64_t size, stc_edge_list* out);
+void stc_free_edge_list(stc_edge_list* el);
+
+/* ---------------------------------------------------------- whole path ---- */
+/* The reference programs' path (MC/tc_serial.cpp:172-210; the Gunrock
+ * plug-in GM/signed_tc.hxx:527-542): dedup, (degree, id) orientation, forward
+ * CSR with int8 signs and the intersection engine, all on the GPU.
+ * src/dst/sign are host arrays, or device arrays with STC_F_DEVICE_INPUT. */
+stc_status stc_count(stc_ctx* ctx, const uint32_t* src, const uint32_t* dst,
+                     const int8_t* sign, uint64_t m, const stc_opts* opts,
+                     stc_counts* out);
+
+/* build_forward_csr + sort_adj_lists (MC/graph_io.h:231-402,
+ * MC/tc_serial.cpp:33-93) on the GPU; the result is returned in host memory
+ * in the reference's layout.  Free with stc_free_forward_csr. */
+stc_status stc_build_forward_csr(stc_ctx* ctx, const uint32_t* src, const uint32_t* dst,
+                                 const int8_t* sign, uint64_t m, const stc_opts* opts,
+                                 stc_forward_csr* out);
+void stc_free_forward_csr(stc_forward_csr* csr);
+
+/* count_triangles (MC/tc_serial.cpp:138-170) over a host forward CSR in the
+ * reference layout (lists sorted by id, every edge from lower to higher rank). */
+stc_status stc_count_forward_csr(stc_ctx* ctx, const stc_forward_csr* csr,
+                                 const stc_opts* opts, stc_counts* out);
+
+/* Per-source counts, the cnt[4n] array of MC/tc_serial.cpp:141-158: entry
+ * 4u + k is the number of type-k triangles (k = 0..3 as in stc_counts) whose
+ * lowest-ranked vertex is u.  `counts` is a host array of 4 * n words where n
+ * is max id + 1 of the kept edges. */
+stc_status stc_vertex_counts(stc_ctx* ctx, const uint32_t* src, const uint32_t* dst,
+                             const int8_t* sign, uint64_t m, const stc_opts* opts,
+                             uint64_t* counts, uint64_t counts_len, uint32_t* n_out);
+
+/* ---------------------------------------------------------------- batch ---- */
+/* Counts G independent graphs; outs[g] receives graph g's counts. */
+stc_status stc_count_batch(stc_ctx* ctx, const stc_graph* graphs, uint32_t G,
+                           const stc_opts* opts, stc_counts* outs);
+
+/* --------------------------------------------------- device generator ---- */
+/* Writes the RMAT samples of stc_synth_rmat (include/stc_synth.h) for the
+ * same arguments directly into device arrays of `samples` elements. */
+stc_status stc_synth_rmat_device(stc_ctx* ctx, uint64_t seed, uint32_t scale, uint64_t n,
+                                 uint64_t samples, double a, double b, double c, double p_pos,
+                                 uint32_t* d_src, uint32_t* d_dst, int8_t* d_sign);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* STC_H */

@@ -1,0 +1,323 @@
+"""B200-native signed triangle counting (host mirror of the reference interface).
+
+The reference's CPU programs expose ``load_graph`` / ``build_forward_csr`` /
+``count_triangles`` and a ``GlobalTriCounts`` result
+("Signed_TC/Multicore Implementations/graph_io.h:100,231",
+"tc_serial.cpp:11-31,138").  This module keeps those names and meanings over
+the C ABI of ``libstc.so`` (include/stc.h); every counting call runs on the
+GPU through hand-written sm_100a kernels and fails loudly when the native
+library or a CUDA device is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Iterable, Optional, Sequence
+
+import numpy as np
+
+from . import _capi
+from ._capi import lib
+
+__all__ = [
+    "GlobalTriCounts", "EdgeList", "ForwardCSR", "Stats", "StcError", "Context",
+    "load_graph", "parse_edge_text", "synth",
+]
+
+
+class StcError(RuntimeError):
+    """A non-zero stc_status, with the context's last error message."""
+
+    def __init__(self, status: int, message: str = ""):
+        name = lib().stc_status_string(status).decode()
+        super().__init__(f"{name} ({status})" + (f": {message}" if message else ""))
+        self.status = status
+        self.message = message
+
+
+@dataclass(frozen=True)
+class GlobalTriCounts:
+    """Per-type triangle counts (tc_serial.cpp:11-31): t3 = +++, t2 = ++-,
+    t1 = +--, t0 = ---."""
+
+    t0: int
+    t1: int
+    t2: int
+    t3: int
+
+    def balanced(self) -> int:
+        return self.t1 + self.t3
+
+    def unbalanced(self) -> int:
+        return self.t0 + self.t2
+
+    def total(self) -> int:
+        return self.t0 + self.t1 + self.t2 + self.t3
+
+    def as_tuple(self) -> tuple:
+        return (self.t0, self.t1, self.t2, self.t3)
+
+    def format(self) -> str:
+        """The block tc_serial prints (tc_serial.cpp:18-30)."""
+        return (
+            "\nTriangle counts\n"
+            f"  T3 (+++ balanced)   : {self.t3}\n"
+            f"  T1 (+-- balanced)   : {self.t1}\n"
+            f"  T2 (++- unbalanced) : {self.t2}\n"
+            f"  T0 (--- unbalanced) : {self.t0}\n"
+            "  --------------------------------\n"
+            f"  balanced total      : {self.balanced()}\n"
+            f"  unbalanced total    : {self.unbalanced()}\n"
+            f"  grand total         : {self.total()}\n")
+
+    def print(self) -> None:
+        print(self.format(), end="")
+
+
+@dataclass
+class EdgeList:
+    """EdgeList (graph_io.h:14-20): src = min endpoint, dst = max endpoint."""
+
+    n: int
+    m: int
+    src: np.ndarray
+    dst: np.ndarray
+    sign: np.ndarray
+    lines: int = 0
+
+
+@dataclass
+class ForwardCSR:
+    """ForwardCSR (graph_io.h:22-30) with lists sorted by neighbour id."""
+
+    n: int
+    m: int
+    offsets: np.ndarray
+    edges: np.ndarray
+    signs: np.ndarray
+    fdeg: np.ndarray
+    rank: np.ndarray
+
+
+@dataclass
+class Stats:
+    n: int
+    m_input: int
+    m_unique: int
+    m_forward: int
+    alg_bytes: int
+    triangles: int
+    ms_h2d: float
+    ms_dedup: float
+    ms_orient: float
+    ms_csr: float
+    ms_count: float
+    ms_total: float
+    kernel_launches: int
+
+
+def _check(status: int, ctx=None) -> None:
+    if status != _capi.STC_OK:
+        msg = lib().stc_ctx_last_error(ctx).decode() if ctx else ""
+        raise StcError(status, msg)
+
+
+def _edge_list_from_c(el: _capi.stc_edge_list) -> EdgeList:
+    m = el.m
+    if m:
+        src = np.ctypeslib.as_array(el.src, (m,)).copy()
+        dst = np.ctypeslib.as_array(el.dst, (m,)).copy()
+        sign = np.ctypeslib.as_array(el.sign, (m,)).copy()
+    else:
+        src = np.zeros(0, np.uint32)
+        dst = np.zeros(0, np.uint32)
+        sign = np.zeros(0, np.int8)
+    return EdgeList(n=el.n, m=m, src=src, dst=dst, sign=sign, lines=el.lines)
+
+
+def load_graph(path: str) -> EdgeList:
+    """load_graph (graph_io.h:100-212): parses a `u v sign` file on the host."""
+    el = _capi.stc_edge_list()
+    st = lib().stc_load_edge_list(str(path).encode(), C.byref(el))
+    if st == _capi.STC_ERR_IO:
+        raise OSError(f"cannot read {path}")
+    _check(st)
+    try:
+        return _edge_list_from_c(el)
+    finally:
+        lib().stc_free_edge_list(C.byref(el))
+
+
+def parse_edge_text(data: bytes) -> EdgeList:
+    el = _capi.stc_edge_list()
+    _check(lib().stc_parse_edge_text(data, len(data), C.byref(el)))
+    try:
+        return _edge_list_from_c(el)
+    finally:
+        lib().stc_free_edge_list(C.byref(el))
+
+
+def _host_arrays(src, dst, sign):
+    src = np.ascontiguousarray(src, dtype=np.uint32)
+    dst = np.ascontiguousarray(dst, dtype=np.uint32)
+    sign = np.ascontiguousarray(sign, dtype=np.int8)
+    if not (len(src) == len(dst) == len(sign)):
+        raise ValueError("src, dst and sign must have the same length")
+    return src, dst, sign
+
+
+def _ptr(a) -> C.c_void_p:
+    if hasattr(a, "data_ptr"):  # torch tensor
+        return C.c_void_p(a.data_ptr())
+    return C.c_void_p(a.ctypes.data)
+
+
+class Context:
+    """Owns an stc_ctx (device memory, stream) on one CUDA device."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        st = lib().stc_ctx_create(device, C.byref(h))
+        _check(st)
+        self._h = h
+        self.device = device
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().stc_ctx_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _opts(strategy="auto", dispatch="fixed", device_input=False, timing=True,
+              stream: Optional[int] = None) -> _capi.stc_opts:
+        o = _capi.stc_opts()
+        o.strategy = _capi.STRATEGY[strategy]
+        o.dispatch = _capi.DISPATCH[dispatch]
+        o.flags = (_capi.F_DEVICE_INPUT if device_input else 0) | (_capi.F_TIMING if timing else 0)
+        o.stream = C.c_void_p(stream) if stream else None
+        return o
+
+    def count(self, src, dst, sign, *, strategy="auto", dispatch="fixed", stream=None,
+              timing=True) -> GlobalTriCounts:
+        """Whole path (dedup, orientation, CSR, intersection) on the GPU.
+
+        Host numpy arrays are copied to the device; torch CUDA tensors
+        (uint32/int32 ids, int8 signs) are used in place."""
+        dev = hasattr(src, "is_cuda") and src.is_cuda
+        if dev:
+            m = int(src.numel())
+            ps, pd, pg = _ptr(src), _ptr(dst), _ptr(sign)
+            if stream is None:  # stay ordered after the torch kernels that made the tensors
+                import torch
+                stream = torch.cuda.current_stream(src.device).cuda_stream
+        else:
+            src, dst, sign = _host_arrays(src, dst, sign)
+            m = len(src)
+            ps, pd, pg = _ptr(src), _ptr(dst), _ptr(sign)
+        out = _capi.stc_counts()
+        o = self._opts(strategy, dispatch, dev, timing, stream)
+        _check(lib().stc_count(self._h, ps, pd, pg, m, C.byref(o), C.byref(out)), self._h)
+        return GlobalTriCounts(out.t0, out.t1, out.t2, out.t3)
+
+    def count_edge_list(self, el: EdgeList, **kw) -> GlobalTriCounts:
+        return self.count(el.src, el.dst, el.sign, **kw)
+
+    def build_forward_csr(self, src, dst, sign) -> ForwardCSR:
+        """build_forward_csr + sort_adj_lists (graph_io.h:231-402,
+        tc_serial.cpp:33-93) on the GPU, returned in the reference layout."""
+        src, dst, sign = _host_arrays(src, dst, sign)
+        out = _capi.stc_forward_csr()
+        o = self._opts()
+        _check(lib().stc_build_forward_csr(self._h, _ptr(src), _ptr(dst), _ptr(sign), len(src),
+                                           C.byref(o), C.byref(out)), self._h)
+        try:
+            n, m = out.n, out.m
+            return ForwardCSR(
+                n=n, m=m,
+                offsets=np.ctypeslib.as_array(out.offsets, (n + 1,)).copy(),
+                edges=np.ctypeslib.as_array(out.edges, (m,)).copy() if m else np.zeros(0, np.uint32),
+                signs=np.ctypeslib.as_array(out.signs, (m,)).copy() if m else np.zeros(0, np.int8),
+                fdeg=np.ctypeslib.as_array(out.fdeg, (n,)).copy() if n else np.zeros(0, np.uint32),
+                rank=np.ctypeslib.as_array(out.rank, (n,)).copy() if n else np.zeros(0, np.uint32))
+        finally:
+            lib().stc_free_forward_csr(C.byref(out))
+
+    def count_triangles(self, csr: ForwardCSR, *, strategy="auto", dispatch="fixed") -> GlobalTriCounts:
+        """count_triangles (tc_serial.cpp:138-170) over a reference-layout CSR."""
+        offsets = np.ascontiguousarray(csr.offsets, np.uint64)
+        edges = np.ascontiguousarray(csr.edges, np.uint32)
+        signs = np.ascontiguousarray(csr.signs, np.int8)
+        fdeg = np.ascontiguousarray(csr.fdeg, np.uint32)
+        rank = np.ascontiguousarray(csr.rank, np.uint32)
+        c = _capi.stc_forward_csr()
+        c.n, c.m = csr.n, csr.m
+        c.offsets = offsets.ctypes.data_as(_capi.u64p)
+        c.edges = edges.ctypes.data_as(_capi.u32p)
+        c.signs = signs.ctypes.data_as(_capi.i8p)
+        c.fdeg = fdeg.ctypes.data_as(_capi.u32p)
+        c.rank = rank.ctypes.data_as(_capi.u32p)
+        out = _capi.stc_counts()
+        o = self._opts(strategy, dispatch)
+        _check(lib().stc_count_forward_csr(self._h, C.byref(c), C.byref(o), C.byref(out)), self._h)
+        return GlobalTriCounts(out.t0, out.t1, out.t2, out.t3)
+
+    def vertex_counts(self, src, dst, sign, *, strategy="auto") -> np.ndarray:
+        """Per-source counts cnt[4n] (tc_serial.cpp:141-158) as an (n, 4) array."""
+        src, dst, sign = _host_arrays(src, dst, sign)
+        n_out = C.c_uint32()
+        o = self._opts(strategy)
+        n_bound = int(max(src.max(initial=0), dst.max(initial=0))) + 1 if len(src) else 0
+        buf = np.zeros(4 * max(n_bound, 1), np.uint64)
+        _check(lib().stc_vertex_counts(self._h, _ptr(src), _ptr(dst), _ptr(sign), len(src),
+                                       C.byref(o), buf.ctypes.data_as(_capi.u64p), len(buf),
+                                       C.byref(n_out)), self._h)
+        return buf[: 4 * n_out.value].reshape(-1, 4)
+
+    def count_batch(self, graphs: Sequence[tuple], *, strategy="auto", dispatch="fixed",
+                    stream=None) -> list:
+        """Counts independent graphs given as (src, dst, sign) triples."""
+        keep = []
+        arr = (_capi.stc_graph * max(1, len(graphs)))()
+        dev = False
+        for i, (s, d, g) in enumerate(graphs):
+            dev = hasattr(s, "is_cuda") and s.is_cuda
+            if not dev:
+                s, d, g = _host_arrays(s, d, g)
+            keep.append((s, d, g))
+            arr[i].src = C.cast(_ptr(s), _capi.u32p)
+            arr[i].dst = C.cast(_ptr(d), _capi.u32p)
+            arr[i].sign = C.cast(_ptr(g), _capi.i8p)
+            arr[i].m = int(s.numel()) if dev else len(s)
+        outs = (_capi.stc_counts * max(1, len(graphs)))()
+        if dev and stream is None:
+            import torch
+            stream = torch.cuda.current_stream(keep[0][0].device).cuda_stream
+        o = self._opts(strategy, dispatch, dev, True, stream)
+        _check(lib().stc_count_batch(self._h, arr, len(graphs), C.byref(o), outs), self._h)
+        return [GlobalTriCounts(x.t0, x.t1, x.t2, x.t3) for x in outs[: len(graphs)]]
+
+    def last_stats(self) -> Stats:
+        s = _capi.stc_stats()
+        _check(lib().stc_ctx_last_stats(self._h, C.byref(s)))
+        return Stats(**{f: getattr(s, f) for f, _ in _capi.stc_stats._fields_ if f != "reserved"})
+
+    def synth_rmat_device(self, seed: int, scale: int, n: int, samples: int, a: float, b: float,
+                          c: float, p_pos: float, src, dst, sign) -> None:
+        """Fills device arrays (torch tensors) with stc_synth_rmat's samples."""
+        _check(lib().stc_synth_rmat_device(self._h, seed, scale, n, samples, a, b, c, p_pos,
+                                           _ptr(src), _ptr(dst), _ptr(sign)), self._h)
+
+
+from . import synth  # noqa: E402  (needs the names above)

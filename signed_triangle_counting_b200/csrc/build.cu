@@ -1,0 +1,429 @@
+// Graph build on the GPU: ingest + dedup, degree, (degree, id) rank,
+// orientation and the forward CSR with an int8 sign array.
+//
+// Reference: build_forward_csr (MC/graph_io.h:231-402) followed by
+// sort_adj_lists (MC/tc_serial.cpp:33-93), MC = "Signed_TC/Multicore
+// Implementations".  The reference sorts 12-byte structs on one thread,
+// counting-sorts vertices by degree and scatters arcs with atomics into
+// unsorted lists that a second pass sorts.  Here every stage is a sort or a
+// streaming pass over HBM:
+//
+//   1. pack   (min << b | max), sign in bit 63; self-loops -> sentinel keys
+//   2. stable radix sort over the 2b id bits; keep the first key of each run
+//      (== the reference's "first of equal (u, v)", made deterministic)
+//   3. degree = atomics over the unique keys (warp-aggregated on the min id)
+//   4. rank   = stable radix sort of (deg << 32 | id) on the degree bits:
+//      ties fall back to ascending id exactly like the counting sort at
+//      MC/graph_io.h:270-317
+//   5. orient + relabel into rank space: arc (rank lo -> rank hi); sorting
+//      these keys gives every list already sorted, so no per-list sort
+//   6. offsets = exclusive scan of out-degrees.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "internal.h"
+#include "radix_sort.cuh"
+#include "stc_device.cuh"
+
+namespace stc {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+inline uint32_t grid_for(uint64_t n, uint32_t per_thread = 1) {
+  uint64_t g = (n + (uint64_t)kThreads * per_thread - 1) / ((uint64_t)kThreads * per_thread);
+  if (g < 1) g = 1;
+  if (g > (uint64_t)kSMs * 16) g = kSMs * 16;
+  return (uint32_t)g;
+}
+
+// Max kept id and self-loop count.
+__global__ void k_scan_ids(const uint32_t* __restrict__ u, const uint32_t* __restrict__ v,
+                           uint64_t m, unsigned long long* __restrict__ ctr) {
+  uint32_t mx = 0;
+  uint32_t self = 0;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
+    const uint32_t a = __ldcs(u + i), b = __ldcs(v + i);
+    if (a == b) {
+      self++;
+    } else {
+      mx = max(mx, max(a, b));
+    }
+  }
+  mx = __reduce_max_sync(kFull, mx);
+  self = __reduce_add_sync(kFull, self);
+  if (lane_id() == 0) {
+    atomicMax(ctr + C_MAX_ID, (unsigned long long)mx);
+    if (self) atomicAdd(ctr + C_SELF, (unsigned long long)self);
+  }
+}
+
+// Dedup keys: (min << bits | max) with the negative flag in bit 63; a
+// self-loop becomes the all-ones sentinel of the 2*bits window, which sorts
+// last and can never equal a real key (real keys have min < max).
+__global__ void k_pack_dedup(const uint32_t* __restrict__ u, const uint32_t* __restrict__ v,
+                             const int8_t* __restrict__ s, uint64_t m, uint32_t bits,
+                             uint64_t* __restrict__ keys) {
+  const uint64_t sentinel = (bits * 2 >= 64) ? ~0ull >> 1 : ((1ull << (2 * bits)) - 1);
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
+    const uint32_t a = __ldcs(u + i), b = __ldcs(v + i);
+    const int8_t sg = __ldcs(s + i);
+    uint64_t k;
+    if (a == b) {
+      k = sentinel;
+    } else {
+      const uint64_t lo = a < b ? a : b, hi = a < b ? b : a;
+      k = (lo << bits) | hi | ((uint64_t)(sg < 0) << 63);
+    }
+    keys[i] = k;
+  }
+}
+
+struct UniqueFlag {
+  const uint64_t* keys;
+  uint64_t mask;
+  __device__ uint32_t operator()(uint64_t i) const {
+    if (i == 0) return 1u;
+    return (keys[i] & mask) != (keys[i - 1] & mask) ? 1u : 0u;
+  }
+};
+struct UniqueEmit {
+  const uint64_t* keys;
+  uint64_t* out;
+  __device__ void operator()(uint64_t i, uint64_t pos, uint32_t flag) const {
+    if (flag) out[pos] = keys[i];
+  }
+};
+
+// Undirected degree over unique keys; the min endpoint arrives in runs (the
+// keys are sorted by it), so lanes sharing it add once.
+__global__ void k_degree(const uint64_t* __restrict__ keys, uint64_t mu, uint32_t bits,
+                         uint32_t* __restrict__ deg) {
+  const uint64_t idmask = (1ull << bits) - 1;
+  const uint64_t wstride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < mu;
+       base += wstride) {
+    const uint64_t i = base + lane_id();
+    const bool valid = i < mu;
+    const uint64_t k = valid ? keys[i] : 0;
+    const uint32_t a = valid ? (uint32_t)((k >> bits) & idmask) : 0xFFFFFFFFu;
+    const uint32_t b = (uint32_t)(k & idmask);
+    const unsigned peers = __match_any_sync(kFull, a);
+    if (valid && (peers & lanemask_lt()) == 0) atomicAdd(deg + a, (uint32_t)__popc(peers));
+    if (valid) atomicAdd(deg + b, 1u);
+  }
+}
+
+// Vertex sort keys (deg << 32 | id) and the max degree.
+__global__ void k_vertex_keys(const uint32_t* __restrict__ deg, uint32_t n,
+                              uint64_t* __restrict__ vkeys, unsigned long long* __restrict__ ctr) {
+  uint32_t mx = 0;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint32_t d = deg[i];
+    vkeys[i] = ((uint64_t)d << 32) | i;
+    mx = max(mx, d);
+  }
+  mx = __reduce_max_sync(kFull, mx);
+  if (lane_id() == 0) atomicMax(ctr + C_MAX_DEG, (unsigned long long)mx);
+}
+
+__global__ void k_rank(const uint64_t* __restrict__ vkeys, uint32_t n, uint32_t* __restrict__ verts,
+                       uint32_t* __restrict__ rank) {
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += stride) {
+    const uint32_t id = (uint32_t)vkeys[r];
+    verts[r] = id;
+    rank[id] = r;
+  }
+}
+
+// Orientation + relabelling: arc key (rank lo << bits | rank hi), sign in
+// bit 63; out-degree histogram by rank.
+__global__ void k_arc_keys(const uint64_t* __restrict__ ukeys, uint64_t mu, uint32_t bits,
+                           const uint32_t* __restrict__ rank, uint64_t* __restrict__ akeys,
+                           uint32_t* __restrict__ fdeg) {
+  const uint64_t idmask = (1ull << bits) - 1;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < mu; i += stride) {
+    const uint64_t k = ukeys[i];
+    const uint32_t ra = rank[(k >> bits) & idmask], rb = rank[k & idmask];
+    const uint32_t lo = min(ra, rb), hi = max(ra, rb);
+    akeys[i] = ((uint64_t)lo << bits) | hi | (k & (1ull << 63));
+    atomicAdd(fdeg + lo, 1u);
+  }
+}
+
+struct LoadU32 {
+  const uint32_t* a;
+  __device__ uint32_t operator()(uint64_t i) const { return a[i]; }
+};
+struct EmitOffset {
+  uint64_t* off;
+  __device__ void operator()(uint64_t i, uint64_t pos, uint32_t) const { off[i] = pos; }
+};
+
+// Splits sorted arc keys into the neighbour and sign arrays and accumulates
+// the merge-model byte count 5 (d+(u) + d+(v)) + 25 per arc.
+__global__ void k_csr_fill(const uint64_t* __restrict__ akeys, uint64_t ma, uint32_t bits,
+                           const uint32_t* __restrict__ fdeg, uint32_t* __restrict__ nbr,
+                           int8_t* __restrict__ sgn, unsigned long long* __restrict__ ctr) {
+  const uint64_t idmask = (1ull << bits) - 1;
+  unsigned long long bytes = 0;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ma; i += stride) {
+    const uint64_t k = akeys[i];
+    const uint32_t src = (uint32_t)((k >> bits) & idmask), dst = (uint32_t)(k & idmask);
+    nbr[i] = dst;
+    sgn[i] = (k >> 63) ? (int8_t)-1 : (int8_t)1;
+    bytes += 5ull * ((unsigned long long)fdeg[src] + fdeg[dst]) + 25ull;
+  }
+  bytes = warp_sum(bytes);
+  if (lane_id() == 0 && bytes) atomicAdd(ctr + C_ALG_BYTES, bytes);
+}
+
+// Arc keys of a reference-layout CSR: one warp per vertex.
+__global__ void k_csr_arc_keys(const uint64_t* __restrict__ off, const uint32_t* __restrict__ edges,
+                               const int8_t* __restrict__ signs, const uint32_t* __restrict__ rank,
+                               uint32_t n, uint32_t bits, uint64_t* __restrict__ akeys,
+                               uint32_t* __restrict__ fdeg, unsigned long long* __restrict__ ctr) {
+  const uint32_t warps = gridDim.x * (blockDim.x / 32);
+  for (uint32_t u = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); u < n; u += warps) {
+    const uint64_t b = off[u], e = off[u + 1];
+    const uint32_t ru = rank[u];
+    for (uint64_t i = b + lane_id(); i < e; i += 32) {
+      const uint32_t w = edges[i];
+      if (w >= n || rank[w] <= ru) {
+        atomicExch(ctr + C_ERROR, 1ull);  // not a forward CSR of this rank order
+        continue;
+      }
+      akeys[i] = ((uint64_t)ru << bits) | rank[w] | ((uint64_t)(signs[i] < 0) << 63);
+    }
+    if (lane_id() == 0) fdeg[ru] = (uint32_t)(e - b);
+  }
+}
+
+// Id-space export keys: (source id << bits | head id), sign in bit 63.
+__global__ void k_export_keys(const uint64_t* __restrict__ ukeys, uint64_t mu, uint32_t bits,
+                              const uint32_t* __restrict__ rank, uint64_t* __restrict__ ekeys,
+                              uint32_t* __restrict__ fdeg_id) {
+  const uint64_t idmask = (1ull << bits) - 1;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < mu; i += stride) {
+    const uint64_t k = ukeys[i];
+    const uint32_t a = (uint32_t)((k >> bits) & idmask), b = (uint32_t)(k & idmask);
+    const bool fwd = rank[a] < rank[b];
+    const uint32_t s = fwd ? a : b, t = fwd ? b : a;
+    ekeys[i] = ((uint64_t)s << bits) | t | (k & (1ull << 63));
+    atomicAdd(fdeg_id + s, 1u);
+  }
+}
+
+void read_counters(stc_ctx* c, int first, int count) {
+  STC_CUDA(cudaMemcpyAsync(c->h_pinned + first, counters(c) + first, count * sizeof(uint64_t),
+                           cudaMemcpyDeviceToHost, c->stream));
+  STC_CUDA(cudaStreamSynchronize(c->stream));
+}
+
+// Rank-space CSR from unique keys: arc keys, sort, offsets, fill.
+void finish_csr_from_arc_keys(stc_ctx* c, DeviceGraph& g, uint64_t* akeys, uint64_t* alt) {
+  uint32_t* sort_counts = buffer<uint32_t>(c, B_SORT_COUNTS, (size_t)kRadix * kMaxSortGrid);
+  uint64_t* sums = buffer<uint64_t>(c, B_SCAN_SUMS, kMaxSortGrid + 1);
+  uint64_t* sorted = radix_sort(akeys, alt, g.m_fwd, 0, 2 * (int)g.bits, sort_counts, c->stream,
+                                &c->launches);
+  g.off = buffer<uint64_t>(c, B_OFF, (size_t)g.n + 1);
+  range_scan(LoadU32{g.fdeg}, EmitOffset{g.off}, g.n, sums, c->stream, &c->launches);
+  STC_CUDA(cudaMemcpyAsync(g.off + g.n, sums + range_partition(g.n, kScanTile, kMaxSortGrid).grid,
+                           sizeof(uint64_t), cudaMemcpyDeviceToDevice, c->stream));
+  g.nbr = buffer<uint32_t>(c, B_NBR, g.m_fwd);
+  g.sgn = buffer<int8_t>(c, B_SGN, g.m_fwd);
+  k_csr_fill<<<grid_for(g.m_fwd, 4), kThreads, 0, c->stream>>>(sorted, g.m_fwd, g.bits, g.fdeg,
+                                                               g.nbr, g.sgn, (unsigned long long*)counters(c));
+  c->launches += 1;
+  STC_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+
+void build_graph(stc_ctx* c, const uint32_t* d_src, const uint32_t* d_dst, const int8_t* d_sign,
+                 uint64_t m, DeviceGraph& g) {
+  cudaStream_t st = c->stream;
+  unsigned long long* ctr = (unsigned long long*)counters(c);
+  g = DeviceGraph{};
+  g.m_input = m;
+  if (m >= (1ull << 32)) fail(STC_ERR_LIMIT, "edge list has 2^32 or more elements");
+
+  // 1. ids: max kept id and self-loops.
+  mark(c, 1);
+  if (m) {
+    k_scan_ids<<<grid_for(m, 4), kThreads, 0, st>>>(d_src, d_dst, m, ctr);
+    c->launches++;
+  }
+  read_counters(c, C_MAX_ID, 2);
+  const uint64_t max_id = c->h_pinned[C_MAX_ID];
+  const uint64_t self = c->h_pinned[C_SELF];
+  if (max_id >= (1ull << 31)) fail(STC_ERR_LIMIT, "vertex id " + std::to_string(max_id) + " >= 2^31");
+  g.n = m ? (uint32_t)max_id + 1 : 0;
+  g.m_valid = m - self;
+  g.bits = std::max<uint32_t>(1, bit_width64(max_id));
+  uint32_t* sort_counts = buffer<uint32_t>(c, B_SORT_COUNTS, (size_t)kRadix * kMaxSortGrid);
+  uint64_t* sums = buffer<uint64_t>(c, B_SCAN_SUMS, kMaxSortGrid + 1);
+
+  // 2. dedup.
+  uint64_t* ka = buffer<uint64_t>(c, B_KEYS_A, m);
+  uint64_t* kb = buffer<uint64_t>(c, B_KEYS_B, m);
+  g.ukeys = buffer<uint64_t>(c, B_UKEYS, g.m_valid);
+  if (g.m_valid) {
+    k_pack_dedup<<<grid_for(m, 4), kThreads, 0, st>>>(d_src, d_dst, d_sign, m, g.bits, ka);
+    c->launches++;
+    uint64_t* sorted = radix_sort(ka, kb, m, 0, 2 * (int)g.bits, sort_counts, st, &c->launches);
+    const uint64_t mask = (1ull << (2 * g.bits)) - 1;
+    range_scan(UniqueFlag{sorted, mask}, UniqueEmit{sorted, g.ukeys}, g.m_valid, sums, st,
+               &c->launches);
+    const uint32_t grid = range_partition(g.m_valid, kScanTile, kMaxSortGrid).grid;
+    STC_CUDA(cudaMemcpyAsync(c->h_pinned + C_WORK, sums + grid, sizeof(uint64_t),
+                             cudaMemcpyDeviceToHost, st));
+    STC_CUDA(cudaStreamSynchronize(st));
+    g.m_unique = c->h_pinned[C_WORK];
+  }
+  STC_CUDA(cudaGetLastError());
+  mark(c, 2);
+
+  // 3-4. degree and (degree, id) rank.
+  g.deg = buffer<uint32_t>(c, B_DEG, g.n);
+  g.rank = buffer<uint32_t>(c, B_RANK, g.n);
+  g.verts = buffer<uint32_t>(c, B_VERTS, g.n);
+  g.fdeg = buffer<uint32_t>(c, B_FDEG, g.n);
+  if (g.n) {
+    STC_CUDA(cudaMemsetAsync(g.deg, 0, (size_t)g.n * sizeof(uint32_t), st));
+    STC_CUDA(cudaMemsetAsync(g.fdeg, 0, (size_t)g.n * sizeof(uint32_t), st));
+    if (g.m_unique) {
+      k_degree<<<grid_for(g.m_unique, 4), kThreads, 0, st>>>(g.ukeys, g.m_unique, g.bits, g.deg);
+      c->launches++;
+    }
+    uint64_t* va = buffer<uint64_t>(c, B_VKEYS_A, g.n);
+    uint64_t* vb = buffer<uint64_t>(c, B_VKEYS_B, g.n);
+    k_vertex_keys<<<grid_for(g.n, 4), kThreads, 0, st>>>(g.deg, g.n, va, ctr);
+    c->launches++;
+    read_counters(c, C_MAX_DEG, 1);
+    g.max_deg = (uint32_t)c->h_pinned[C_MAX_DEG];
+    uint64_t* vs = radix_sort(va, vb, g.n, 32, 32 + (int)bit_width64(g.max_deg), sort_counts, st,
+                              &c->launches);
+    k_rank<<<grid_for(g.n, 4), kThreads, 0, st>>>(vs, g.n, g.verts, g.rank);
+    c->launches++;
+  }
+  STC_CUDA(cudaGetLastError());
+  mark(c, 3);
+
+  // 5-6. orientation into rank space and the forward CSR.
+  g.m_fwd = g.m_unique;
+  if (g.m_fwd) {
+    k_arc_keys<<<grid_for(g.m_fwd, 4), kThreads, 0, st>>>(g.ukeys, g.m_fwd, g.bits, g.rank, ka,
+                                                          g.fdeg);
+    c->launches++;
+    finish_csr_from_arc_keys(c, g, ka, kb);
+  } else {
+    g.off = buffer<uint64_t>(c, B_OFF, (size_t)g.n + 1);
+    STC_CUDA(cudaMemsetAsync(g.off, 0, ((size_t)g.n + 1) * sizeof(uint64_t), st));
+    g.nbr = buffer<uint32_t>(c, B_NBR, 1);
+    g.sgn = buffer<int8_t>(c, B_SGN, 1);
+  }
+  mark(c, 4);
+}
+
+void graph_from_forward_csr(stc_ctx* c, uint32_t n, uint64_t m, const uint64_t* d_off,
+                            const uint32_t* d_edges, const int8_t* d_signs, const uint32_t* d_rank,
+                            DeviceGraph& g) {
+  cudaStream_t st = c->stream;
+  unsigned long long* ctr = (unsigned long long*)counters(c);
+  g = DeviceGraph{};
+  g.n = n;
+  g.m_input = g.m_valid = g.m_unique = g.m_fwd = m;
+  if (m >= (1ull << 32)) fail(STC_ERR_LIMIT, "forward CSR has 2^32 or more edges");
+  if (n >= (1u << 31)) fail(STC_ERR_LIMIT, "forward CSR has 2^31 or more vertices");
+  g.bits = std::max<uint32_t>(1, bit_width64(n ? n - 1 : 0));
+  g.rank = const_cast<uint32_t*>(d_rank);
+  g.fdeg = buffer<uint32_t>(c, B_FDEG, n);
+  mark(c, 1);
+  mark(c, 2);
+  mark(c, 3);
+  if (m) {
+    uint64_t* ka = buffer<uint64_t>(c, B_KEYS_A, m);
+    uint64_t* kb = buffer<uint64_t>(c, B_KEYS_B, m);
+    k_csr_arc_keys<<<kSMs * 8, kThreads, 0, st>>>(d_off, d_edges, d_signs, d_rank, n, g.bits, ka,
+                                                  g.fdeg, ctr);
+    c->launches++;
+    read_counters(c, C_ERROR, 1);
+    if (c->h_pinned[C_ERROR]) {
+      fail(STC_ERR_INVALID_ARGUMENT,
+           "forward CSR has an edge that does not go from lower to higher rank or an id >= n");
+    }
+    finish_csr_from_arc_keys(c, g, ka, kb);
+  } else {
+    g.off = buffer<uint64_t>(c, B_OFF, (size_t)n + 1);
+    STC_CUDA(cudaMemsetAsync(g.off, 0, ((size_t)n + 1) * sizeof(uint64_t), st));
+    g.nbr = buffer<uint32_t>(c, B_NBR, 1);
+    g.sgn = buffer<int8_t>(c, B_SGN, 1);
+  }
+  mark(c, 4);
+}
+
+void export_forward_csr(stc_ctx* c, const DeviceGraph& g, stc_forward_csr* out) {
+  cudaStream_t st = c->stream;
+  const uint32_t n = g.n;
+  const uint64_t mu = g.m_unique;
+  uint32_t* fdeg_id = buffer<uint32_t>(c, B_EXPORT_FDEG, n);
+  uint64_t* off_id = buffer<uint64_t>(c, B_EXPORT_OFF, (size_t)n + 1);
+  uint64_t* ka = buffer<uint64_t>(c, B_KEYS_A, mu);
+  uint64_t* kb = buffer<uint64_t>(c, B_KEYS_B, mu);
+  uint32_t* sort_counts = buffer<uint32_t>(c, B_SORT_COUNTS, (size_t)kRadix * kMaxSortGrid);
+  uint64_t* sums = buffer<uint64_t>(c, B_SCAN_SUMS, kMaxSortGrid + 1);
+  uint32_t* edges = buffer<uint32_t>(c, B_NBR, mu);
+  int8_t* signs = buffer<int8_t>(c, B_SGN, mu);
+  if (n) STC_CUDA(cudaMemsetAsync(fdeg_id, 0, (size_t)n * sizeof(uint32_t), st));
+  uint64_t* sorted = ka;
+  if (mu) {
+    k_export_keys<<<grid_for(mu, 4), kThreads, 0, st>>>(g.ukeys, mu, g.bits, g.rank, ka, fdeg_id);
+    sorted = radix_sort(ka, kb, mu, 0, 2 * (int)g.bits, sort_counts, st, &c->launches);
+  }
+  if (n) {
+    range_scan(LoadU32{fdeg_id}, EmitOffset{off_id}, n, sums, st, &c->launches);
+    STC_CUDA(cudaMemcpyAsync(off_id + n, sums + range_partition(n, kScanTile, kMaxSortGrid).grid,
+                             sizeof(uint64_t), cudaMemcpyDeviceToDevice, st));
+  }
+  if (mu) {
+    k_csr_fill<<<grid_for(mu, 4), kThreads, 0, st>>>(sorted, mu, g.bits, fdeg_id, edges, signs,
+                                                     (unsigned long long*)counters(c));
+  }
+  STC_CUDA(cudaGetLastError());
+  out->n = n;
+  out->m = mu;
+  out->offsets = (uint64_t*)malloc(((size_t)n + 1) * sizeof(uint64_t));
+  out->edges = (uint32_t*)malloc((mu ? mu : 1) * sizeof(uint32_t));
+  out->signs = (int8_t*)malloc(mu ? mu : 1);
+  out->fdeg = (uint32_t*)malloc((n ? n : 1) * sizeof(uint32_t));
+  out->rank = (uint32_t*)malloc((n ? n : 1) * sizeof(uint32_t));
+  if (!out->offsets || !out->edges || !out->signs || !out->fdeg || !out->rank) {
+    stc_free_forward_csr(out);
+    fail(STC_ERR_OUT_OF_MEMORY, "host allocation for the forward CSR failed");
+  }
+  if (n) {
+    STC_CUDA(cudaMemcpyAsync(out->offsets, off_id, ((size_t)n + 1) * sizeof(uint64_t),
+                             cudaMemcpyDeviceToHost, st));
+    STC_CUDA(cudaMemcpyAsync(out->fdeg, fdeg_id, (size_t)n * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    STC_CUDA(cudaMemcpyAsync(out->rank, g.rank, (size_t)n * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  } else {
+    out->offsets[0] = 0;
+  }
+  if (mu) {
+    STC_CUDA(cudaMemcpyAsync(out->edges, edges, mu * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    STC_CUDA(cudaMemcpyAsync(out->signs, signs, mu, cudaMemcpyDeviceToHost, st));
+  }
+  STC_CUDA(cudaStreamSynchronize(st));
+}
+
+}  // namespace stc

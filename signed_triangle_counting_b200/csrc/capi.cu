@@ -1,0 +1,390 @@
+// C ABI of libstc (include/stc.h): contexts, the whole counting path, CSR
+// export/import, per-source counts and the device RMAT generator.
+#include <cuda_runtime.h>
+
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+#include "stc.h"
+#include "stc_device.cuh"
+#include "stc_gen.h"
+#include "stc_synth.h"
+
+namespace stc {
+
+void fail(stc_status s, const std::string& msg) { throw Error{s, msg}; }
+
+void cuda_check(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return;
+  (void)cudaGetLastError();
+  fail(e == cudaErrorMemoryAllocation ? STC_ERR_OUT_OF_MEMORY : STC_ERR_CUDA,
+       std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+uint64_t* counters(stc_ctx* c) { return buffer<uint64_t>(c, B_COUNTERS, C_SLOTS); }
+
+void mark(stc_ctx* c, int slot) {
+  if (c->timing) STC_CUDA(cudaEventRecord(c->ev[slot], c->stream));
+}
+
+namespace {
+
+// Runs `body` with the context's error handling; every ABI entry uses it.
+template <class F>
+stc_status guarded(stc_ctx* c, F body) {
+  try {
+    if (c) {
+      c->last_error.clear();
+      STC_CUDA(cudaSetDevice(c->device));
+    }
+    body();
+    return STC_OK;
+  } catch (const Error& e) {
+    if (c) c->last_error = e.msg;
+    return e.status;
+  } catch (const std::bad_alloc&) {
+    if (c) c->last_error = "host allocation failed";
+    return STC_ERR_OUT_OF_MEMORY;
+  } catch (...) {
+    if (c) c->last_error = "unexpected internal error";
+    return STC_ERR_INTERNAL;
+  }
+}
+
+void begin_call(stc_ctx* c, const stc_opts* o) {
+  c->stream = (o && o->stream) ? (cudaStream_t)o->stream : c->own_stream;
+  c->timing = o && (o->flags & STC_F_TIMING);
+  c->launches = 0;
+  c->stats = stc_stats{};
+  STC_CUDA(cudaMemsetAsync(counters(c), 0, C_SLOTS * sizeof(uint64_t), c->stream));
+  mark(c, 0);
+}
+
+float elapsed(stc_ctx* c, int a, int b) {
+  float ms = 0.f;
+  STC_CUDA(cudaEventElapsedTime(&ms, c->ev[a], c->ev[b]));
+  return ms;
+}
+
+// Reads the per-type counters and fills the statistics.
+void end_call(stc_ctx* c, const DeviceGraph& g, stc_counts* out) {
+  STC_CUDA(cudaMemcpyAsync(c->h_pinned, counters(c), C_SLOTS * sizeof(uint64_t),
+                           cudaMemcpyDeviceToHost, c->stream));
+  STC_CUDA(cudaStreamSynchronize(c->stream));
+  STC_CUDA(cudaGetLastError());
+  if (c->h_pinned[C_ERROR]) fail(STC_ERR_DEVICE_TIMEOUT, "device reported error word " +
+                                                             std::to_string(c->h_pinned[C_ERROR]));
+  if (out) {
+    out->t0 = c->h_pinned[C_T0];
+    out->t1 = c->h_pinned[C_T1];
+    out->t2 = c->h_pinned[C_T2];
+    out->t3 = c->h_pinned[C_T3];
+  }
+  stc_stats& s = c->stats;
+  s.n = g.n;
+  s.m_input = g.m_input;
+  s.m_unique = g.m_unique;
+  s.m_forward = g.m_fwd;
+  s.alg_bytes = c->h_pinned[C_ALG_BYTES];
+  s.triangles = c->h_pinned[C_T0] + c->h_pinned[C_T1] + c->h_pinned[C_T2] + c->h_pinned[C_T3];
+  s.kernel_launches = (uint32_t)c->launches;
+  if (c->timing) {
+    s.ms_h2d = elapsed(c, 0, 1);
+    s.ms_dedup = elapsed(c, 1, 2);
+    s.ms_orient = elapsed(c, 2, 3);
+    s.ms_csr = elapsed(c, 3, 4);
+    s.ms_count = elapsed(c, 4, 5);
+    s.ms_total = elapsed(c, 0, 5);
+  }
+}
+
+struct DeviceInput {
+  const uint32_t* src;
+  const uint32_t* dst;
+  const int8_t* sign;
+};
+
+DeviceInput stage_input(stc_ctx* c, const uint32_t* src, const uint32_t* dst, const int8_t* sign,
+                        uint64_t m, const stc_opts* o) {
+  if (m && (!src || !dst || !sign)) fail(STC_ERR_INVALID_ARGUMENT, "null edge array");
+  if (o && (o->flags & STC_F_DEVICE_INPUT)) return DeviceInput{src, dst, sign};
+  uint32_t* ds = buffer<uint32_t>(c, B_IN_SRC, m);
+  uint32_t* dd = buffer<uint32_t>(c, B_IN_DST, m);
+  int8_t* dg = buffer<int8_t>(c, B_IN_SIGN, m);
+  if (m) {
+    STC_CUDA(cudaMemcpyAsync(ds, src, m * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
+    STC_CUDA(cudaMemcpyAsync(dd, dst, m * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
+    STC_CUDA(cudaMemcpyAsync(dg, sign, m, cudaMemcpyHostToDevice, c->stream));
+  }
+  return DeviceInput{ds, dd, dg};
+}
+
+CountConfig count_config(const stc_opts* o) {
+  CountConfig cfg;
+  if (o) {
+    if (o->strategy > STC_STRATEGY_SEARCH) fail(STC_ERR_INVALID_ARGUMENT, "unknown strategy");
+    if (o->dispatch > STC_DISPATCH_LEARNED) fail(STC_ERR_INVALID_ARGUMENT, "unknown dispatch");
+    cfg.strategy = o->strategy;
+    cfg.dispatch = o->dispatch;
+  }
+  return cfg;
+}
+
+__global__ void k_synth_rmat(uint64_t seed, stcgen::RmatParams rp, stcgen::Perm perm,
+                             uint64_t pos_thr, uint64_t samples, uint32_t* __restrict__ src,
+                             uint32_t* __restrict__ dst, int8_t* __restrict__ sign) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < samples; i += stride) {
+    uint32_t u, v;
+    stcgen::rmat_sample(seed, i, rp, &u, &v);
+    u = (uint32_t)stcgen::perm_apply(perm, u);
+    v = (uint32_t)stcgen::perm_apply(perm, v);
+    src[i] = u;
+    dst[i] = v;
+    sign[i] = stcgen::edge_sign(seed, u, v, pos_thr);
+  }
+}
+
+}  // namespace
+}  // namespace stc
+
+using namespace stc;
+
+extern "C" {
+
+const char* stc_status_string(stc_status s) {
+  switch (s) {
+    case STC_OK: return "ok";
+    case STC_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case STC_ERR_IO: return "i/o error";
+    case STC_ERR_CUDA: return "CUDA error";
+    case STC_ERR_OUT_OF_MEMORY: return "out of memory";
+    case STC_ERR_LIMIT: return "input beyond supported limits";
+    case STC_ERR_DEVICE_TIMEOUT: return "device-side wait expired";
+    case STC_ERR_NO_DEVICE: return "no usable CUDA device";
+    case STC_ERR_INTERNAL: return "internal error";
+  }
+  return "unknown status";
+}
+
+int stc_abi_version(void) { return STC_ABI_VERSION; }
+
+stc_status stc_ctx_create(int device, stc_ctx** out) {
+  if (!out) return STC_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+    (void)cudaGetLastError();
+    return STC_ERR_NO_DEVICE;
+  }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10) {
+    (void)cudaGetLastError();
+    return STC_ERR_NO_DEVICE;
+  }
+  stc_ctx* c = new (std::nothrow) stc_ctx();
+  if (!c) return STC_ERR_OUT_OF_MEMORY;
+  c->device = device;
+  stc_status s = guarded(c, [&] {
+    STC_CUDA(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
+    c->stream = c->own_stream;
+    STC_CUDA(cudaMallocHost(&c->h_pinned, C_SLOTS * sizeof(uint64_t)));
+    for (auto& e : c->ev) STC_CUDA(cudaEventCreate(&e));
+    (void)counters(c);
+  });
+  if (s != STC_OK) {
+    stc_ctx_destroy(c);
+    return s;
+  }
+  *out = c;
+  return STC_OK;
+}
+
+void stc_ctx_destroy(stc_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->own_stream) cudaStreamSynchronize(c->own_stream);
+  for (auto& b : c->bufs)
+    if (b.p) cudaFree(b.p);
+  for (auto& e : c->ev)
+    if (e) cudaEventDestroy(e);
+  if (c->h_pinned) cudaFreeHost(c->h_pinned);
+  if (c->own_stream) cudaStreamDestroy(c->own_stream);
+  (void)cudaGetLastError();
+  delete c;
+}
+
+const char* stc_ctx_last_error(const stc_ctx* c) { return c ? c->last_error.c_str() : ""; }
+
+stc_status stc_ctx_last_stats(const stc_ctx* c, stc_stats* out) {
+  if (!c || !out) return STC_ERR_INVALID_ARGUMENT;
+  *out = c->stats;
+  return STC_OK;
+}
+
+stc_status stc_ctx_trim(stc_ctx* c) {
+  if (!c) return STC_ERR_INVALID_ARGUMENT;
+  return guarded(c, [&] {
+    STC_CUDA(cudaStreamSynchronize(c->own_stream));
+    for (int i = 0; i < B_COUNT_; i++) {
+      if (i == B_COUNTERS) continue;
+      if (c->bufs[i].p) STC_CUDA(cudaFree(c->bufs[i].p));
+      c->bufs[i] = DevBuf{};
+    }
+  });
+}
+
+stc_status stc_count(stc_ctx* c, const uint32_t* src, const uint32_t* dst, const int8_t* sign,
+                     uint64_t m, const stc_opts* o, stc_counts* out) {
+  if (!c || !out) return STC_ERR_INVALID_ARGUMENT;
+  return guarded(c, [&] {
+    CountConfig cfg = count_config(o);
+    begin_call(c, o);
+    DeviceInput in = stage_input(c, src, dst, sign, m, o);
+    DeviceGraph g;
+    build_graph(c, in.src, in.dst, in.sign, m, g);
+    count_triangles(c, g, cfg);
+    mark(c, 5);
+    end_call(c, g, out);
+  });
+}
+
+stc_status stc_build_forward_csr(stc_ctx* c, const uint32_t* src, const uint32_t* dst,
+                                 const int8_t* sign, uint64_t m, const stc_opts* o,
+                                 stc_forward_csr* out) {
+  if (!c || !out) return STC_ERR_INVALID_ARGUMENT;
+  memset(out, 0, sizeof(*out));
+  return guarded(c, [&] {
+    begin_call(c, o);
+    DeviceInput in = stage_input(c, src, dst, sign, m, o);
+    DeviceGraph g;
+    build_graph(c, in.src, in.dst, in.sign, m, g);
+    export_forward_csr(c, g, out);
+    mark(c, 5);
+    end_call(c, g, nullptr);
+  });
+}
+
+void stc_free_forward_csr(stc_forward_csr* csr) {
+  if (!csr) return;
+  free(csr->offsets);
+  free(csr->edges);
+  free(csr->signs);
+  free(csr->fdeg);
+  free(csr->rank);
+  memset(csr, 0, sizeof(*csr));
+}
+
+stc_status stc_count_forward_csr(stc_ctx* c, const stc_forward_csr* csr, const stc_opts* o,
+                                 stc_counts* out) {
+  if (!c || !csr || !out) return STC_ERR_INVALID_ARGUMENT;
+  return guarded(c, [&] {
+    const uint32_t n = csr->n;
+    const uint64_t m = csr->m;
+    if (!csr->offsets || (n && !csr->rank) || (m && (!csr->edges || !csr->signs)))
+      fail(STC_ERR_INVALID_ARGUMENT, "null CSR array");
+    if (csr->offsets[0] != 0 || csr->offsets[n] != m)
+      fail(STC_ERR_INVALID_ARGUMENT, "offsets[0] must be 0 and offsets[n] must equal m");
+    for (uint32_t v = 0; v < n; v++)
+      if (csr->offsets[v + 1] < csr->offsets[v])
+        fail(STC_ERR_INVALID_ARGUMENT, "offsets are not monotone");
+    {
+      std::vector<uint8_t> seen(n, 0);
+      for (uint32_t v = 0; v < n; v++) {
+        if (csr->rank[v] >= n || seen[csr->rank[v]])
+          fail(STC_ERR_INVALID_ARGUMENT, "rank is not a permutation of [0, n)");
+        seen[csr->rank[v]] = 1;
+      }
+    }
+    CountConfig cfg = count_config(o);
+    begin_call(c, o);
+    uint64_t* d_off = buffer<uint64_t>(c, B_EXPORT_OFF, (size_t)n + 1);
+    uint32_t* d_edges = buffer<uint32_t>(c, B_IN_SRC, m);
+    int8_t* d_signs = buffer<int8_t>(c, B_IN_SIGN, m);
+    uint32_t* d_rank = buffer<uint32_t>(c, B_IN_DST, n);
+    STC_CUDA(cudaMemcpyAsync(d_off, csr->offsets, ((size_t)n + 1) * sizeof(uint64_t),
+                             cudaMemcpyHostToDevice, c->stream));
+    if (m) {
+      STC_CUDA(cudaMemcpyAsync(d_edges, csr->edges, m * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                               c->stream));
+      STC_CUDA(cudaMemcpyAsync(d_signs, csr->signs, m, cudaMemcpyHostToDevice, c->stream));
+    }
+    if (n)
+      STC_CUDA(cudaMemcpyAsync(d_rank, csr->rank, (size_t)n * sizeof(uint32_t),
+                               cudaMemcpyHostToDevice, c->stream));
+    DeviceGraph g;
+    graph_from_forward_csr(c, n, m, d_off, d_edges, d_signs, d_rank, g);
+    count_triangles(c, g, cfg);
+    mark(c, 5);
+    end_call(c, g, out);
+  });
+}
+
+stc_status stc_vertex_counts(stc_ctx* c, const uint32_t* src, const uint32_t* dst,
+                             const int8_t* sign, uint64_t m, const stc_opts* o, uint64_t* counts,
+                             uint64_t counts_len, uint32_t* n_out) {
+  if (!c || !n_out) return STC_ERR_INVALID_ARGUMENT;
+  return guarded(c, [&] {
+    CountConfig cfg = count_config(o);
+    begin_call(c, o);
+    DeviceInput in = stage_input(c, src, dst, sign, m, o);
+    DeviceGraph g;
+    build_graph(c, in.src, in.dst, in.sign, m, g);
+    *n_out = g.n;
+    if (!counts || counts_len < 4ull * g.n)
+      fail(STC_ERR_INVALID_ARGUMENT, "counts must hold 4 * n = " + std::to_string(4ull * g.n) +
+                                         " words");
+    uint64_t* dv = buffer<uint64_t>(c, B_VCOUNTS, 4ull * g.n);
+    if (g.n) STC_CUDA(cudaMemsetAsync(dv, 0, 4ull * g.n * sizeof(uint64_t), c->stream));
+    cfg.vertex_counts = dv;
+    count_triangles(c, g, cfg);
+    mark(c, 5);
+    if (g.n)
+      STC_CUDA(cudaMemcpyAsync(counts, dv, 4ull * g.n * sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                               c->stream));
+    end_call(c, g, nullptr);
+  });
+}
+
+stc_status stc_count_batch(stc_ctx* c, const stc_graph* graphs, uint32_t G, const stc_opts* o,
+                           stc_counts* outs) {
+  if (!c || (G && (!graphs || !outs))) return STC_ERR_INVALID_ARGUMENT;
+  // Graph-at-a-time fallback path; the persistent batched engine replaces it.
+  for (uint32_t i = 0; i < G; i++) {
+    stc_status s = stc_count(c, graphs[i].src, graphs[i].dst, graphs[i].sign, graphs[i].m, o, &outs[i]);
+    if (s != STC_OK) return s;
+  }
+  return STC_OK;
+}
+
+stc_status stc_synth_rmat_device(stc_ctx* c, uint64_t seed, uint32_t scale, uint64_t n,
+                                 uint64_t samples, double a, double b, double cc, double p_pos,
+                                 uint32_t* d_src, uint32_t* d_dst, int8_t* d_sign) {
+  if (!c || !d_src || !d_dst || !d_sign) return STC_ERR_INVALID_ARGUMENT;
+  if (scale == 0 || scale > 31 || n < 2 || n > (1ull << scale)) return STC_ERR_INVALID_ARGUMENT;
+  return guarded(c, [&] {
+    auto thr32 = [](double p) -> uint32_t {
+      if (!(p > 0.0)) return 0;
+      if (p >= 1.0) return UINT32_MAX;
+      return (uint32_t)ldexp(p, 32);
+    };
+    stcgen::RmatParams rp;
+    rp.scale = scale;
+    rp.n = n;
+    rp.t_a = thr32(a);
+    rp.t_ab = thr32(a + b);
+    rp.t_abc = thr32(a + b + cc);
+    uint64_t thr = !(p_pos > 0.0) ? 0 : p_pos >= 1.0 ? UINT64_MAX : (uint64_t)ldexp(p_pos, 64);
+    stcgen::Perm perm = stcgen::make_perm(seed, n);
+    k_synth_rmat<<<kSMs * 16, 256, 0, c->own_stream>>>(seed, rp, perm, thr, samples, d_src, d_dst,
+                                                       d_sign);
+    STC_CUDA(cudaGetLastError());
+    STC_CUDA(cudaStreamSynchronize(c->own_stream));
+  });
+}
+
+}  // extern "C"

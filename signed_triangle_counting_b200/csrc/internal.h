@@ -1,0 +1,145 @@
+// Host-side internals of libstc: the context, device buffers and the stages
+// of the counting path.  Nothing here crosses the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "stc.h"
+
+namespace stc {
+
+// Internal error carrying an ABI status; caught at every extern "C" entry.
+struct Error {
+  stc_status status;
+  std::string msg;
+};
+
+[[noreturn]] void fail(stc_status s, const std::string& msg);
+void cuda_check(cudaError_t e, const char* what);
+#define STC_CUDA(call) ::stc::cuda_check((call), #call)
+
+// Named device allocations cached on a context and grown on demand.
+enum BufId {
+  B_IN_SRC, B_IN_DST, B_IN_SIGN,  // staged host input
+  B_KEYS_A, B_KEYS_B,             // sort double buffer
+  B_UKEYS,                        // unique undirected keys
+  B_DEG, B_RANK, B_VERTS, B_FDEG,
+  B_VKEYS_A, B_VKEYS_B,
+  B_OFF, B_NBR, B_SGN, B_ASRC,
+  B_SORT_COUNTS, B_SCAN_SUMS,
+  B_COUNTERS,                     // per-type counters, totals, flags
+  B_WORK,                         // work queues / strategy worklists
+  B_WORK2,
+  B_EXPORT_OFF, B_EXPORT_FDEG,
+  B_VCOUNTS,
+  B_BATCH_META,
+  B_COUNT_
+};
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+};
+
+// Device counters block (B_COUNTERS), 64-bit words.
+enum CounterSlot {
+  C_T0 = 0, C_T1, C_T2, C_T3,  // per-type triangle counts
+  C_MAX_ID = 4,                // max kept id (u32 in the low word)
+  C_SELF = 5,                  // self-loop count
+  C_MAX_DEG = 6,
+  C_ALG_BYTES = 7,
+  C_WORK = 8,                  // dynamic work counters (8 slots)
+  C_ERROR = 16,                // device error word (0 = ok)
+  C_SLOTS = 32
+};
+
+}  // namespace stc
+
+struct stc_ctx {
+  int device = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  stc::DevBuf bufs[stc::B_COUNT_];
+  uint64_t* h_pinned = nullptr;  // C_SLOTS words of pinned host memory
+  std::string last_error;
+  stc_stats stats{};
+  cudaEvent_t ev[8] = {};
+  bool timing = false;
+  int launches = 0;
+};
+
+namespace stc {
+
+template <class T>
+T* buffer(stc_ctx* c, BufId id, size_t count) {
+  DevBuf& b = c->bufs[id];
+  size_t bytes = count * sizeof(T);
+  if (bytes == 0) bytes = 16;
+  if (b.cap < bytes) {
+    if (b.p) STC_CUDA(cudaFree(b.p));
+    b.p = nullptr;
+    b.cap = 0;
+    size_t want = bytes + bytes / 8;  // headroom for slightly larger reuse
+    cudaError_t e = cudaMalloc(&b.p, want);
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      e = cudaMalloc(&b.p, bytes);
+      want = bytes;
+    }
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      b.p = nullptr;
+      fail(STC_ERR_OUT_OF_MEMORY, "device allocation of " + std::to_string(bytes) + " bytes failed");
+    }
+    b.cap = want;
+  }
+  return static_cast<T*>(b.p);
+}
+
+// The graph built on the device, in rank space: vertex r is the r-th vertex
+// of (degree, id) order, and every arc goes from lower to higher rank.
+struct DeviceGraph {
+  uint32_t n = 0;        // max kept id + 1
+  uint32_t bits = 1;     // bits per id inside a 64-bit key
+  uint64_t m_input = 0;
+  uint64_t m_valid = 0;  // without self-loops
+  uint64_t m_unique = 0;
+  uint64_t m_fwd = 0;
+  uint32_t max_deg = 0;
+  uint64_t* ukeys = nullptr;  // sorted unique keys: min << bits | max, sign in bit 63
+  uint32_t* deg = nullptr;    // undirected degree, by id
+  uint32_t* rank = nullptr;   // id -> rank
+  uint32_t* verts = nullptr;  // rank -> id
+  uint64_t* off = nullptr;    // n + 1, rank space
+  uint32_t* nbr = nullptr;    // arcs: head vertex (rank), sorted within each list
+  int8_t* sgn = nullptr;      // arcs: +1 / -1
+  uint32_t* fdeg = nullptr;   // out-degree by rank
+};
+
+// Stage timing helper: records an event when the context is timing.
+void mark(stc_ctx* c, int slot);
+
+// Graph build: input device arrays -> DeviceGraph (all fields).
+void build_graph(stc_ctx* c, const uint32_t* d_src, const uint32_t* d_dst, const int8_t* d_sign,
+                 uint64_t m, DeviceGraph& g);
+// Rank-space CSR from a reference-layout forward CSR already on the device.
+void graph_from_forward_csr(stc_ctx* c, uint32_t n, uint64_t m, const uint64_t* d_off,
+                            const uint32_t* d_edges, const int8_t* d_signs, const uint32_t* d_rank,
+                            DeviceGraph& g);
+// Forward CSR in the reference's id-space layout, copied to host arrays.
+void export_forward_csr(stc_ctx* c, const DeviceGraph& g, stc_forward_csr* out);
+
+// Intersection engine: adds per-type counts into the C_T0..C_T3 slots.
+struct CountConfig {
+  uint32_t strategy = STC_STRATEGY_AUTO;
+  uint32_t dispatch = STC_DISPATCH_FIXED;
+  uint64_t* vertex_counts = nullptr;  // optional per-source counts (rank space, 4 per vertex)
+};
+void count_triangles(stc_ctx* c, const DeviceGraph& g, const CountConfig& cfg);
+
+uint64_t* counters(stc_ctx* c);
+
+}  // namespace stc

@@ -1,0 +1,261 @@
+// Stable LSD radix sort of 64-bit keys over a bit window [lo, hi), plus the
+// range-partitioned scans the graph build uses.
+//
+// Design (B200): every pass is a reduce-then-scan over a fixed grid of
+// CTA-contiguous key ranges (4 CTAs per SM), so no kernel ever waits on
+// another CTA:
+//   upsweep   per-CTA digit histogram of its range      (reads 8 B/key)
+//   scan      one CTA turns [digit][cta] counts into offsets
+//   downsweep per 4096-key tile: warp-striped match.any ranking (stable),
+//             tile-local reorder through shared memory, coalesced scatter
+//             (reads 8 B/key, writes 8 B/key).
+// Bits of the key outside [lo, hi) ride along untouched, which is how the
+// edge sign travels in bit 63 without a separate payload array.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "stc_device.cuh"
+
+namespace stc {
+
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys
+constexpr int kRadix = 256;
+constexpr int kMaxSortGrid = kSMs * 4;
+
+struct RangePartition {
+  uint32_t grid;     // CTAs
+  uint64_t per_cta;  // keys per CTA, a multiple of the tile
+};
+
+inline RangePartition range_partition(uint64_t m, uint64_t tile, uint32_t max_grid) {
+  uint64_t tiles = (m + tile - 1) / tile;
+  if (tiles == 0) tiles = 1;
+  uint64_t grid = tiles < max_grid ? tiles : max_grid;
+  uint64_t per = (tiles + grid - 1) / grid;
+  grid = (tiles + per - 1) / per;
+  return RangePartition{(uint32_t)grid, per * tile};
+}
+
+__global__ void __launch_bounds__(kSortThreads) k_radix_upsweep(
+    const uint64_t* __restrict__ keys, uint64_t m, uint64_t per_cta, int shift,
+    uint32_t dmask, uint32_t* __restrict__ counts, uint32_t grid) {
+  __shared__ uint32_t hist[kSortWarps][kRadix + 1];
+  const unsigned tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
+  for (unsigned i = tid; i < kSortWarps * (kRadix + 1); i += kSortThreads) (&hist[0][0])[i] = 0;
+  __syncthreads();
+  const uint64_t begin = (uint64_t)blockIdx.x * per_cta;
+  const uint64_t end = begin + per_cta < m ? begin + per_cta : m;
+  for (uint64_t base = begin + warp * 32; base < end; base += kSortThreads) {
+    const uint64_t i = base + lane;
+    const uint32_t d = i < end ? (uint32_t)(__ldcs(keys + i) >> shift) & dmask : kRadix;
+    const unsigned peers = __match_any_sync(kFull, d);
+    if ((peers & lanemask_lt()) == 0) hist[warp][d] += __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+  for (unsigned d = tid; d < kRadix; d += kSortThreads) {
+    uint32_t s = 0;
+#pragma unroll
+    for (int w = 0; w < kSortWarps; w++) s += hist[w][d];
+    counts[(uint64_t)d * grid + blockIdx.x] = s;
+  }
+}
+
+// Exclusive scan of `n` 32-bit counts in place by one CTA of 1024 threads.
+__global__ void __launch_bounds__(1024) k_scan_counts(uint32_t* __restrict__ a, uint32_t n) {
+  __shared__ uint32_t tmp[33];
+  const uint32_t per = (n + 1023) / 1024;
+  const uint32_t b = threadIdx.x * per, e = b + per < n ? b + per : n;
+  uint32_t s = 0;
+  for (uint32_t i = b; i < e; i++) s += a[i];
+  uint32_t total;
+  uint32_t run = block_exclusive_scan<1024>(s, tmp, total);
+  for (uint32_t i = b; i < e; i++) {
+    uint32_t x = a[i];
+    a[i] = run;
+    run += x;
+  }
+}
+
+__global__ void __launch_bounds__(kSortThreads, 2) k_radix_downsweep(
+    const uint64_t* __restrict__ in, uint64_t* __restrict__ out, uint64_t m, uint64_t per_cta,
+    int shift, uint32_t dmask, const uint32_t* __restrict__ offsets, uint32_t grid) {
+  __shared__ uint64_t sbuf[kSortTile];
+  __shared__ uint16_t whist[kSortWarps][kRadix + 1];
+  __shared__ uint32_t tile_start[kRadix];
+  __shared__ uint32_t gofs[kRadix];
+  __shared__ uint32_t scan_tmp[kSortWarps + 1];
+  const unsigned tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
+  const uint64_t begin = (uint64_t)blockIdx.x * per_cta;
+  const uint64_t end = begin + per_cta < m ? begin + per_cta : m;
+  for (unsigned d = tid; d < kRadix; d += kSortThreads) gofs[d] = offsets[(uint64_t)d * grid + blockIdx.x];
+  const unsigned lt = lanemask_lt();
+  for (uint64_t tile = begin; tile < end; tile += kSortTile) {
+    for (unsigned i = tid; i < kSortWarps * (kRadix + 1); i += kSortThreads) (&whist[0][0])[i] = 0;
+    __syncthreads();
+    uint64_t k[kSortItems];
+    uint32_t dg[kSortItems];
+    uint32_t r[kSortItems];
+    const uint64_t wbase = tile + (uint64_t)warp * (32 * kSortItems) + lane;
+#pragma unroll
+    for (int j = 0; j < kSortItems; j++) {
+      const uint64_t idx = wbase + (uint64_t)j * 32;
+      k[j] = idx < end ? __ldcs(in + idx) : 0;
+      dg[j] = idx < end ? (uint32_t)(k[j] >> shift) & dmask : kRadix;
+    }
+#pragma unroll
+    for (int j = 0; j < kSortItems; j++) {
+      const unsigned peers = __match_any_sync(kFull, dg[j]);
+      const uint32_t base = whist[warp][dg[j]];
+      const uint32_t below = __popc(peers & lt);
+      __syncwarp();
+      if (below == 0 && dg[j] != kRadix) whist[warp][dg[j]] = (uint16_t)(base + __popc(peers));
+      __syncwarp();
+      r[j] = base + below;
+    }
+    __syncthreads();
+    uint32_t cnt = 0;
+    {
+      const unsigned d = tid;  // kSortThreads == kRadix
+#pragma unroll
+      for (int w = 0; w < kSortWarps; w++) {
+        const uint32_t c = whist[w][d];
+        whist[w][d] = (uint16_t)cnt;
+        cnt += c;
+      }
+    }
+    uint32_t total;
+    const uint32_t st = block_exclusive_scan<kSortThreads>(cnt, scan_tmp, total);
+    tile_start[tid] = st;
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kSortItems; j++) {
+      if (dg[j] != kRadix) sbuf[tile_start[dg[j]] + whist[warp][dg[j]] + r[j]] = k[j];
+    }
+    __syncthreads();
+    const uint32_t valid = (uint32_t)(end - tile < (uint64_t)kSortTile ? end - tile : kSortTile);
+    for (uint32_t i = tid; i < valid; i += kSortThreads) {
+      const uint64_t key = sbuf[i];
+      const uint32_t d = (uint32_t)(key >> shift) & dmask;
+      out[(uint64_t)gofs[d] + (i - tile_start[d])] = key;
+    }
+    __syncthreads();
+    gofs[tid] += cnt;
+    __syncthreads();
+  }
+}
+
+// Scratch for radix_sort: `counts` holds kRadix * kMaxSortGrid words.
+// Sorts keys[0, m) by bits [lo, hi) stably; returns the buffer that holds the
+// result (`keys` or `alt`).  m must be below 2^32.
+inline uint64_t* radix_sort(uint64_t* keys, uint64_t* alt, uint64_t m, int lo, int hi,
+                            uint32_t* counts, cudaStream_t st, int* launches = nullptr) {
+  if (m <= 1 || hi <= lo) return keys;
+  RangePartition p = range_partition(m, kSortTile, kMaxSortGrid);
+  uint64_t* src = keys;
+  uint64_t* dst = alt;
+  for (int shift = lo; shift < hi; shift += 8) {
+    const int w = hi - shift < 8 ? hi - shift : 8;
+    const uint32_t dmask = (1u << w) - 1;
+    k_radix_upsweep<<<p.grid, kSortThreads, 0, st>>>(src, m, p.per_cta, shift, dmask, counts, p.grid);
+    k_scan_counts<<<1, 1024, 0, st>>>(counts, kRadix * p.grid);
+    k_radix_downsweep<<<p.grid, kSortThreads, 0, st>>>(src, dst, m, p.per_cta, shift, dmask, counts,
+                                                       p.grid);
+    if (launches) *launches += 3;
+    uint64_t* t = src;
+    src = dst;
+    dst = t;
+  }
+  return src;
+}
+
+// ------------------------------------------------------- range scans ----
+// Exclusive scan of 32-bit values produced by functor F (F(i) for i < n)
+// into 64-bit outputs; `emit(i, prefix, value)` receives each element's
+// exclusive prefix.  Three launches, no inter-CTA waiting:
+//   k_range_reduce -> k_scan_small -> k_range_apply.
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+template <class F>
+__global__ void __launch_bounds__(kScanThreads) k_range_reduce(F f, uint64_t n, uint64_t per_cta,
+                                                               uint64_t* __restrict__ sums) {
+  __shared__ uint64_t tmp[kScanThreads / 32 + 1];
+  const uint64_t begin = (uint64_t)blockIdx.x * per_cta;
+  const uint64_t end = begin + per_cta < n ? begin + per_cta : n;
+  uint64_t s = 0;
+  for (uint64_t i = begin + threadIdx.x; i < end; i += kScanThreads) s += f(i);
+  s = warp_sum(s);
+  if (lane_id() == 0) tmp[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint64_t t = 0;
+    for (int w = 0; w < kScanThreads / 32; w++) t += tmp[w];
+    sums[blockIdx.x] = t;
+  }
+}
+
+// Exclusive scan of a[0, n) in place; a[n] receives the total.
+__global__ void __launch_bounds__(1024) k_scan_small(uint64_t* __restrict__ a, uint32_t n) {
+  __shared__ uint64_t tmp[33];
+  const uint32_t per = (n + 1023) / 1024;
+  const uint32_t b = threadIdx.x * per, e = b + per < n ? b + per : n;
+  uint64_t s = 0;
+  for (uint32_t i = b; i < e; i++) s += a[i];
+  uint64_t total;
+  uint64_t run = block_exclusive_scan<1024>(s, tmp, total);
+  for (uint32_t i = b; i < e; i++) {
+    uint64_t x = a[i];
+    a[i] = run;
+    run += x;
+  }
+  if (threadIdx.x == 0) a[n] = total;
+}
+
+template <class F, class E>
+__global__ void __launch_bounds__(kScanThreads) k_range_apply(F f, E emit, uint64_t n,
+                                                              uint64_t per_cta,
+                                                              const uint64_t* __restrict__ offs) {
+  __shared__ uint64_t tmp[kScanThreads / 32 + 1];
+  const uint64_t begin = (uint64_t)blockIdx.x * per_cta;
+  const uint64_t end = begin + per_cta < n ? begin + per_cta : n;
+  uint64_t carry = offs[blockIdx.x];
+  for (uint64_t tile = begin; tile < end; tile += kScanTile) {
+    // Blocked arrangement: thread t owns kScanItems consecutive elements.
+    const uint64_t b = tile + (uint64_t)threadIdx.x * kScanItems;
+    uint32_t v[kScanItems];
+    uint64_t s = 0;
+#pragma unroll
+    for (int j = 0; j < kScanItems; j++) {
+      v[j] = (b + j < end) ? f(b + j) : 0u;
+      s += v[j];
+    }
+    uint64_t total;
+    uint64_t run = carry + block_exclusive_scan<kScanThreads>(s, tmp, total);
+#pragma unroll
+    for (int j = 0; j < kScanItems; j++) {
+      if (b + j < end) emit(b + j, run, v[j]);
+      run += v[j];
+    }
+    carry += total;
+  }
+}
+
+// Runs the three-launch scan; `sums` needs kMaxSortGrid + 1 words.  Returns
+// the grand total through `*d_total` (device) when non-null.
+template <class F, class E>
+inline void range_scan(F f, E emit, uint64_t n, uint64_t* sums, cudaStream_t st,
+                       int* launches = nullptr) {
+  RangePartition p = range_partition(n, kScanTile, kMaxSortGrid);
+  k_range_reduce<<<p.grid, kScanThreads, 0, st>>>(f, n, p.per_cta, sums);
+  k_scan_small<<<1, 1024, 0, st>>>(sums, p.grid);
+  k_range_apply<<<p.grid, kScanThreads, 0, st>>>(f, emit, n, p.per_cta, sums);
+  if (launches) *launches += 3;
+}
+
+}  // namespace stc

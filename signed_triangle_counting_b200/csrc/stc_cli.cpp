@@ -1,0 +1,146 @@
+// stc — command-line drop-in for the reference programs
+// (MC/tc_serial.cpp:172-210, MC/tc_merge_sign_enu.cpp:46-154,
+// MC/tc_hash_sign_enu.cpp:76-177).
+//
+//   stc [--strategy auto|merge|hash|search] [--dispatch fixed|learned]
+//       [--device N] [--json] <graph_file>
+//
+// Prints the union of the reference outputs: tc_serial's stage lines,
+// `n=.. raw_edges=..`, `forward_edges=..` and per-type block, then the
+// Balanced / Unbalanced / Total lines of the merge and hash programs, then the
+// total time.  Exit status 1 on a usage or I/O error, as in the reference.
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+
+#include "stc.h"
+
+namespace {
+
+struct Clock {
+  std::chrono::high_resolution_clock::time_point t0 = std::chrono::high_resolution_clock::now();
+  double sec() const {
+    return std::chrono::duration<double>(std::chrono::high_resolution_clock::now() - t0).count();
+  }
+};
+
+// Stage line in the reference format (MC/timer.h:24-26).
+void stage(const char* label, double seconds) { std::printf("[%s] took %.4f seconds\n", label, seconds); }
+
+int usage(const char* prog) {
+  std::fprintf(stderr,
+               "usage: %s [--strategy auto|merge|hash|search] [--dispatch fixed|learned] "
+               "[--device N] [--json] <graph_file>\n",
+               prog);
+  return 1;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  const char* path = nullptr;
+  stc_opts opts{};
+  opts.flags = STC_F_TIMING;
+  int device = 0;
+  bool json = false;
+  for (int i = 1; i < argc; i++) {
+    std::string a = argv[i];
+    if (a == "--strategy" && i + 1 < argc) {
+      std::string v = argv[++i];
+      if (v == "auto") opts.strategy = STC_STRATEGY_AUTO;
+      else if (v == "merge") opts.strategy = STC_STRATEGY_MERGE;
+      else if (v == "hash") opts.strategy = STC_STRATEGY_HASH;
+      else if (v == "search") opts.strategy = STC_STRATEGY_SEARCH;
+      else return usage(argv[0]);
+    } else if (a == "--dispatch" && i + 1 < argc) {
+      std::string v = argv[++i];
+      if (v == "fixed") opts.dispatch = STC_DISPATCH_FIXED;
+      else if (v == "learned") opts.dispatch = STC_DISPATCH_LEARNED;
+      else return usage(argv[0]);
+    } else if (a == "--device" && i + 1 < argc) {
+      device = std::atoi(argv[++i]);
+    } else if (a == "--json") {
+      json = true;
+    } else if (a == "-h" || a == "--help") {
+      return usage(argv[0]);
+    } else if (!path && (a.empty() || a[0] != '-')) {
+      path = argv[i];
+    } else {
+      return usage(argv[0]);
+    }
+  }
+  if (!path) return usage(argv[0]);
+
+  Clock total;
+  stc_edge_list el;
+  Clock io;
+  stc_status s = stc_load_edge_list(path, &el);
+  if (s == STC_ERR_IO) {
+    std::perror(path);
+    return 1;
+  }
+  if (s != STC_OK) {
+    std::fprintf(stderr, "%s: %s\n", path, stc_status_string(s));
+    return 1;
+  }
+  stage("Graph Load (I/O + parse)", io.sec());
+  std::printf("  n=%u  raw_edges=%llu\n", el.n, (unsigned long long)el.lines);
+
+  stc_ctx* ctx = nullptr;
+  s = stc_ctx_create(device, &ctx);
+  if (s != STC_OK) {
+    std::fprintf(stderr, "stc: cannot open CUDA device %d: %s\n", device, stc_status_string(s));
+    stc_free_edge_list(&el);
+    return 1;
+  }
+  stc_counts c{};
+  Clock run;
+  s = stc_count(ctx, el.src, el.dst, el.sign, el.m, &opts, &c);
+  const double run_s = run.sec();
+  stc_free_edge_list(&el);
+  if (s != STC_OK) {
+    std::fprintf(stderr, "stc: %s: %s\n", stc_status_string(s), stc_ctx_last_error(ctx));
+    stc_ctx_destroy(ctx);
+    return 1;
+  }
+  stc_stats st{};
+  stc_ctx_last_stats(ctx, &st);
+  stc_ctx_destroy(ctx);
+
+  stage("Build Forward CSR", (st.ms_h2d + st.ms_dedup + st.ms_orient) / 1e3);
+  stage("Algorithm-Specific Preprocessing (Adjacency List Sort)", st.ms_csr / 1e3);
+  std::printf("  forward_edges=%llu\n", (unsigned long long)st.m_forward);
+  stage("Triangle Counting Execution", st.ms_count / 1e3);
+
+  std::printf("\nTriangle counts\n");
+  std::printf("  T3 (+++ balanced)   : %llu\n", (unsigned long long)c.t3);
+  std::printf("  T1 (+-- balanced)   : %llu\n", (unsigned long long)c.t1);
+  std::printf("  T2 (++- unbalanced) : %llu\n", (unsigned long long)c.t2);
+  std::printf("  T0 (--- unbalanced) : %llu\n", (unsigned long long)c.t0);
+  std::printf("  --------------------------------\n");
+  std::printf("  balanced total      : %llu\n", (unsigned long long)stc_balanced(&c));
+  std::printf("  unbalanced total    : %llu\n", (unsigned long long)stc_unbalanced(&c));
+  std::printf("  grand total         : %llu\n", (unsigned long long)stc_total(&c));
+  std::printf("Balanced   = %llu\n", (unsigned long long)stc_balanced(&c));
+  std::printf("Unbalanced = %llu\n", (unsigned long long)stc_unbalanced(&c));
+  std::printf("Total      = %llu\n", (unsigned long long)stc_total(&c));
+  stage("Total execution time", total.sec());
+  if (json) {
+    const double count_s = st.ms_count / 1e3;
+    std::printf(
+        "{\"n\": %llu, \"m_unique\": %llu, \"forward_edges\": %llu, \"t0\": %llu, \"t1\": %llu, "
+        "\"t2\": %llu, \"t3\": %llu, \"balanced\": %llu, \"unbalanced\": %llu, "
+        "\"ms_dedup\": %.4f, \"ms_orient\": %.4f, \"ms_csr\": %.4f, \"ms_count\": %.4f, "
+        "\"ms_device_total\": %.4f, \"wall_s\": %.4f, \"alg_bytes\": %llu, "
+        "\"edges_per_s_count\": %.6g}\n",
+        (unsigned long long)st.n, (unsigned long long)st.m_unique, (unsigned long long)st.m_forward,
+        (unsigned long long)c.t0, (unsigned long long)c.t1, (unsigned long long)c.t2,
+        (unsigned long long)c.t3, (unsigned long long)stc_balanced(&c),
+        (unsigned long long)stc_unbalanced(&c), st.ms_dedup, st.ms_orient, st.ms_csr, st.ms_count,
+        st.ms_total, run_s, (unsigned long long)st.alg_bytes,
+        count_s > 0 ? st.m_unique / count_s : 0.0);
+  }
+  return 0;
+}
