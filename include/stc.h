@@ -19,7 +19,7 @@
  *    lower to the higher vertex of that order (MC/graph_io.h:261-330);
  *  - a triangle's type is its number of negative edges: 0 -> T3 (+++),
  *    1 -> T2 (++-), 2 -> T1 (+--), 3 -> T0 (---) (MC/tc_serial.cpp:95-112).
- * Vertex ids must be below 2^31 and an edge list below 2^32 elements.
+ * Vertex ids must be below 2^31 - 1 and an edge list below 2^32 elements.
  */
 #ifndef STC_H
 #define STC_H
@@ -39,7 +39,7 @@ typedef enum stc_status {
   STC_ERR_IO = 2,               /* file cannot be opened / read (MC/graph_io.h:40-59) */
   STC_ERR_CUDA = 3,             /* a CUDA call failed; see stc_ctx_last_error */
   STC_ERR_OUT_OF_MEMORY = 4,    /* host or device allocation failed */
-  STC_ERR_LIMIT = 5,            /* id >= 2^31 or list >= 2^32 elements */
+  STC_ERR_LIMIT = 5,            /* id >= 2^31 - 1 or list >= 2^32 elements */
   STC_ERR_DEVICE_TIMEOUT = 6,   /* a bounded device-side wait expired */
   STC_ERR_NO_DEVICE = 7,        /* no CUDA device, or not an sm_100 part */
   STC_ERR_INTERNAL = 8          /* a self-check failed (e.g. strategies disagree) */

@@ -239,8 +239,8 @@ void finish_csr_from_arc_keys(stc_ctx* c, DeviceGraph& g, uint64_t* akeys, uint6
   range_scan(LoadU32{g.fdeg}, EmitOffset{g.off}, g.n, sums, c->stream, &c->launches);
   STC_CUDA(cudaMemcpyAsync(g.off + g.n, sums + range_partition(g.n, kScanTile, kMaxSortGrid).grid,
                            sizeof(uint64_t), cudaMemcpyDeviceToDevice, c->stream));
-  g.nbr = buffer<uint32_t>(c, B_NBR, g.m_fwd);
-  g.sgn = buffer<int8_t>(c, B_SGN, g.m_fwd);
+  g.nbr = buffer<uint32_t>(c, B_NBR, g.m_fwd + 4);  // + 4: the engine reads whole int4 chunks
+  g.sgn = buffer<int8_t>(c, B_SGN, g.m_fwd + 4);
   k_csr_fill<<<grid_for(g.m_fwd, 4), kThreads, 0, c->stream>>>(sorted, g.m_fwd, g.bits, g.fdeg,
                                                                g.nbr, g.sgn, (unsigned long long*)counters(c));
   c->launches += 1;
@@ -266,7 +266,9 @@ void build_graph(stc_ctx* c, const uint32_t* d_src, const uint32_t* d_dst, const
   read_counters(c, C_MAX_ID, 2);
   const uint64_t max_id = c->h_pinned[C_MAX_ID];
   const uint64_t self = c->h_pinned[C_SELF];
-  if (max_id >= (1ull << 31)) fail(STC_ERR_LIMIT, "vertex id " + std::to_string(max_id) + " >= 2^31");
+  // Ids (and ranks) stay below 2^31 - 1: the engine keeps a sign in bit 31.
+  if (max_id >= (1ull << 31) - 1)
+    fail(STC_ERR_LIMIT, "vertex id " + std::to_string(max_id) + " >= 2^31 - 1");
   g.n = m ? (uint32_t)max_id + 1 : 0;
   g.m_valid = m - self;
   g.bits = std::max<uint32_t>(1, bit_width64(max_id));
@@ -344,7 +346,7 @@ void graph_from_forward_csr(stc_ctx* c, uint32_t n, uint64_t m, const uint64_t* 
   g.n = n;
   g.m_input = g.m_valid = g.m_unique = g.m_fwd = m;
   if (m >= (1ull << 32)) fail(STC_ERR_LIMIT, "forward CSR has 2^32 or more edges");
-  if (n >= (1u << 31)) fail(STC_ERR_LIMIT, "forward CSR has 2^31 or more vertices");
+  if (n >= (1u << 31) - 1) fail(STC_ERR_LIMIT, "forward CSR has 2^31 - 1 or more vertices");
   g.bits = std::max<uint32_t>(1, bit_width64(n ? n - 1 : 0));
   g.rank = const_cast<uint32_t*>(d_rank);
   g.fdeg = buffer<uint32_t>(c, B_FDEG, n);

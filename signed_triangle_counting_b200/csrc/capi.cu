@@ -76,8 +76,11 @@ void end_call(stc_ctx* c, const DeviceGraph& g, stc_counts* out) {
                            cudaMemcpyDeviceToHost, c->stream));
   STC_CUDA(cudaStreamSynchronize(c->stream));
   STC_CUDA(cudaGetLastError());
-  if (c->h_pinned[C_ERROR]) fail(STC_ERR_DEVICE_TIMEOUT, "device reported error word " +
-                                                             std::to_string(c->h_pinned[C_ERROR]));
+  if (c->h_pinned[C_ERROR]) {
+    const uint64_t e = c->h_pinned[C_ERROR];
+    fail(e == kDeviceErrTimeout ? STC_ERR_DEVICE_TIMEOUT : STC_ERR_INTERNAL,
+         "device reported error word " + std::to_string(e));
+  }
   if (out) {
     out->t0 = c->h_pinned[C_T0];
     out->t1 = c->h_pinned[C_T1];

@@ -9,24 +9,31 @@
 // higher rank than its tail, so for the arc u -> v stored at position k of
 // N+(u), the third vertex w of a triangle lies in the suffix
 // A' = N+(u)[k+1 ..] and in B = N+(v); the reference's rank filter
-// (tc_serial.cpp:126) is implied, and B is only scanned up to max(A').
+// (tc_serial.cpp:126) is implied.
 //
 // Work is grouped by source vertex u, in classes of d = |N+(u)|:
-//   tiny   2 <= d <= kTinyMax     one thread per vertex, A in registers,
-//                                  monotone binary search of A' in B
-//   warp   ..  <= kWarpMax        one warp per vertex, N+(u) staged in the
-//                                  warp's shared memory (sorted + hash)
-//   block  ..  <= kBlockMax       one CTA per vertex (dynamic queue), staged
-//   large  ..  <= large cap       one 512-thread CTA per vertex, staged
-//   giant  larger                  one CTA per vertex, A read from global
-// Inside warp/block classes a warp takes one arc at a time and a 16x16
-// dispatch table indexed by (bucket |A'|, bucket |B|) picks the strategy:
-//   MERGE   lanes stream B in 16-byte (int4) chunks, locate each chunk in the
-//           staged sorted A' and merge the four keys forward
-//   HASH    lanes stream B and probe the shared-memory hash of N+(u)
-//   SEARCH  lanes take A' elements and binary-search them in B (global)
-// Counters: per-lane u64 by number of negative edges, warp shuffle + block
-// reduction, one atomic per counter per CTA.
+//   tiny   2 <= d <= 8        one thread per vertex, A in registers,
+//                             monotone binary search of A' in B
+//   warp   d <= 128           one warp per vertex     } N+(u) staged in
+//   block  d <= 1024          one CTA per vertex      } shared memory
+//   large  d <= 4096          one 512-thread CTA      }
+//   giant  larger             one CTA per vertex, A read from global memory
+// A 16x16 dispatch table indexed by (bucket |A'|, bucket |B|) picks each
+// arc's strategy:
+//   HASH    B is streamed and every element is tested against a shared-memory
+//           bitmap filter of N+(u); the few that pass are checked exactly in
+//           a shared-memory hash of N+(u)
+//   MERGE   B is streamed and each 16-byte chunk is located in the staged
+//           sorted A' by one binary search, its four keys merged forward
+//   SEARCH  a warp takes the arc: each lane holds one pivot of B, an A'
+//           element finds its segment with five shuffles and is searched in
+//           that short segment of B
+// HASH and MERGE arcs of one vertex form a single stream of aligned int4
+// chunks (prefix sums over the arcs' chunk counts, a per-thread arc cursor),
+// so every lane stays busy across arc boundaries and several loads stay in
+// flight per thread.  Counters: per-thread packed 16-bit fields by number of
+// negative edges, widened into u64 per vertex, then warp shuffle + block
+// reduction and one atomic per counter per CTA.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -39,17 +46,24 @@ namespace stc {
 namespace {
 
 constexpr uint32_t kEmpty = 0xFFFFFFFFu;
-constexpr uint32_t kWarpCap = 128;  // staged capacity of the warp class
+constexpr uint32_t kTinyMax = 8;
+constexpr uint32_t kWarpCap = 128;    // staged capacity of the warp class
+constexpr uint32_t kBlockCap = 1024;  // ... of the block class
+constexpr uint32_t kLargeCap = 4096;  // ... of the large class
+constexpr int kStreamUnroll = 2;      // int4 chunks in flight per thread
+// Device error word value: a list exceeded its staged shared-memory capacity
+// (the kernel skipped it instead of overrunning).
+constexpr unsigned long long kErrStageCapacity = 3;
 
 struct Csr {
   const uint64_t* __restrict__ off;
-  const uint32_t* __restrict__ nbr;
+  const uint32_t* __restrict__ nbr;  // padded by 4 entries for whole int4 chunks
   const int8_t* __restrict__ sgn;
   const uint32_t* __restrict__ verts;  // rank -> id (per-source counts only)
   uint32_t n;
 };
 
-// Per-lane type counters indexed by the number of negative edges.
+// Per-thread type counters indexed by the number of negative edges.
 struct TypeCounts {
   unsigned long long c[4] = {0, 0, 0, 0};
   __device__ __forceinline__ void add(uint32_t neg) {
@@ -57,6 +71,20 @@ struct TypeCounts {
     c[1] += neg == 1;
     c[2] += neg == 2;
     c[3] += neg == 3;
+  }
+};
+
+// Four 16-bit counters packed in one word: one add per triangle; widened
+// into TypeCounts before any field can reach 2^16.
+struct PackedCounts {
+  unsigned long long w = 0;
+  __device__ __forceinline__ void add(uint32_t neg) { w += 1ull << (16 * neg); }
+  __device__ __forceinline__ void drain(TypeCounts& tc) {
+    tc.c[0] += w & 0xFFFF;
+    tc.c[1] += (w >> 16) & 0xFFFF;
+    tc.c[2] += (w >> 32) & 0xFFFF;
+    tc.c[3] += w >> 48;
+    w = 0;
   }
 };
 
@@ -76,120 +104,324 @@ __device__ __forceinline__ uint32_t lower_bound(const uint32_t* a, uint32_t len,
   return lo;
 }
 
-__device__ __forceinline__ uint32_t hash_slot(uint32_t x, uint32_t shift) {
+// Bitmap filter index and hash slot use different multipliers so that a
+// filter false positive is not correlated with a hash collision.
+__device__ __forceinline__ uint32_t bit_index(uint32_t x, uint32_t shift) {
   return (x * 0x9E3779B1u) >> shift;
 }
-
-// N+(u) as one team sees it: sorted ids and signs (shared or global memory)
-// and, when staged, an open-addressing hash of the same list.
-struct Staged {
-  const uint32_t* a;
-  const int8_t* s;
-  const uint32_t* hk;  // nullptr: no hash
-  const int8_t* hs;
-  uint32_t d;
-  uint32_t mask;
-  uint32_t shift;
-};
-
-struct Arc {
-  uint32_t k;    // position of v in N+(u)
-  uint32_t nuv;  // 1 if the arc u -> v is negative
-  const uint32_t* __restrict__ b;
-  const int8_t* __restrict__ sb;
-  uint32_t blen;
-};
-
-__device__ __forceinline__ void arc_hash(const Staged& L, const Arc& A, uint32_t lane,
-                                         TypeCounts& tc) {
-  const uint32_t alast = L.a[L.d - 1];
-  for (uint32_t j = lane; j < A.blen; j += 32) {
-    const uint32_t x = A.b[j];
-    if (x > alast) break;
-    uint32_t h = hash_slot(x, L.shift);
-    while (true) {
-      const uint32_t key = L.hk[h];
-      if (key == x) {
-        tc.add(A.nuv + (L.hs[h] < 0) + (A.sb[j] < 0));
-        break;
-      }
-      if (key == kEmpty) break;
-      h = (h + 1) & L.mask;
-    }
-  }
+__device__ __forceinline__ uint32_t hash_slot(uint32_t x, uint32_t shift) {
+  return (x * 0x85EBCA77u) >> shift;
 }
 
-__device__ __forceinline__ void arc_search(const Staged& L, const Arc& A, uint32_t lane,
-                                           TypeCounts& tc) {
-  for (uint32_t i = A.k + 1 + lane; i < L.d; i += 32) {
-    const uint32_t x = L.a[i];
-    const uint32_t j = lower_bound(A.b, A.blen, x);
-    if (j < A.blen && A.b[j] == x) tc.add(A.nuv + (L.s[i] < 0) + (A.sb[j] < 0));
-  }
-}
-
-__device__ __forceinline__ void merge_one(const Staged& L, const Arc& A, uint32_t a0, uint32_t alen,
-                                          uint32_t j, uint32_t x, TypeCounts& tc) {
-  const uint32_t p = lower_bound(L.a + a0, alen, x);
-  if (p < alen && L.a[a0 + p] == x) tc.add(A.nuv + (L.s[a0 + p] < 0) + (A.sb[j] < 0));
-}
-
-__device__ __forceinline__ void arc_merge(const Staged& L, const Arc& A, uint32_t lane,
-                                          TypeCounts& tc) {
-  const uint32_t a0 = A.k + 1, alen = L.d - a0;
-  const uint32_t alast = L.a[L.d - 1];
-  // Scalar head up to 16-byte alignment of B, then int4 chunks, then tail.
-  const uint32_t mis = (uint32_t)(((uintptr_t)A.b >> 2) & 3);
-  const uint32_t head = min((4 - mis) & 3, A.blen);
-  if (lane < head) {
-    const uint32_t x = A.b[lane];
-    if (x <= alast) merge_one(L, A, a0, alen, lane, x, tc);
-  }
-  const uint32_t nch = (A.blen - head) >> 2;
-  const uint4* b4 = reinterpret_cast<const uint4*>(A.b + head);
-  for (uint32_t c = lane; c < nch; c += 32) {
-    const uint4 q = b4[c];
-    if (q.x > alast) break;
-    uint32_t p = lower_bound(L.a + a0, alen, q.x);
-    const uint32_t jb = head + 4 * c;
-    const uint32_t xs[4] = {q.x, q.y, q.z, q.w};
+// SEARCH for one arc by one warp: each lane holds the pivot B[lane * step];
+// an A' element (a[i], i in [i0, d)) finds its segment with five shuffles and
+// is searched inside that short segment of B, so a lookup costs about one
+// memory latency instead of log2 |B| dependent loads.
+template <class Counts>
+__device__ __forceinline__ void arc_search(const uint32_t* a, const int8_t* s, uint32_t i0,
+                                           uint32_t d, uint32_t nuv, const uint32_t* __restrict__ b,
+                                           const int8_t* __restrict__ sb, uint32_t blen,
+                                           uint32_t lane, Counts& cnt) {
+  const uint32_t step = (blen + 31) >> 5;
+  const uint32_t piv = b[min(lane * step, blen - 1)];
+  for (uint32_t base = i0; base < d; base += 32) {
+    const uint32_t i = base + lane;
+    const uint32_t x = i < d ? a[i] : kEmpty;
+    uint32_t seg = 0;
 #pragma unroll
-    for (int e = 0; e < 4; e++) {
-      const uint32_t x = xs[e];
-      while (p < alen && L.a[a0 + p] < x) p++;
-      if (p < alen && L.a[a0 + p] == x) tc.add(A.nuv + (L.s[a0 + p] < 0) + (A.sb[jb + e] < 0));
+    for (uint32_t bit = 16; bit; bit >>= 1) {
+      const uint32_t p = __shfl_sync(kFull, piv, seg + bit);
+      if ((seg + bit) * step < blen && p <= x) seg += bit;
+    }
+    if (i >= d) continue;
+    const uint32_t lo = seg * step;
+    const uint32_t j = lo + lower_bound(b + lo, min(step, blen - lo), x);
+    if (j < blen && b[j] == x) cnt.add(nuv + (s[i] < 0) + (sb[j] < 0));
+  }
+}
+
+// MERGE for one arc by one warp over B streamed in int4 chunks (giant lists,
+// whose A stays in global memory).
+__device__ __forceinline__ void arc_merge_global(const uint32_t* a, const int8_t* s, uint32_t a0,
+                                                 uint32_t d, uint32_t nuv,
+                                                 const uint32_t* __restrict__ b,
+                                                 const int8_t* __restrict__ sb, uint32_t blen,
+                                                 uint32_t lane, TypeCounts& tc) {
+  const uint32_t alen = d - a0;
+  const uint32_t alast = a[d - 1];
+  for (uint32_t base = 0; base < blen; base += 128) {
+    const uint32_t j0 = base + 4 * lane;
+    if (__shfl_sync(kFull, j0 < blen ? b[j0] : kEmpty, 0) > alast) return;
+    if (j0 >= blen) continue;
+    uint32_t p = lower_bound(a + a0, alen, b[j0]);
+    for (uint32_t j = j0; j < min(j0 + 4, blen); j++) {
+      const uint32_t x = b[j];
+      while (p < alen && a[a0 + p] < x) p++;
+      if (p < alen && a[a0 + p] == x) tc.add(nuv + (s[a0 + p] < 0) + (sb[j] < 0));
     }
   }
-  for (uint32_t j = head + 4 * nch + lane; j < A.blen; j += 32) {
-    const uint32_t x = A.b[j];
-    if (x <= alast) merge_one(L, A, a0, alen, j, x, tc);
+}
+
+// ---------------------------------------------------------- staging ----
+// Strategy codes in the per-arc table: STC_STRATEGY_MERGE / _HASH / _SEARCH,
+// or kNoArc for the last arc of a list (empty A') and arcs with empty B.
+constexpr uint8_t kNoArc = 0xFF;
+constexpr uint32_t kIdMask = 0x7FFFFFFFu;  // hash keys: id | negative << 31
+
+// Shared-memory image of one staged list of capacity `cap` with `nb` hash
+// buckets: the hash (two 32-bit keys per 8-byte bucket), the sorted ids,
+// each arc's B extent [lo, hi) as element indices of the CSR, the chunk
+// prefix sums, then the byte arrays (list signs, arc strategies).
+struct StageMem {
+  uint32_t* hk;
+  uint32_t* a;
+  uint32_t* lo;
+  uint32_t* hi;
+  uint32_t* pre;
+  int8_t* s;
+  uint8_t* st;
+  __host__ __device__ static constexpr size_t bytes(uint32_t cap, uint32_t nb) {
+    return 8ull * nb + 18ull * cap + 4;
+  }
+  __device__ static StageMem carve(unsigned char* p, uint32_t cap, uint32_t nb) {
+    StageMem m;
+    uint32_t* w = reinterpret_cast<uint32_t*>(p);
+    m.hk = w;
+    w += 2 * nb;
+    m.a = w;
+    w += cap;
+    m.lo = w;
+    w += cap;
+    m.hi = w;
+    w += cap;
+    m.pre = w;
+    w += cap + 1;
+    int8_t* b = reinterpret_cast<int8_t*>(w);
+    m.s = b;
+    b += cap;
+    m.st = reinterpret_cast<uint8_t*>(b);
+    return m;
+  }
+};
+
+// Hash geometry for a list of length d: next_pow2(4 d) buckets of two keys
+// (load <= 1/8), at most `nb_cap` buckets (load <= 1/4 when capped).
+struct Geo {
+  uint32_t nb, shift;
+  __device__ static Geo of(uint32_t d, uint32_t nb_cap) {
+    Geo g;
+    g.nb = 4;
+    while (g.nb < 4 * d && g.nb < nb_cap) g.nb <<= 1;
+    g.shift = 32 - (31 - __clz(g.nb));
+    return g;
+  }
+};
+
+struct WarpSync {
+  __device__ __forceinline__ void operator()() const { __syncwarp(); }
+};
+struct BlockSync {
+  __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+
+// Stages N+(u) (d entries at ub) for a team of TS threads (index t): clears
+// the hash, copies ids and signs, fetches every arc's B extent, then fills
+// the hash and picks each arc's strategy from the table.
+template <int TS, class Sync>
+__device__ __forceinline__ void stage(const Csr& g, uint64_t ub, uint32_t d, uint32_t t,
+                                      const StageMem& m, const Geo& geo,
+                                      const uint8_t (*table)[16], Sync sync) {
+  for (uint32_t i = t; i < 2 * geo.nb; i += TS) m.hk[i] = kEmpty;
+  for (uint32_t i = t; i < d; i += TS) {
+    const uint32_t v = g.nbr[ub + i];
+    m.a[i] = v;
+    m.s[i] = g.sgn[ub + i];
+    m.lo[i] = (uint32_t)g.off[v];
+    m.hi[i] = (uint32_t)g.off[v + 1];
+  }
+  sync();
+  for (uint32_t i = t; i < d; i += TS) {
+    const uint32_t x = m.a[i];
+    const uint32_t key = x | ((uint32_t)(m.s[i] < 0) << 31);
+    uint32_t b = hash_slot(x, geo.shift);
+    while (atomicCAS(&m.hk[2 * b], kEmpty, key) != kEmpty &&
+           atomicCAS(&m.hk[2 * b + 1], kEmpty, key) != kEmpty)
+      b = (b + 1) & (geo.nb - 1);
+    const uint32_t blen = m.hi[i] - m.lo[i];
+    m.st[i] = (i + 1 < d && blen) ? table[size_bucket(d - i - 1)][size_bucket(blen)] : kNoArc;
+  }
+  sync();
+}
+
+// Exact lookup continuing from bucket b (after a full bucket without a
+// match): 0 if x is not in the hash, else 1 | (the key's sign flag << 1).
+__device__ __noinline__ uint32_t probe_rest(const uint32_t* hk, uint32_t nb, uint32_t b, uint32_t x) {
+  while (true) {
+    const uint2 w = *reinterpret_cast<const uint2*>(hk + 2 * b);
+    if ((w.x & kIdMask) == x) return 1u | ((w.x >> 31) << 1);
+    if ((w.y & kIdMask) == x) return 1u | ((w.y >> 31) << 1);
+    if (w.y == kEmpty) return 0;
+    b = (b + 1) & (nb - 1);
   }
 }
 
-// One warp processes arc k of the staged list.
-__device__ __forceinline__ void process_arc(const Csr& g, const Staged& L, uint32_t k,
-                                            const uint8_t (*table)[16], uint32_t lane,
-                                            TypeCounts& tc) {
-  Arc A;
-  A.k = k;
-  const uint32_t v = L.a[k];
-  A.nuv = L.s[k] < 0;
-  const uint64_t vb = g.off[v];
-  A.blen = (uint32_t)(g.off[v + 1] - vb);
-  if (A.blen == 0) return;
-  A.b = g.nbr + vb;
-  A.sb = g.sgn + vb;
-  const uint32_t alen = L.d - k - 1;
-  uint32_t s = table[size_bucket(alen)][size_bucket(A.blen)];
-  if (s == STC_STRATEGY_HASH && L.hk == nullptr) s = STC_STRATEGY_MERGE;
-  if (s == STC_STRATEGY_HASH)
-    arc_hash(L, A, lane, tc);
-  else if (s == STC_STRATEGY_SEARCH)
-    arc_search(L, A, lane, tc);
-  else
-    arc_merge(L, A, lane, tc);
+__device__ __forceinline__ uint32_t arc_chunks(const StageMem& m, uint32_t i) {
+  const uint8_t st = m.st[i];
+  if (st != STC_STRATEGY_HASH && st != STC_STRATEGY_MERGE) return 0;
+  return ((m.hi[i] + 3) >> 2) - (m.lo[i] >> 2);
 }
 
+// pre[i] = int4 chunks of the streamed arcs before arc i; pre[d] = total.
+__device__ __forceinline__ void warp_chunk_scan(const StageMem& m, uint32_t d, uint32_t lane) {
+  uint32_t carry = 0;
+  for (uint32_t r = 0; r < d; r += 32) {
+    const uint32_t i = r + lane;
+    const uint32_t c = i < d ? arc_chunks(m, i) : 0;
+    const uint32_t inc = warp_inclusive_scan(c);
+    if (i < d) m.pre[i] = carry + inc - c;
+    carry += __shfl_sync(kFull, inc, 31);
+  }
+  if (lane == 0) m.pre[d] = carry;
+  __syncwarp();
+}
+
+template <int THREADS>
+__device__ __forceinline__ void block_chunk_scan(const StageMem& m, uint32_t d, uint32_t* tmp) {
+  uint32_t carry = 0;
+  for (uint32_t r = 0; r < d; r += THREADS) {
+    const uint32_t i = r + threadIdx.x;
+    const uint32_t c = i < d ? arc_chunks(m, i) : 0;
+    uint32_t total;
+    const uint32_t excl = block_exclusive_scan<THREADS>(c, tmp, total);
+    if (i < d) m.pre[i] = carry + excl;
+    carry += total;
+  }
+  if (threadIdx.x == 0) m.pre[d] = carry;
+  __syncthreads();
+}
+
+__device__ __forceinline__ uint32_t pick4(const uint4& q, uint32_t e) {
+  const uint32_t lo = (e & 1) ? q.y : q.x;
+  const uint32_t hi = (e & 1) ? q.w : q.z;
+  return (e & 2) ? hi : lo;
+}
+
+// The streamed arcs of a staged list as one sequence of aligned int4
+// chunks.  Warp w takes a contiguous share of the sequence and its lanes
+// take consecutive chunks (coalesced); each lane keeps the extent of its
+// current arc in registers and moves its cursor only at an arc boundary.
+// Per chunk: the four ids (one 16-byte load) and their four sign bytes (one
+// 4-byte load), a 4-bit mask of the ids inside the arc, then for HASH one
+// 8-byte bucket read per id answers membership and the A' sign together;
+// MERGE chunks are merged against the sorted A' instead.
+template <int U>
+__device__ __forceinline__ void stream_pass(const Csr& g, const StageMem& m, uint32_t d,
+                                            uint32_t warp, uint32_t warps, uint32_t lane,
+                                            const Geo& geo, PackedCounts& pc, TypeCounts& tc) {
+  const uint32_t total = m.pre[d];
+  const uint32_t per = (total + warps - 1) / warps;
+  const uint32_t c_begin = min(total, warp * per), c_end = min(total, c_begin + per);
+  if (c_begin >= c_end) return;
+  const uint4* __restrict__ nbr4 = reinterpret_cast<const uint4*>(g.nbr);
+  const uint32_t* __restrict__ sgn4 = reinterpret_cast<const uint32_t*>(g.sgn);
+  // Arc cursor: the last arc with pre[k] <= first chunk of this lane.
+  uint32_t k;
+  {
+    uint32_t lo_k = 0, hi_k = d;  // pre[d] = total > chunk
+    const uint32_t c0 = c_begin + lane;
+    while (hi_k - lo_k > 1) {
+      const uint32_t mid = (lo_k + hi_k) >> 1;
+      if (m.pre[mid] <= c0) lo_k = mid; else hi_k = mid;
+    }
+    k = lo_k;
+  }
+  uint32_t pk = m.pre[k], pk1 = m.pre[k + 1], alo = m.lo[k], ahi = m.hi[k];
+  uint32_t ast = m.st[k], anuv = m.s[k] < 0;
+  uint32_t rounds = 0;
+  for (uint32_t base = c_begin; base < c_end; base += 32 * U) {
+    uint4 q[U];
+    uint32_t sw[U], vm[U], sk[U], snuv[U], sst[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const uint32_t c = base + 32 * u + lane;
+      vm[u] = 0;
+      if (c < c_end) {
+        if (c >= pk1) {
+          do {
+            k++;
+          } while (m.pre[k + 1] <= c);
+          pk = m.pre[k];
+          pk1 = m.pre[k + 1];
+          alo = m.lo[k];
+          ahi = m.hi[k];
+          ast = m.st[k];
+          anuv = m.s[k] < 0;
+        }
+        const uint32_t ci = (alo >> 2) + (c - pk);
+        q[u] = nbr4[ci];
+        sw[u] = sgn4[ci];
+        const uint32_t g0 = 4 * ci;
+        const uint32_t first = alo > g0 ? alo - g0 : 0;
+        const uint32_t last = min(ahi - g0, 4u);
+        vm[u] = ((1u << last) - 1) & ~((1u << first) - 1);
+        sk[u] = k;
+        snuv[u] = anuv;
+        sst[u] = ast;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      if (vm[u] == 0) continue;
+      if (sst[u] == STC_STRATEGY_HASH) {
+#pragma unroll
+        for (uint32_t e = 0; e < 4; e++) {
+          const uint32_t x = pick4(q[u], e);
+          const uint32_t b = hash_slot(x, geo.shift);
+          const uint2 w = *reinterpret_cast<const uint2*>(m.hk + 2 * b);
+          const bool m0 = (w.x & kIdMask) == x, m1 = (w.y & kIdMask) == x;
+          uint32_t hit = (m0 | m1) & (vm[u] >> e) & 1u;
+          uint32_t na = (m0 ? w.x : w.y) >> 31;
+          if (!(m0 | m1) && w.y != kEmpty && ((vm[u] >> e) & 1u)) {
+            const uint32_t r = probe_rest(m.hk, geo.nb, (b + 1) & (geo.nb - 1), x);
+            hit = r & 1u;
+            na = r >> 1;
+          }
+          const uint32_t nb = (sw[u] >> (8 * e + 7)) & 1u;
+          if (hit) pc.add(snuv[u] + na + nb);
+        }
+      } else {  // MERGE: ids ascend within the chunk
+        const uint32_t a0 = sk[u] + 1, alen = d - a0;
+        const uint32_t* a = m.a + a0;
+        const uint32_t e0 = __ffs(vm[u]) - 1;
+        uint32_t p = lower_bound(a, alen, pick4(q[u], e0));
+        for (uint32_t e = e0; e < 4 && ((vm[u] >> e) & 1u); e++) {
+          const uint32_t x = pick4(q[u], e);
+          while (p < alen && a[p] < x) p++;
+          if (p < alen && a[p] == x)
+            pc.add(snuv[u] + (m.s[a0 + p] < 0) + ((sw[u] >> (8 * e + 7)) & 1u));
+        }
+      }
+    }
+    if (++rounds == 8000) {  // at most 4 * U adds per field per round
+      pc.drain(tc);
+      rounds = 0;
+    }
+  }
+}
+
+// SEARCH arcs of a staged list, one arc per warp.
+__device__ __forceinline__ void search_pass(const Csr& g, const StageMem& m, uint32_t d,
+                                            uint32_t warp, uint32_t warps, uint32_t lane,
+                                            PackedCounts& pc, TypeCounts& tc) {
+  for (uint32_t k = warp; k + 1 < d; k += warps) {
+    if (m.st[k] != STC_STRATEGY_SEARCH) continue;
+    const uint32_t lo = m.lo[k];
+    arc_search(m.a, m.s, k + 1, d, m.s[k] < 0, g.nbr + lo, g.sgn + lo, m.hi[k] - lo, lane, pc);
+    pc.drain(tc);
+  }
+}
+
+// ------------------------------------------------------- reductions ----
 // Block reduction of the four counters and one atomic per counter.
 // Slot C_T0 + k receives type Tk = 3 - (negative edges).
 template <int THREADS>
@@ -210,8 +442,7 @@ __device__ __forceinline__ void flush_counts(const TypeCounts& tc, unsigned long
   }
 }
 
-// Per-source counts: reduce the team's per-vertex counters into
-// vcounts[4 * id + type].
+// Per-source counts of one vertex: vcounts[4 * id + type].
 template <int THREADS>
 __device__ __forceinline__ void block_vertex_flush(const TypeCounts& vc, uint32_t u, const Csr& g,
                                                    unsigned long long* __restrict__ vcounts) {
@@ -231,6 +462,15 @@ __device__ __forceinline__ void block_vertex_flush(const TypeCounts& vc, uint32_
   __syncthreads();
 }
 
+__device__ __forceinline__ void warp_vertex_flush(const TypeCounts& vc, uint32_t u, const Csr& g,
+                                                  uint32_t lane, unsigned long long* __restrict__ vcounts) {
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const unsigned long long s = warp_sum(vc.c[k]);
+    if (lane == 0) vcounts[4ull * g.verts[u] + (3 - k)] = s;
+  }
+}
+
 // ------------------------------------------------------------ classes ----
 struct ClassBounds {
   uint32_t tiny_max, warp_max, block_max, large_max;
@@ -248,11 +488,16 @@ constexpr int kClasses = 5;
 __global__ void k_classify_count(const uint64_t* __restrict__ off, uint32_t n, ClassBounds cb,
                                  unsigned long long* __restrict__ ctr) {
   uint32_t cnt[kClasses] = {0, 0, 0, 0, 0};
+  uint32_t dmax = 0;
   for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
-    const uint32_t c = cb.of((uint32_t)(off[u + 1] - off[u]));
+    const uint32_t d = (uint32_t)(off[u + 1] - off[u]);
+    const uint32_t c = cb.of(d);
+    dmax = max(dmax, d);
 #pragma unroll
     for (int i = 0; i < kClasses; i++) cnt[i] += c == (uint32_t)i;
   }
+  dmax = __reduce_max_sync(kFull, dmax);
+  if (lane_id() == 0) atomicMax(ctr + C_MAX_FDEG, (unsigned long long)dmax);
 #pragma unroll
   for (int i = 0; i < kClasses; i++) {
     const uint32_t s = __reduce_add_sync(kFull, cnt[i]);
@@ -322,74 +567,104 @@ __global__ void __launch_bounds__(256) k_tiny(Csr g, const uint32_t* __restrict_
   if (!kVC) flush_counts<256>(tc, ctr);
 }
 
-// Warp class: one warp per vertex, N+(u) staged in the warp's shared memory.
+// Warp class: one warp per vertex, staged in the warp's slice of shared
+// memory (256 hash buckets).
+constexpr uint32_t kWarpBuckets = 2 * kWarpCap;
+constexpr size_t kWarpStageBytes = (StageMem::bytes(kWarpCap, kWarpBuckets) + 15) & ~size_t(15);
+
 template <bool kVC>
 __global__ void __launch_bounds__(256) k_warp(Csr g, const uint32_t* __restrict__ list, uint32_t cnt,
                                               unsigned long long* __restrict__ ctr,
                                               unsigned long long* __restrict__ vcounts,
                                               const uint8_t* __restrict__ gtable) {
   constexpr int kWarps = 8;
-  __shared__ uint32_t sa[kWarps][kWarpCap];
-  __shared__ uint32_t hk[kWarps][2 * kWarpCap];
-  __shared__ int8_t ss[kWarps][kWarpCap];
-  __shared__ int8_t hs[kWarps][2 * kWarpCap];
+  __shared__ __align__(16) unsigned char smem[kWarps * kWarpStageBytes];
   __shared__ uint8_t table[16][16];
   for (int i = threadIdx.x; i < 256; i += blockDim.x) (&table[0][0])[i] = gtable[i];
   __syncthreads();
   const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
+  const StageMem m = StageMem::carve(smem + w * kWarpStageBytes, kWarpCap, kWarpBuckets);
   TypeCounts tc;
   const uint32_t warps = gridDim.x * kWarps;
   for (uint32_t idx = blockIdx.x * kWarps + w; idx < cnt; idx += warps) {
     const uint32_t u = list[idx];
     const uint64_t ub = g.off[u];
     const uint32_t d = (uint32_t)(g.off[u + 1] - ub);
-    uint32_t H = 4;
-    while (H < 2 * d) H <<= 1;
-    const uint32_t shift = 32 - (31 - __clz(H));
-    for (uint32_t i = lane; i < H; i += 32) hk[w][i] = kEmpty;
-    for (uint32_t i = lane; i < d; i += 32) {
-      sa[w][i] = g.nbr[ub + i];
-      ss[w][i] = g.sgn[ub + i];
+    if (d > kWarpCap) {  // uniform over the warp
+      if (lane == 0) atomicExch(ctr + C_ERROR, kErrStageCapacity);
+      continue;
     }
-    __syncwarp();
-    for (uint32_t i = lane; i < d; i += 32) {
-      const uint32_t x = sa[w][i];
-      uint32_t h = hash_slot(x, shift);
-      while (atomicCAS(&hk[w][h], kEmpty, x) != kEmpty) h = (h + 1) & (H - 1);
-      hs[w][h] = ss[w][i];
-    }
-    __syncwarp();
-    Staged L{sa[w], ss[w], hk[w], hs[w], d, H - 1, shift};
+    const Geo geo = Geo::of(d, kWarpBuckets);
+    stage<32>(g, ub, d, lane, m, geo, table, WarpSync{});
+    warp_chunk_scan(m, d, lane);
     TypeCounts vc;
-    for (uint32_t k = 0; k + 1 < d; k++) process_arc(g, L, k, table, lane, kVC ? vc : tc);
-    if (kVC) {
-#pragma unroll
-      for (int k = 0; k < 4; k++) {
-        const unsigned long long s = warp_sum(vc.c[k]);
-        if (lane == 0) vcounts[4ull * g.verts[u] + (3 - k)] = s;
-      }
-    }
+    TypeCounts& out = kVC ? vc : tc;
+    PackedCounts pc;
+    stream_pass<kStreamUnroll>(g, m, d, 0, 1, lane, geo, pc, out);
+    search_pass(g, m, d, 0, 1, lane, pc, out);
+    pc.drain(out);
+    if (kVC) warp_vertex_flush(vc, u, g, lane, vcounts);
     __syncwarp();
   }
   if (!kVC) flush_counts<256>(tc, ctr);
 }
 
-// Block classes: one CTA per vertex from a dynamic queue; `cap` is the
-// staged capacity (dynamic shared memory: cap ids, cap signs, 2*cap hash
-// keys and signs).  With kStaged == false (giant vertices) A is read from
-// global memory and HASH falls back to MERGE.
-template <int THREADS, bool kStaged, bool kVC>
+// Block classes: one CTA per vertex from a dynamic queue, the list staged in
+// dynamic shared memory of capacity `cap` with `nb` hash buckets
+// (nb >= 2 * cap, powers of two).
+inline size_t block_stage_bytes(uint32_t cap, uint32_t nb) { return StageMem::bytes(cap, nb); }
+
+template <int THREADS, bool kVC>
 __global__ void __launch_bounds__(THREADS) k_block(Csr g, const uint32_t* __restrict__ list,
-                                                   uint32_t cnt, uint32_t cap,
+                                                   uint32_t cnt, uint32_t cap, uint32_t nb,
                                                    unsigned long long* __restrict__ queue,
                                                    unsigned long long* __restrict__ ctr,
                                                    unsigned long long* __restrict__ vcounts,
                                                    const uint8_t* __restrict__ gtable) {
   extern __shared__ __align__(16) unsigned char smem[];
-  uint32_t* sa = reinterpret_cast<uint32_t*>(smem);
-  uint32_t* hk = sa + cap;
-  int8_t* ss = reinterpret_cast<int8_t*>(hk + 2 * cap);
-  int8_t* hs = ss + cap;
+  __shared__ uint8_t table[16][16];
+  __shared__ uint32_t scan_tmp[THREADS / 32 + 1];
+  __shared__ uint32_t s_item;
+  for (int i = threadIdx.x; i < 256; i += THREADS) (&table[0][0])[i] = gtable[i];
+  const StageMem m = StageMem::carve(smem, cap, nb);
+  constexpr uint32_t kWarps = THREADS / 32;
+  const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
+  TypeCounts tc;
+  while (true) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_item = (uint32_t)atomicAdd(queue, 1ull);
+    __syncthreads();
+    const uint32_t item = s_item;
+    if (item >= cnt) break;
+    const uint32_t u = list[item];
+    const uint64_t ub = g.off[u];
+    const uint32_t d = (uint32_t)(g.off[u + 1] - ub);
+    if (d > cap) {  // uniform over the CTA
+      if (threadIdx.x == 0) atomicExch(ctr + C_ERROR, kErrStageCapacity);
+      continue;
+    }
+    const Geo geo = Geo::of(d, nb);
+    stage<THREADS>(g, ub, d, threadIdx.x, m, geo, table, BlockSync{});
+    block_chunk_scan<THREADS>(m, d, scan_tmp);
+    TypeCounts vc;
+    TypeCounts& out = kVC ? vc : tc;
+    PackedCounts pc;
+    stream_pass<kStreamUnroll>(g, m, d, w, kWarps, lane, geo, pc, out);
+    search_pass(g, m, d, w, kWarps, lane, pc, out);
+    pc.drain(out);
+    if (kVC) block_vertex_flush<THREADS>(vc, u, g, vcounts);
+  }
+  if (!kVC) flush_counts<THREADS>(tc, ctr);
+}
+
+// Giant lists (d > kLargeCap): one CTA per vertex, A read from global memory,
+// one arc per warp; HASH falls back to MERGE (no staged hash).
+template <int THREADS, bool kVC>
+__global__ void __launch_bounds__(THREADS) k_giant(Csr g, const uint32_t* __restrict__ list,
+                                                   uint32_t cnt, unsigned long long* __restrict__ queue,
+                                                   unsigned long long* __restrict__ ctr,
+                                                   unsigned long long* __restrict__ vcounts,
+                                                   const uint8_t* __restrict__ gtable) {
   __shared__ uint8_t table[16][16];
   __shared__ uint32_t s_item;
   for (int i = threadIdx.x; i < 256; i += THREADS) (&table[0][0])[i] = gtable[i];
@@ -405,30 +680,24 @@ __global__ void __launch_bounds__(THREADS) k_block(Csr g, const uint32_t* __rest
     const uint32_t u = list[item];
     const uint64_t ub = g.off[u];
     const uint32_t d = (uint32_t)(g.off[u + 1] - ub);
-    Staged L;
-    if (kStaged) {
-      uint32_t H = 4;
-      while (H < 2 * d) H <<= 1;
-      const uint32_t shift = 32 - (31 - __clz(H));
-      for (uint32_t i = threadIdx.x; i < H; i += THREADS) hk[i] = kEmpty;
-      for (uint32_t i = threadIdx.x; i < d; i += THREADS) {
-        sa[i] = g.nbr[ub + i];
-        ss[i] = g.sgn[ub + i];
-      }
-      __syncthreads();
-      for (uint32_t i = threadIdx.x; i < d; i += THREADS) {
-        const uint32_t x = sa[i];
-        uint32_t h = hash_slot(x, shift);
-        while (atomicCAS(&hk[h], kEmpty, x) != kEmpty) h = (h + 1) & (H - 1);
-        hs[h] = ss[i];
-      }
-      __syncthreads();
-      L = Staged{sa, ss, hk, hs, d, H - 1, shift};
-    } else {
-      L = Staged{g.nbr + ub, g.sgn + ub, nullptr, nullptr, d, 0, 0};
-    }
+    const uint32_t* a = g.nbr + ub;
+    const int8_t* s = g.sgn + ub;
     TypeCounts vc;
-    for (uint32_t k = w; k + 1 < d; k += kWarps) process_arc(g, L, k, table, lane, kVC ? vc : tc);
+    TypeCounts& out = kVC ? vc : tc;
+    for (uint32_t k = w; k + 1 < d; k += kWarps) {
+      const uint32_t v = a[k];
+      const uint64_t vb = g.off[v];
+      const uint32_t blen = (uint32_t)(g.off[v + 1] - vb);
+      if (blen == 0) continue;
+      const uint32_t st = table[size_bucket(d - k - 1)][size_bucket(blen)];
+      if (st == STC_STRATEGY_SEARCH) {
+        PackedCounts pc;
+        arc_search(a, s, k + 1, d, s[k] < 0, g.nbr + vb, g.sgn + vb, blen, lane, pc);
+        pc.drain(out);
+      } else {
+        arc_merge_global(a, s, k + 1, d, s[k] < 0, g.nbr + vb, g.sgn + vb, blen, lane, out);
+      }
+    }
     if (kVC) block_vertex_flush<THREADS>(vc, u, g, vcounts);
   }
   if (!kVC) flush_counts<THREADS>(tc, ctr);
@@ -468,12 +737,13 @@ void count_triangles(stc_ctx* c, const DeviceGraph& g, const CountConfig& cfg) {
 
   // Vertex classes (a forced strategy disables the tiny class, which only
   // implements the search form).
-  ClassBounds cb{cfg.strategy == STC_STRATEGY_AUTO || cfg.strategy == STC_STRATEGY_SEARCH ? 8u : 1u,
-                 kWarpCap, 1024u, 8192u};
+  const bool tiny = cfg.strategy == STC_STRATEGY_AUTO || cfg.strategy == STC_STRATEGY_SEARCH;
+  const ClassBounds cb{tiny ? kTinyMax : 1u, kWarpCap, kBlockCap, kLargeCap};
   k_classify_count<<<kSMs * 4, 256, 0, st>>>(g.off, g.n, cb, ctr);
-  STC_CUDA(cudaMemcpyAsync(c->h_pinned + C_WORK, counters(c) + C_WORK, kClasses * sizeof(uint64_t),
-                           cudaMemcpyDeviceToHost, st));
+  STC_CUDA(cudaMemcpyAsync(c->h_pinned + C_WORK, counters(c) + C_WORK,
+                           (C_MAX_FDEG + 1 - C_WORK) * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
   STC_CUDA(cudaStreamSynchronize(st));
+  const uint32_t max_fdeg = (uint32_t)c->h_pinned[C_MAX_FDEG];
   uint32_t counts[kClasses], starts[kClasses + 1];
   starts[0] = 0;
   for (int i = 0; i < kClasses; i++) {
@@ -483,7 +753,7 @@ void count_triangles(stc_ctx* c, const DeviceGraph& g, const CountConfig& cfg) {
   uint32_t* lists = buffer<uint32_t>(c, B_WORK, (size_t)starts[kClasses] + 8);
   uint32_t* d_starts = lists + starts[kClasses];
   STC_CUDA(cudaMemcpyAsync(d_starts, starts, kClasses * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-  // Cursors for the fill and the dynamic queues live in C_WORK + 8 ...
+  // Cursors of the fill, then the dynamic queues, live in C_WORK ...
   STC_CUDA(cudaMemsetAsync(counters(c) + C_WORK, 0, 8 * sizeof(uint64_t), st));
   k_classify_fill<<<kSMs * 4, 256, 0, st>>>(g.off, g.n, cb, lists, d_starts, ctr + C_WORK);
   STC_CUDA(cudaMemsetAsync(counters(c) + C_WORK, 0, 8 * sizeof(uint64_t), st));
@@ -491,8 +761,8 @@ void count_triangles(stc_ctx* c, const DeviceGraph& g, const CountConfig& cfg) {
 
   if (counts[0]) {
     const uint32_t grid = std::min<uint32_t>((counts[0] + 255) / 256, kSMs * 8);
-    if (vc) k_tiny<8, true><<<grid, 256, 0, st>>>(csr, lists + starts[0], counts[0], ctr, vcounts);
-    else k_tiny<8, false><<<grid, 256, 0, st>>>(csr, lists + starts[0], counts[0], ctr, vcounts);
+    if (vc) k_tiny<kTinyMax, true><<<grid, 256, 0, st>>>(csr, lists + starts[0], counts[0], ctr, vcounts);
+    else k_tiny<kTinyMax, false><<<grid, 256, 0, st>>>(csr, lists + starts[0], counts[0], ctr, vcounts);
     c->launches++;
   }
   if (counts[1]) {
@@ -502,28 +772,32 @@ void count_triangles(stc_ctx* c, const DeviceGraph& g, const CountConfig& cfg) {
     c->launches++;
   }
   if (counts[2]) {
-    const uint32_t cap = cb.block_max;
-    const size_t smem = (size_t)cap * 15;
+    const uint32_t cap = kBlockCap, nb = 4 * kBlockCap;
+    const size_t smem = block_stage_bytes(cap, nb);
+    auto kern = vc ? k_block<256, true> : k_block<256, false>;
+    STC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const uint32_t grid = std::min<uint32_t>(counts[2], kSMs * 8);
-    auto kern = vc ? k_block<256, true, true> : k_block<256, true, false>;
-    kern<<<grid, 256, smem, st>>>(csr, lists + starts[2], counts[2], cap, ctr + C_WORK + 0, ctr,
+    kern<<<grid, 256, smem, st>>>(csr, lists + starts[2], counts[2], cap, nb, ctr + C_WORK + 0, ctr,
                                   vcounts, d_table);
     c->launches++;
   }
   if (counts[3]) {
-    const uint32_t cap = cb.large_max;
-    const size_t smem = (size_t)cap * 15;
-    auto kern = vc ? k_block<512, true, true> : k_block<512, true, false>;
+    // Capacity: the class's largest list rounded up to a power of two.
+    uint32_t cap = kBlockCap;
+    while (cap < std::min<uint32_t>(max_fdeg, kLargeCap)) cap <<= 1;
+    const uint32_t nb = 2 * cap;
+    const size_t smem = block_stage_bytes(cap, nb);
+    auto kern = vc ? k_block<512, true> : k_block<512, false>;
     STC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const uint32_t grid = std::min<uint32_t>(counts[3], kSMs);
-    kern<<<grid, 512, smem, st>>>(csr, lists + starts[3], counts[3], cap, ctr + C_WORK + 1, ctr,
+    const uint32_t grid = std::min<uint32_t>(counts[3], kSMs * 2);
+    kern<<<grid, 512, smem, st>>>(csr, lists + starts[3], counts[3], cap, nb, ctr + C_WORK + 1, ctr,
                                   vcounts, d_table);
     c->launches++;
   }
   if (counts[4]) {
-    auto kern = vc ? k_block<512, false, true> : k_block<512, false, false>;
-    const uint32_t grid = std::min<uint32_t>(counts[4], kSMs);
-    kern<<<grid, 512, 0, st>>>(csr, lists + starts[4], counts[4], 0, ctr + C_WORK + 2, ctr, vcounts,
+    auto kern = vc ? k_giant<512, true> : k_giant<512, false>;
+    const uint32_t grid = std::min<uint32_t>(counts[4], kSMs * 2);
+    kern<<<grid, 512, 0, st>>>(csr, lists + starts[4], counts[4], ctr + C_WORK + 2, ctr, vcounts,
                                d_table);
     c->launches++;
   }

@@ -53,8 +53,15 @@ enum CounterSlot {
   C_ALG_BYTES = 7,
   C_WORK = 8,                  // dynamic work counters (8 slots)
   C_ERROR = 16,                // device error word (0 = ok)
+  C_MAX_FDEG = 17,             // largest out-degree of the forward CSR
   C_SLOTS = 32
 };
+
+// Values of the device error word: 1 = malformed forward CSR,
+// 2 = a bounded device-side wait expired, 3 = a list exceeded its staged
+// shared-memory capacity (the kernel skipped it instead of overrunning).
+constexpr uint64_t kDeviceErrCsr = 1;
+constexpr uint64_t kDeviceErrTimeout = 2;
 
 }  // namespace stc
 

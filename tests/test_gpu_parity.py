@@ -130,9 +130,10 @@ def test_degenerate_inputs(ctx):
 
 
 def test_id_limit(ctx):
-    with pytest.raises(stc.StcError) as e:
-        ctx.count(np.array([1 << 31], np.uint32), np.array([1], np.uint32), np.array([1], np.int8))
-    assert e.value.status == _capi.STC_ERR_LIMIT
+    for bad in ((1 << 31) - 1, 1 << 31, (1 << 32) - 1):
+        with pytest.raises(stc.StcError) as e:
+            ctx.count(np.array([bad], np.uint32), np.array([1], np.uint32), np.array([1], np.int8))
+        assert e.value.status == _capi.STC_ERR_LIMIT
 
 
 def test_vertex_counts(ctx):
