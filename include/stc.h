@@ -189,6 +189,29 @@ stc_status stc_vertex_counts(stc_ctx* ctx, const uint32_t* src, const uint32_t* 
 stc_status stc_count_batch(stc_ctx* ctx, const stc_graph* graphs, uint32_t G,
                            const stc_opts* opts, stc_counts* outs);
 
+/* ------------------------------------------------------- no allocation ---- */
+/* No counterpart in the reference.  Counts the triangles of an oriented
+ * forward CSR that already sits in device memory, and allocates nothing:
+ * for callers that cannot call cudaMalloc, such as code that must draw all
+ * device memory from its own pool or allocator, or that runs inside a memory
+ * budget where an allocation by a library would fail or fragment the heap.
+ * Input: d_offsets (n + 1 entries), d_heads and d_signs (m entries each plus
+ * 4 readable padding entries; d_heads 16-byte aligned, d_signs 4-byte
+ * aligned); each list sorted ascending and each head above its tail (any
+ * acyclic orientation gives the same counts); a negative sign byte marks a
+ * negative edge.  The input is checked on the device first: a malformed CSR
+ * returns STC_ERR_INVALID_ARGUMENT.  Limits: n <= 4,194,304 and m < 2^32,
+ * else STC_ERR_LIMIT.
+ * Scratch: one file-scope device array of about 16 MiB, which every GPU that
+ * loads the library keeps until the process exits.  All calls share it, so
+ * calls that overlap on the GPU race.  The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress) with that device
+ * current; make that first call before any stream capture.  `stream` may be
+ * NULL (the legacy default stream). */
+stc_status stc_count_oriented_csr_noalloc(const uint64_t* d_offsets, const uint32_t* d_heads,
+                                          const int8_t* d_signs, uint32_t n, uint64_t m,
+                                          void* stream, stc_counts* out);
+
 /* --------------------------------------------------- device generator ---- */
 /* Writes the RMAT samples of stc_synth_rmat (include/stc_synth.h) for the
  * same arguments directly into device arrays of `samples` elements. */

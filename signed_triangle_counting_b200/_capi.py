@@ -98,6 +98,8 @@ SIGNATURES = [
                                     C.POINTER(stc_opts), u64p, C.c_uint64, u32p]),
     ("stc_count_batch", C.c_int, [C.c_void_p, C.POINTER(stc_graph), C.c_uint32,
                                   C.POINTER(stc_opts), C.POINTER(stc_counts)]),
+    ("stc_count_oriented_csr_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                                 C.c_uint64, C.c_void_p, C.POINTER(stc_counts)]),
     ("stc_synth_rmat_device", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint64,
                                         C.c_uint64, C.c_double, C.c_double, C.c_double,
                                         C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -37,6 +37,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "internal.h"
 #include "stc_device.cuh"
@@ -805,3 +806,177 @@ void count_triangles(stc_ctx* c, const DeviceGraph& g, const CountConfig& cfg) {
 }
 
 }  // namespace stc
+
+// ===================================================== no-allocation path ===
+// stc_count_oriented_csr_noalloc counts an oriented forward CSR that already
+// sits in device memory without allocating anything: for callers that cannot
+// call cudaMalloc (code running under a custom device allocator or inside a
+// memory budget it does not control).  Its scratch (vertex worklists, the
+// dispatch table, counters) lives in one file-scope device array of fixed
+// size; every GPU that loads the library holds that array until exit, every
+// call shares it, and calls that overlap on the GPU race on it.
+namespace stc {
+namespace {
+
+constexpr uint32_t kNoAllocMaxVertices = 1u << 22;  // 16 MiB of worklists
+constexpr int kNoAllocMaxDevices = 64;
+
+struct NoAllocScratch {
+  unsigned long long ctr[C_SLOTS];
+  uint8_t table[256];
+  uint32_t lists[kNoAllocMaxVertices + 8];
+};
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
+
+// Input checks on the device: offsets start at 0, never decrease and end at
+// m; every head is below n, above its tail and above the previous head of
+// its list.  Any violation sets ctr[C_ERROR] = kDeviceErrCsr.
+__global__ void k_check_oriented(const uint64_t* __restrict__ off, const uint32_t* __restrict__ heads,
+                                 uint32_t n, uint64_t m, unsigned long long* __restrict__ ctr) {
+  const uint32_t stride = gridDim.x * blockDim.x;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && (off[0] != 0 || off[n] != m))
+    atomicExch(ctr + C_ERROR, (unsigned long long)kDeviceErrCsr);
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += stride) {
+    const uint64_t b = off[u], e = off[u + 1];
+    bool bad = e < b || e > m;
+    if (!bad) {
+      uint32_t prev = u;
+      for (uint64_t i = b; i < e; i++) {
+        const uint32_t h = heads[i];
+        if (h >= n || h <= prev) {
+          bad = true;
+          break;
+        }
+        prev = h;
+      }
+    }
+    if (bad) atomicExch(ctr + C_ERROR, (unsigned long long)kDeviceErrCsr);
+  }
+}
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device (looked up once
+// per device with that device current).
+cudaError_t noalloc_scratch(int device, NoAllocScratch** out) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    g_noalloc_addr[device] = p;
+  }
+  *out = static_cast<NoAllocScratch*>(g_noalloc_addr[device]);
+  return cudaSuccess;
+}
+
+stc_status noalloc_cuda(cudaError_t e) {
+  (void)cudaGetLastError();
+  return e == cudaErrorMemoryAllocation ? STC_ERR_OUT_OF_MEMORY : STC_ERR_CUDA;
+}
+
+}  // namespace
+
+}  // namespace stc
+
+#define STC_NA(call)                                   \
+  do {                                                 \
+    const cudaError_t e_ = (call);                     \
+    if (e_ != cudaSuccess) return stc::noalloc_cuda(e_); \
+  } while (0)
+
+extern "C" stc_status stc_count_oriented_csr_noalloc(const uint64_t* d_offsets,
+                                                      const uint32_t* d_heads,
+                                                      const int8_t* d_signs, uint32_t n,
+                                                      uint64_t m, void* stream, stc_counts* out) {
+  using namespace stc;
+  if (!out || !d_offsets || (m && (!d_heads || !d_signs))) return STC_ERR_INVALID_ARGUMENT;
+  if ((reinterpret_cast<uintptr_t>(d_heads) & 15) || (reinterpret_cast<uintptr_t>(d_signs) & 3))
+    return STC_ERR_INVALID_ARGUMENT;
+  if (n > kNoAllocMaxVertices || m >= (1ull << 32)) return STC_ERR_LIMIT;
+  *out = stc_counts{0, 0, 0, 0};
+  if (n == 0) return STC_OK;
+  int device = 0;
+  STC_NA(cudaGetDevice(&device));
+  if (device < 0 || device >= kNoAllocMaxDevices) return STC_ERR_NO_DEVICE;
+  NoAllocScratch* scr = nullptr;
+  STC_NA(noalloc_scratch(device, &scr));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  unsigned long long* ctr = scr->ctr;
+  STC_NA(cudaMemsetAsync(ctr, 0, sizeof(scr->ctr), st));
+  k_check_oriented<<<kSMs * 4, 256, 0, st>>>(d_offsets, d_heads, n, m, ctr);
+  STC_NA(cudaGetLastError());
+  uint64_t slots[C_SLOTS];
+  STC_NA(cudaMemcpyAsync(slots, ctr, sizeof(slots), cudaMemcpyDeviceToHost, st));
+  STC_NA(cudaStreamSynchronize(st));
+  if (slots[C_ERROR]) return STC_ERR_INVALID_ARGUMENT;
+  if (m == 0) return STC_OK;
+
+  uint8_t table[16][16];
+  fixed_table(table);
+  STC_NA(cudaMemcpyAsync(scr->table, table, sizeof(table), cudaMemcpyHostToDevice, st));
+  const ClassBounds cb{kTinyMax, kWarpCap, kBlockCap, kLargeCap};
+  k_classify_count<<<kSMs * 4, 256, 0, st>>>(d_offsets, n, cb, ctr);
+  STC_NA(cudaMemcpyAsync(slots, ctr, sizeof(slots), cudaMemcpyDeviceToHost, st));
+  STC_NA(cudaStreamSynchronize(st));
+  const uint32_t max_fdeg = (uint32_t)slots[C_MAX_FDEG];
+  uint32_t counts[kClasses], starts[kClasses + 1];
+  starts[0] = 0;
+  for (int i = 0; i < kClasses; i++) {
+    counts[i] = (uint32_t)slots[C_WORK + i];
+    starts[i + 1] = starts[i] + counts[i];
+  }
+  uint32_t* lists = scr->lists;
+  uint32_t* d_starts = lists + starts[kClasses];
+  STC_NA(cudaMemcpyAsync(d_starts, starts, kClasses * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+  STC_NA(cudaMemsetAsync(ctr + C_WORK, 0, 8 * sizeof(uint64_t), st));
+  k_classify_fill<<<kSMs * 4, 256, 0, st>>>(d_offsets, n, cb, lists, d_starts, ctr + C_WORK);
+  STC_NA(cudaMemsetAsync(ctr + C_WORK, 0, 8 * sizeof(uint64_t), st));
+
+  const Csr csr{d_offsets, d_heads, d_signs, nullptr, n};
+  const uint8_t* d_table = scr->table;
+  if (counts[0]) {
+    const uint32_t grid = std::min<uint32_t>((counts[0] + 255) / 256, kSMs * 8);
+    k_tiny<kTinyMax, false><<<grid, 256, 0, st>>>(csr, lists + starts[0], counts[0], ctr, nullptr);
+  }
+  if (counts[1]) {
+    const uint32_t grid = std::min<uint32_t>((counts[1] + 7) / 8, kSMs * 8);
+    k_warp<false><<<grid, 256, 0, st>>>(csr, lists + starts[1], counts[1], ctr, nullptr, d_table);
+  }
+  if (counts[2]) {
+    const uint32_t cap = kBlockCap, nb = 4 * kBlockCap;
+    const size_t smem = block_stage_bytes(cap, nb);
+    STC_NA(cudaFuncSetAttribute(k_block<256, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem));
+    const uint32_t grid = std::min<uint32_t>(counts[2], kSMs * 8);
+    k_block<256, false><<<grid, 256, smem, st>>>(csr, lists + starts[2], counts[2], cap, nb,
+                                                  ctr + C_WORK + 0, ctr, nullptr, d_table);
+  }
+  if (counts[3]) {
+    uint32_t cap = kBlockCap;
+    while (cap < std::min<uint32_t>(max_fdeg, kLargeCap)) cap <<= 1;
+    const uint32_t nb = 2 * cap;
+    const size_t smem = block_stage_bytes(cap, nb);
+    STC_NA(cudaFuncSetAttribute(k_block<512, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem));
+    const uint32_t grid = std::min<uint32_t>(counts[3], kSMs * 2);
+    k_block<512, false><<<grid, 512, smem, st>>>(csr, lists + starts[3], counts[3], cap, nb,
+                                                  ctr + C_WORK + 1, ctr, nullptr, d_table);
+  }
+  if (counts[4]) {
+    const uint32_t grid = std::min<uint32_t>(counts[4], kSMs * 2);
+    k_giant<512, false><<<grid, 512, 0, st>>>(csr, lists + starts[4], counts[4], ctr + C_WORK + 2,
+                                               ctr, nullptr, d_table);
+  }
+  STC_NA(cudaGetLastError());
+  STC_NA(cudaMemcpyAsync(slots, ctr, sizeof(slots), cudaMemcpyDeviceToHost, st));
+  STC_NA(cudaStreamSynchronize(st));
+  if (slots[C_ERROR]) return STC_ERR_INTERNAL;
+  out->t0 = slots[C_T0];
+  out->t1 = slots[C_T1];
+  out->t2 = slots[C_T2];
+  out->t3 = slots[C_T3];
+  return STC_OK;
+}
