@@ -26,6 +26,8 @@ import threading
 import time
 from pathlib import Path
 
+import numpy as np
+
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
@@ -37,6 +39,8 @@ WORKLOADS = {
     1: "ER G(n=10,000, m=100,000), p(+)=0.7",
     2: "Delaunay of 1,000,000 uniform points, 20% of edges deleted, p(+)=0.6",
     3: "RMAT scale 24, edge factor 16, (.57,.19,.19,.05), symmetrised + deduped, p(+)=0.5",
+    4: "batch of 4,096 graphs: n log-uniform in [1e3, 1e6], ER deg 8 / RMAT ef 8 / Delaunay-20%, "
+       "p(+) uniform in [0.3, 0.9]",
     5: "skew: 64Mi vertices, 128Mi samples, backbone + 32 hubs deg in [1e5,1e7], p(+)=0.8",
 }
 
@@ -124,7 +128,10 @@ def golden_counts(workload: int):
     p = ROOT / "tests" / "golden" / "golden.json"
     if not p.exists():
         return None
-    w = json.loads(p.read_text()).get("workloads", {}).get(f"{workload}/0")
+    g = json.loads(p.read_text())
+    if workload == 4:
+        return g["batch"]["t"] if "batch" in g else None
+    w = g.get("workloads", {}).get(f"{workload}/0")
     return tuple(w["t"]) if w else None
 
 
@@ -141,6 +148,25 @@ def make_device_workload(ctx, workload: int, seed_offset: int, torch, scale: int
         sign = torch.empty(samples, dtype=torch.int8, device=dev)
         ctx.synth_rmat_device(seed, scale, n, samples, 0.57, 0.19, 0.19, 0.5, src, dst, sign)
         return src, dst, sign
+    if workload == 4:
+        specs = synth.batch_specs(4096)
+        parts, offs, pos = [], [0], 0
+        dev = torch.device("cuda", ctx.device)
+        for g0 in range(0, len(specs), 256):
+            el, o = synth.batch_packed(specs, g0, min(len(specs), g0 + 256))
+            parts.append(el)
+            offs.extend(int(x) + pos for x in o[1:])
+            pos += el.m
+        src = torch.empty(pos, dtype=torch.int32, device=dev)
+        dst = torch.empty(pos, dtype=torch.int32, device=dev)
+        sign = torch.empty(pos, dtype=torch.int8, device=dev)
+        at = 0
+        for el in parts:
+            src[at:at + el.m] = torch.from_numpy(el.src.view("int32")).to(dev)
+            dst[at:at + el.m] = torch.from_numpy(el.dst.view("int32")).to(dev)
+            sign[at:at + el.m] = torch.from_numpy(el.sign).to(dev)
+            at += el.m
+        return src, dst, sign, offs
     el = synth.workload(workload)
     if seed_offset:
         raise SystemExit("only the RMAT workload has per-rank instances")
@@ -214,13 +240,19 @@ def run_gpu(args) -> None:
         torch.cuda.set_device(local)
     ctx = stc.Context(local)
     stream = torch.cuda.current_stream(local)
-    src, dst, sign = make_device_workload(ctx, args.workload, rank, torch, args.rmat_scale)
+    wl = make_device_workload(ctx, args.workload, rank, torch, args.rmat_scale)
+    src, dst, sign = wl[:3]
+    offs = np.asarray(wl[3], np.uint64) if len(wl) > 3 else None
     torch.cuda.synchronize()
     m_input = src.numel()
 
     def step():
-        c = ctx.count(src, dst, sign, strategy=args.strategy, dispatch=args.dispatch,
-                      stream=stream.cuda_stream)
+        if offs is not None:
+            c = ctx.count_batch_packed(src, dst, sign, offs, strategy=args.strategy,
+                                       dispatch=args.dispatch, stream=stream.cuda_stream)
+        else:
+            c = ctx.count(src, dst, sign, strategy=args.strategy, dispatch=args.dispatch,
+                          stream=stream.cuda_stream)
         return c, ctx.last_stats()
 
     counts, st = None, None
@@ -229,7 +261,12 @@ def run_gpu(args) -> None:
     # Exact-count check of rank 0's instance against the reference's counts.
     full = args.workload != 3 or args.rmat_scale == 24
     want = golden_counts(args.workload) if rank == 0 and full else None
-    exact = (counts.as_tuple() == want) if want is not None else None
+    if offs is not None:
+        exact = [list(c.as_tuple()) for c in counts] == want if want is not None else None
+        counts_out = [int(sum(c.as_tuple()[k] for c in counts)) for k in range(4)]
+    else:
+        exact = (counts.as_tuple() == want) if want is not None else None
+        counts_out = list(counts.as_tuple())
 
     # ---- timed region: inputs resident in HBM (2.4 GB > 126 MB L2)
     sampler = ClockSampler(local)
@@ -260,21 +297,35 @@ def run_gpu(args) -> None:
     value = world * edges * args.steps / (ms / 1e3)
 
     # ---- end to end through the C ABI from pinned host memory
-    h_src = torch.empty(m_input, dtype=torch.int32, pin_memory=True)
-    h_dst = torch.empty(m_input, dtype=torch.int32, pin_memory=True)
-    h_sign = torch.empty(m_input, dtype=torch.int8, pin_memory=True)
+    try:
+        h_src = torch.empty(m_input, dtype=torch.int32, pin_memory=True)
+        h_dst = torch.empty(m_input, dtype=torch.int32, pin_memory=True)
+        h_sign = torch.empty(m_input, dtype=torch.int8, pin_memory=True)
+        pinned = True
+    except RuntimeError:
+        h_src = torch.empty(m_input, dtype=torch.int32)
+        h_dst = torch.empty(m_input, dtype=torch.int32)
+        h_sign = torch.empty(m_input, dtype=torch.int8)
+        pinned = False
     h_src.copy_(src)
     h_dst.copy_(dst)
     h_sign.copy_(sign)
     torch.cuda.synchronize()
     import ctypes as C
     from signed_triangle_counting_b200 import _capi
-    out = _capi.stc_counts()
     o = stc.Context._opts(args.strategy, args.dispatch, False, True, stream.cuda_stream)
+    G = len(offs) - 1 if offs is not None else 1
+    out = (_capi.stc_counts * G)()
 
     def e2e_step():
-        s_ = _capi.lib().stc_count(ctx._h, C.c_void_p(h_src.data_ptr()), C.c_void_p(h_dst.data_ptr()),
-                                   C.c_void_p(h_sign.data_ptr()), m_input, C.byref(o), C.byref(out))
+        if offs is not None:
+            s_ = _capi.lib().stc_count_batch_packed(
+                ctx._h, C.c_void_p(h_src.data_ptr()), C.c_void_p(h_dst.data_ptr()),
+                C.c_void_p(h_sign.data_ptr()), offs.ctypes.data_as(_capi.u64p), G, C.byref(o), out)
+        else:
+            s_ = _capi.lib().stc_count(ctx._h, C.c_void_p(h_src.data_ptr()),
+                                       C.c_void_p(h_dst.data_ptr()), C.c_void_p(h_sign.data_ptr()),
+                                       m_input, C.byref(o), out)
         assert s_ == 0, stc.StcError(s_)
 
     e2e_step()
@@ -318,9 +369,9 @@ def run_gpu(args) -> None:
                        f"RMAT scale {args.rmat_scale}, edge factor 16, (.57,.19,.19,.05), p(+)=0.5",
                        "m_input": m_input,
                        "m_unique": edges, "n": st.n, "strategy": args.strategy,
-                       "dispatch": args.dispatch, "l2": "inputs 2.4 GB > 126 MB L2, no flush",
+                       "dispatch": args.dispatch, "l2": f"inputs {m_input * 9 / 1e9:.1f} GB > 126 MB L2, no flush",
                        "parallelism": f"{world} rank(s), one graph instance each"},
-            "exact": exact, "counts": list(counts.as_tuple()),
+            "exact": exact, "counts": counts_out,
             "stage_ms": {"dedup": st.ms_dedup, "orient": st.ms_orient, "csr": st.ms_csr,
                          "count": st.ms_count, "device_total": st.ms_total},
             "roofline": {"bound": "hbm", "kernel": "intersection engine (count)",
@@ -330,7 +381,8 @@ def run_gpu(args) -> None:
                          "count_ms": cms},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": m_input * 9,
-                    "d2h_bytes_per_step": 32, "steps": e2e_steps},
+                    "d2h_bytes_per_step": 32 * G, "steps": e2e_steps,
+                    "host_memory": "pinned" if pinned else "pageable"},
             "gpu_launches": launches,
             "clocks": clocks,
         }
@@ -347,7 +399,7 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["mine", "reference"], default="mine")
-    ap.add_argument("--workload", type=int, default=3, choices=[1, 2, 3, 5])
+    ap.add_argument("--workload", type=int, default=3, choices=[1, 2, 3, 4, 5])
     ap.add_argument("--strategy", default="auto", choices=["auto", "merge", "hash", "search"])
     ap.add_argument("--dispatch", default="fixed", choices=["fixed", "learned"])
     ap.add_argument("--skip-cpu", action="store_true")

@@ -185,7 +185,8 @@ stc_status stc_vertex_counts(stc_ctx* ctx, const uint32_t* src, const uint32_t* 
                              uint64_t* counts, uint64_t counts_len, uint32_t* n_out);
 
 /* ---------------------------------------------------------------- batch ---- */
-/* Counts G independent graphs; outs[g] receives graph g's counts. */
+/* Counts G independent graphs (gathered on the device, then counted as by
+ * stc_count_batch_packed); outs[g] receives graph g's counts. */
 stc_status stc_count_batch(stc_ctx* ctx, const stc_graph* graphs, uint32_t G,
                            const stc_opts* opts, stc_counts* outs);
 
@@ -211,6 +212,18 @@ stc_status stc_count_batch(stc_ctx* ctx, const stc_graph* graphs, uint32_t G,
 stc_status stc_count_oriented_csr_noalloc(const uint64_t* d_offsets, const uint32_t* d_heads,
                                           const int8_t* d_signs, uint32_t n, uint64_t m,
                                           void* stream, stc_counts* out);
+
+/* Counts G graphs stored back to back: graph g owns elements
+ * [offsets[g], offsets[g + 1]) of src/dst/sign (host arrays, or device arrays
+ * with STC_F_DEVICE_INPUT) with ids local to the graph; `offsets` is a host
+ * array of G + 1 entries and outs[g] receives graph g's counts.  The graphs
+ * are counted together as one disjoint union whose vertex order is
+ * graph-major and (degree, id) within each graph, so every graph is oriented
+ * exactly as it would be alone.  No counterpart in the reference, which
+ * counts one graph per process. */
+stc_status stc_count_batch_packed(stc_ctx* ctx, const uint32_t* src, const uint32_t* dst,
+                                  const int8_t* sign, const uint64_t* offsets, uint32_t G,
+                                  const stc_opts* opts, stc_counts* outs);
 
 /* --------------------------------------------------- device generator ---- */
 /* Writes the RMAT samples of stc_synth_rmat (include/stc_synth.h) for the

@@ -61,6 +61,12 @@ int stc_synth_batch_specs(uint64_t seed, uint32_t G, stc_batch_spec* specs);
 /* Builds graph `spec` of a batch. */
 int stc_synth_batch_graph(const stc_batch_spec* spec, stc_synth_graph* out);
 
+/* Graphs [g_begin, g_end) of a batch, generated in parallel and packed back
+ * to back into `out` (ids local to each graph); offsets[i] (g_end - g_begin
+ * + 1 entries, caller-owned) receives the start of graph g_begin + i. */
+int stc_synth_batch_packed(const stc_batch_spec* specs, uint32_t g_begin, uint32_t g_end,
+                           stc_synth_graph* out, uint64_t* offsets);
+
 /* The five named workloads: 1 = ER(1e4, 1e5, p=.7); 2 = Delaunay(1e6 points,
  * 20% deleted, p=.6); 3 = RMAT(scale 24, ef 16, .57/.19/.19/.05, p=.5);
  * 5 = skew(64Mi vertices, 128Mi samples, 32 hubs in [1e5, 1e7], p=.8).

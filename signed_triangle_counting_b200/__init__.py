@@ -308,6 +308,27 @@ class Context:
         _check(lib().stc_count_batch(self._h, arr, len(graphs), C.byref(o), outs), self._h)
         return [GlobalTriCounts(x.t0, x.t1, x.t2, x.t3) for x in outs[: len(graphs)]]
 
+    def count_batch_packed(self, src, dst, sign, offsets, *, strategy="auto", dispatch="fixed",
+                           stream=None, timing=True) -> list:
+        """Counts graphs stored back to back (graph g owns entries
+        [offsets[g], offsets[g + 1]), ids local to the graph); numpy arrays
+        are host input, torch CUDA tensors device input."""
+        offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+        G = len(offsets) - 1
+        dev = hasattr(src, "is_cuda") and src.is_cuda
+        if dev:
+            if stream is None:
+                import torch
+                stream = torch.cuda.current_stream(src.device).cuda_stream
+        else:
+            src, dst, sign = _host_arrays(src, dst, sign)
+        outs = (_capi.stc_counts * max(1, G))()
+        o = self._opts(strategy, dispatch, dev, timing, stream)
+        _check(lib().stc_count_batch_packed(self._h, _ptr(src), _ptr(dst), _ptr(sign),
+                                            offsets.ctypes.data_as(_capi.u64p), G, C.byref(o),
+                                            outs), self._h)
+        return [GlobalTriCounts(x.t0, x.t1, x.t2, x.t3) for x in outs[:G]]
+
     def last_stats(self) -> Stats:
         s = _capi.stc_stats()
         _check(lib().stc_ctx_last_stats(self._h, C.byref(s)))

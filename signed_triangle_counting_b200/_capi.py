@@ -98,6 +98,9 @@ SIGNATURES = [
                                     C.POINTER(stc_opts), u64p, C.c_uint64, u32p]),
     ("stc_count_batch", C.c_int, [C.c_void_p, C.POINTER(stc_graph), C.c_uint32,
                                   C.POINTER(stc_opts), C.POINTER(stc_counts)]),
+    ("stc_count_batch_packed", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         u64p, C.c_uint32, C.POINTER(stc_opts),
+                                         C.POINTER(stc_counts)]),
     ("stc_count_oriented_csr_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                                  C.c_uint64, C.c_void_p, C.POINTER(stc_counts)]),
     ("stc_synth_rmat_device", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint64,
@@ -114,6 +117,8 @@ SIGNATURES = [
                                  C.c_uint64, C.c_double, C.POINTER(stc_synth_graph)]),
     ("stc_synth_batch_specs", C.c_int, [C.c_uint64, C.c_uint32, C.POINTER(stc_batch_spec)]),
     ("stc_synth_batch_graph", C.c_int, [C.POINTER(stc_batch_spec), C.POINTER(stc_synth_graph)]),
+    ("stc_synth_batch_packed", C.c_int, [C.POINTER(stc_batch_spec), C.c_uint32, C.c_uint32,
+                                         C.POINTER(stc_synth_graph), u64p]),
     ("stc_synth_workload", C.c_int, [C.c_int, C.c_uint32, C.POINTER(stc_synth_graph)]),
     ("stc_synth_workload_seed", C.c_uint64, [C.c_int]),
     ("stc_synth_set_threads", None, [C.c_uint32]),

@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <vector>
 
 #include "internal.h"
 #include "radix_sort.cuh"
@@ -247,6 +248,92 @@ void finish_csr_from_arc_keys(stc_ctx* c, DeviceGraph& g, uint64_t* akeys, uint6
   STC_CUDA(cudaGetLastError());
 }
 
+// ------------------------------------------------------------ batches ----
+// A batch of G graphs is counted as one disjoint union: graph g's local id x
+// becomes vbase[g] + x, where vbase is the prefix sum of the graphs' id
+// spaces.  Edges (and vertices) of one graph are contiguous, so a CTA that
+// owns a contiguous range finds the graph of its first element by binary
+// search and then only moves a cursor forward.
+__device__ __forceinline__ uint32_t first_segment(const uint64_t* __restrict__ bounds, uint32_t G,
+                                                  uint64_t i) {
+  uint32_t lo = 0, hi = G;  // largest g with bounds[g] <= i
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (bounds[mid] <= i) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// Id space of every graph (max endpoint + 1) and the self-loop count.
+__global__ void k_batch_ids(const uint32_t* __restrict__ u, const uint32_t* __restrict__ v,
+                            uint64_t m, const uint64_t* __restrict__ eoff, uint32_t G,
+                            uint64_t per_cta, unsigned int* __restrict__ gspace,
+                            unsigned long long* __restrict__ ctr) {
+  const uint64_t begin = (uint64_t)blockIdx.x * per_cta;
+  const uint64_t end = begin + per_cta < m ? begin + per_cta : m;
+  if (begin >= end) return;
+  uint32_t g = first_segment(eoff, G, begin);
+  uint32_t self = 0;
+  for (uint64_t base = begin + (threadIdx.x & ~31u); base < end; base += blockDim.x) {
+    const uint64_t i = base + lane_id();
+    const bool valid = i < end;
+    uint32_t space = 0;
+    if (valid) {
+      while (eoff[g + 1] <= i) g++;
+      const uint32_t a = u[i], b = v[i];
+      self += a == b;
+      space = max(a, b) + 1;
+    }
+    const uint32_t key = valid ? g : 0xFFFFFFFFu;
+    const unsigned peers = __match_any_sync(kFull, key);
+    const uint32_t mx = __reduce_max_sync(peers, space);
+    if (valid && (peers & lanemask_lt()) == 0) atomicMax(gspace + g, mx);
+  }
+  self = __reduce_add_sync(kFull, self);
+  if (lane_id() == 0 && self) atomicAdd(ctr + C_SELF, (unsigned long long)self);
+}
+
+// Dedup keys of the union (global ids), as k_pack_dedup.
+__global__ void k_batch_pack(const uint32_t* __restrict__ u, const uint32_t* __restrict__ v,
+                             const int8_t* __restrict__ s, uint64_t m,
+                             const uint64_t* __restrict__ eoff, const uint64_t* __restrict__ vbase,
+                             uint32_t G, uint64_t per_cta, uint32_t bits,
+                             uint64_t* __restrict__ keys) {
+  const uint64_t begin = (uint64_t)blockIdx.x * per_cta;
+  const uint64_t end = begin + per_cta < m ? begin + per_cta : m;
+  if (begin >= end) return;
+  const uint64_t sentinel = (bits * 2 >= 64) ? ~0ull >> 1 : ((1ull << (2 * bits)) - 1);
+  uint32_t g = first_segment(eoff, G, begin);
+  for (uint64_t i = begin + threadIdx.x; i < end; i += blockDim.x) {
+    while (eoff[g + 1] <= i) g++;
+    const uint32_t a = u[i], b = v[i];
+    uint64_t k;
+    if (a == b) {
+      k = sentinel;
+    } else {
+      const uint64_t vb = vbase[g];
+      const uint64_t lo = vb + (a < b ? a : b), hi = vb + (a < b ? b : a);
+      k = (lo << bits) | hi | ((uint64_t)(s[i] < 0) << 63);
+    }
+    keys[i] = k;
+  }
+}
+
+// Adds each vertex's graph above its degree in the vertex sort key, so that
+// ranks are graph-major and (degree, id) within a graph.
+__global__ void k_batch_vertex_graph(uint64_t* __restrict__ vkeys, uint32_t n,
+                                     const uint64_t* __restrict__ vbase, uint32_t G,
+                                     uint64_t per_cta, uint32_t shift) {
+  const uint64_t begin = (uint64_t)blockIdx.x * per_cta;
+  const uint64_t end = begin + per_cta < n ? begin + per_cta : n;
+  if (begin >= end) return;
+  uint32_t g = first_segment(vbase, G, begin);
+  for (uint64_t i = begin + threadIdx.x; i < end; i += blockDim.x) {
+    while (vbase[g + 1] <= i) g++;
+    vkeys[i] |= (uint64_t)g << shift;
+  }
+}
+
 }  // namespace
 
 void build_graph(stc_ctx* c, const uint32_t* d_src, const uint32_t* d_dst, const int8_t* d_sign,
@@ -370,6 +457,115 @@ void graph_from_forward_csr(stc_ctx* c, uint32_t n, uint64_t m, const uint64_t* 
     STC_CUDA(cudaMemsetAsync(g.off, 0, ((size_t)n + 1) * sizeof(uint64_t), st));
     g.nbr = buffer<uint32_t>(c, B_NBR, 1);
     g.sgn = buffer<int8_t>(c, B_SGN, 1);
+  }
+  mark(c, 4);
+}
+
+void build_graph_batch(stc_ctx* c, const uint32_t* d_src, const uint32_t* d_dst,
+                       const int8_t* d_sign, uint64_t m, const uint64_t* h_eoff, uint32_t G,
+                       DeviceGraph& g) {
+  cudaStream_t st = c->stream;
+  unsigned long long* ctr = (unsigned long long*)counters(c);
+  g = DeviceGraph{};
+  g.m_input = m;
+  g.G = G;
+  if (m >= (1ull << 32)) fail(STC_ERR_LIMIT, "batch has 2^32 or more edges");
+  uint64_t* d_eoff = buffer<uint64_t>(c, B_BATCH_META, 2ull * (G + 1));
+  uint64_t* d_vbase = d_eoff + (G + 1);
+  unsigned int* d_space = reinterpret_cast<unsigned int*>(buffer<uint32_t>(c, B_BATCH_SPACE, G));
+  STC_CUDA(cudaMemcpyAsync(d_eoff, h_eoff, (G + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+  STC_CUDA(cudaMemsetAsync(d_space, 0, G * sizeof(uint32_t), st));
+
+  // 1. id space per graph -> vertex bases of the union.
+  mark(c, 1);
+  const RangePartition ep = range_partition(m, kSortTile, kMaxSortGrid);
+  if (m) {
+    k_batch_ids<<<ep.grid, kThreads, 0, st>>>(d_src, d_dst, m, d_eoff, G, ep.per_cta, d_space, ctr);
+    c->launches++;
+  }
+  std::vector<uint32_t> space(G);
+  STC_CUDA(cudaMemcpyAsync(space.data(), d_space, G * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  read_counters(c, C_SELF, 1);
+  std::vector<uint64_t> vbase(G + 1, 0);
+  for (uint32_t i = 0; i < G; i++) vbase[i + 1] = vbase[i] + space[i];
+  const uint64_t ntot = vbase[G];
+  if (ntot >= (1ull << 31) - 1)
+    fail(STC_ERR_LIMIT, "batch has 2^31 - 1 or more vertices in total");
+  STC_CUDA(cudaMemcpyAsync(d_vbase, vbase.data(), (G + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice,
+                           st));
+  g.n = (uint32_t)ntot;
+  g.m_valid = m - c->h_pinned[C_SELF];
+  g.bits = std::max<uint32_t>(1, bit_width64(ntot ? ntot - 1 : 0));
+  g.gbase = d_vbase;
+  uint32_t* sort_counts = buffer<uint32_t>(c, B_SORT_COUNTS, (size_t)kRadix * kMaxSortGrid);
+  uint64_t* sums = buffer<uint64_t>(c, B_SCAN_SUMS, kMaxSortGrid + 1);
+
+  // 2. dedup over the union.
+  uint64_t* ka = buffer<uint64_t>(c, B_KEYS_A, m);
+  uint64_t* kb = buffer<uint64_t>(c, B_KEYS_B, m);
+  g.ukeys = buffer<uint64_t>(c, B_UKEYS, g.m_valid);
+  if (g.m_valid) {
+    k_batch_pack<<<ep.grid, kThreads, 0, st>>>(d_src, d_dst, d_sign, m, d_eoff, d_vbase, G,
+                                                ep.per_cta, g.bits, ka);
+    c->launches++;
+    uint64_t* sorted = radix_sort(ka, kb, m, 0, 2 * (int)g.bits, sort_counts, st, &c->launches);
+    const uint64_t mask = (1ull << (2 * g.bits)) - 1;
+    range_scan(UniqueFlag{sorted, mask}, UniqueEmit{sorted, g.ukeys}, g.m_valid, sums, st,
+               &c->launches);
+    const uint32_t grid = range_partition(g.m_valid, kScanTile, kMaxSortGrid).grid;
+    STC_CUDA(cudaMemcpyAsync(c->h_pinned + C_WORK, sums + grid, sizeof(uint64_t),
+                             cudaMemcpyDeviceToHost, st));
+    STC_CUDA(cudaStreamSynchronize(st));
+    g.m_unique = c->h_pinned[C_WORK];
+  }
+  STC_CUDA(cudaGetLastError());
+  mark(c, 2);
+
+  // 3-4. degree and graph-major (graph, degree, id) rank.
+  g.deg = buffer<uint32_t>(c, B_DEG, g.n);
+  g.rank = buffer<uint32_t>(c, B_RANK, g.n);
+  g.verts = buffer<uint32_t>(c, B_VERTS, g.n);
+  g.fdeg = buffer<uint32_t>(c, B_FDEG, g.n);
+  if (g.n) {
+    STC_CUDA(cudaMemsetAsync(g.deg, 0, (size_t)g.n * sizeof(uint32_t), st));
+    STC_CUDA(cudaMemsetAsync(g.fdeg, 0, (size_t)g.n * sizeof(uint32_t), st));
+    if (g.m_unique) {
+      k_degree<<<grid_for(g.m_unique, 4), kThreads, 0, st>>>(g.ukeys, g.m_unique, g.bits, g.deg);
+      c->launches++;
+    }
+    uint64_t* va = buffer<uint64_t>(c, B_VKEYS_A, g.n);
+    uint64_t* vb = buffer<uint64_t>(c, B_VKEYS_B, g.n);
+    k_vertex_keys<<<grid_for(g.n, 4), kThreads, 0, st>>>(g.deg, g.n, va, ctr);
+    c->launches++;
+    read_counters(c, C_MAX_DEG, 1);
+    g.max_deg = (uint32_t)c->h_pinned[C_MAX_DEG];
+    const int dbits = (int)bit_width64(g.max_deg);
+    const int gbits = (int)bit_width64(G > 1 ? G - 1 : 0);
+    if (32 + dbits + gbits > 64) fail(STC_ERR_LIMIT, "batch too large for the vertex sort key");
+    if (gbits) {
+      const RangePartition vp = range_partition(g.n, kSortTile, kMaxSortGrid);
+      k_batch_vertex_graph<<<vp.grid, kThreads, 0, st>>>(va, g.n, d_vbase, G, vp.per_cta, 32 + dbits);
+      c->launches++;
+    }
+    uint64_t* vs = radix_sort(va, vb, g.n, 32, 32 + dbits + gbits, sort_counts, st, &c->launches);
+    k_rank<<<grid_for(g.n, 4), kThreads, 0, st>>>(vs, g.n, g.verts, g.rank);
+    c->launches++;
+  }
+  STC_CUDA(cudaGetLastError());
+  mark(c, 3);
+
+  // 5-6. orientation and the forward CSR (graphs stay contiguous in rank space).
+  g.m_fwd = g.m_unique;
+  if (g.m_fwd) {
+    k_arc_keys<<<grid_for(g.m_fwd, 4), kThreads, 0, st>>>(g.ukeys, g.m_fwd, g.bits, g.rank, ka,
+                                                          g.fdeg);
+    c->launches++;
+    finish_csr_from_arc_keys(c, g, ka, kb);
+  } else {
+    g.off = buffer<uint64_t>(c, B_OFF, (size_t)g.n + 1);
+    STC_CUDA(cudaMemsetAsync(g.off, 0, ((size_t)g.n + 1) * sizeof(uint64_t), st));
+    g.nbr = buffer<uint32_t>(c, B_NBR, 4);
+    g.sgn = buffer<int8_t>(c, B_SGN, 4);
   }
   mark(c, 4);
 }

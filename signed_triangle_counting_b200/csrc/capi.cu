@@ -126,6 +126,11 @@ DeviceInput stage_input(stc_ctx* c, const uint32_t* src, const uint32_t* dst, co
   return DeviceInput{ds, dd, dg};
 }
 
+// Graphs of a batch are counted in groups of at most this many edges (one
+// pass of the union pipeline each), which bounds the device memory a batch
+// needs to about 45 bytes per edge of a group.
+constexpr uint64_t kBatchGroupEdges = 1536ull << 20;
+
 CountConfig count_config(const stc_opts* o) {
   CountConfig cfg;
   if (o) {
@@ -353,15 +358,112 @@ stc_status stc_vertex_counts(stc_ctx* c, const uint32_t* src, const uint32_t* ds
   });
 }
 
+stc_status stc_count_batch_packed(stc_ctx* c, const uint32_t* src, const uint32_t* dst,
+                                  const int8_t* sign, const uint64_t* offsets, uint32_t G,
+                                  const stc_opts* o, stc_counts* outs) {
+  if (!c || (G && (!offsets || !outs))) return STC_ERR_INVALID_ARGUMENT;
+  return guarded(c, [&] {
+    if (G == 0) return;
+    if (offsets[0] != 0) fail(STC_ERR_INVALID_ARGUMENT, "offsets[0] must be 0");
+    for (uint32_t i = 0; i < G; i++)
+      if (offsets[i + 1] < offsets[i]) fail(STC_ERR_INVALID_ARGUMENT, "offsets decrease");
+    const uint64_t M = offsets[G];
+    if (M && (!src || !dst || !sign)) fail(STC_ERR_INVALID_ARGUMENT, "null edge array");
+    CountConfig cfg = count_config(o);
+    begin_call(c, o);
+    const bool dev = o && (o->flags & STC_F_DEVICE_INPUT);
+    stc_stats total{};
+    uint32_t g0 = 0;
+    while (g0 < G) {
+      // Group of graphs whose edges fit one pass of the union pipeline.
+      uint32_t g1 = g0 + 1;
+      while (g1 < G && offsets[g1 + 1] - offsets[g0] <= kBatchGroupEdges) g1++;
+      const uint64_t e0 = offsets[g0], me = offsets[g1] - e0;
+      const uint32_t gn = g1 - g0;
+      std::vector<uint64_t> eoff(gn + 1);
+      for (uint32_t i = 0; i <= gn; i++) eoff[i] = offsets[g0 + i] - e0;
+      STC_CUDA(cudaMemsetAsync(counters(c), 0, C_SLOTS * sizeof(uint64_t), c->stream));
+      DeviceInput in;
+      if (dev) {
+        in = DeviceInput{src + e0, dst + e0, sign + e0};
+      } else {
+        in = stage_input(c, src + e0, dst + e0, sign + e0, me, o);
+      }
+      DeviceGraph g;
+      build_graph_batch(c, in.src, in.dst, in.sign, me, eoff.data(), gn, g);
+      uint64_t* gc = buffer<uint64_t>(c, B_BATCH_COUNTS, 4ull * gn);
+      STC_CUDA(cudaMemsetAsync(gc, 0, 4ull * gn * sizeof(uint64_t), c->stream));
+      cfg.graph_counts = gc;
+      count_triangles(c, g, cfg);
+      mark(c, 5);
+      std::vector<uint64_t> h(4ull * gn);
+      STC_CUDA(cudaMemcpyAsync(h.data(), gc, h.size() * sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                               c->stream));
+      STC_CUDA(cudaMemcpyAsync(c->h_pinned, counters(c), C_SLOTS * sizeof(uint64_t),
+                               cudaMemcpyDeviceToHost, c->stream));
+      STC_CUDA(cudaStreamSynchronize(c->stream));
+      if (c->h_pinned[C_ERROR])
+        fail(STC_ERR_INTERNAL, "device reported error word " + std::to_string(c->h_pinned[C_ERROR]));
+      if (c->timing) {  // stage times summed over the groups
+        total.ms_dedup += elapsed(c, 1, 2);
+        total.ms_orient += elapsed(c, 2, 3);
+        total.ms_csr += elapsed(c, 3, 4);
+        total.ms_count += elapsed(c, 4, 5);
+      }
+      for (uint32_t i = 0; i < gn; i++) {
+        stc_counts& r = outs[g0 + i];
+        r.t0 = h[4ull * i + 0];
+        r.t1 = h[4ull * i + 1];
+        r.t2 = h[4ull * i + 2];
+        r.t3 = h[4ull * i + 3];
+        total.triangles += r.t0 + r.t1 + r.t2 + r.t3;
+      }
+      total.n += g.n;
+      total.m_input += g.m_input;
+      total.m_unique += g.m_unique;
+      total.m_forward += g.m_fwd;
+      total.alg_bytes += c->h_pinned[C_ALG_BYTES];
+      g0 = g1;
+    }
+    mark(c, 7);
+    STC_CUDA(cudaStreamSynchronize(c->stream));
+    total.kernel_launches = (uint32_t)c->launches;
+    if (c->timing) total.ms_total = elapsed(c, 0, 7);
+    c->stats = total;
+  });
+}
+
 stc_status stc_count_batch(stc_ctx* c, const stc_graph* graphs, uint32_t G, const stc_opts* o,
                            stc_counts* outs) {
   if (!c || (G && (!graphs || !outs))) return STC_ERR_INVALID_ARGUMENT;
-  // Graph-at-a-time fallback path; the persistent batched engine replaces it.
-  for (uint32_t i = 0; i < G; i++) {
-    stc_status s = stc_count(c, graphs[i].src, graphs[i].dst, graphs[i].sign, graphs[i].m, o, &outs[i]);
-    if (s != STC_OK) return s;
-  }
-  return STC_OK;
+  // Gathers the graphs back to back on the device, then counts them packed.
+  std::vector<uint64_t> off(G + 1, 0);
+  for (uint32_t i = 0; i < G; i++) off[i + 1] = off[i] + graphs[i].m;
+  const bool dev = o && (o->flags & STC_F_DEVICE_INPUT);
+  stc_status s = guarded(c, [&] {
+    const uint64_t M = off[G];
+    cudaStream_t st = (o && o->stream) ? (cudaStream_t)o->stream : c->own_stream;
+    uint32_t* ds = buffer<uint32_t>(c, B_IN_SRC, M);
+    uint32_t* dd = buffer<uint32_t>(c, B_IN_DST, M);
+    int8_t* dg = buffer<int8_t>(c, B_IN_SIGN, M);
+    const cudaMemcpyKind kind = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    for (uint32_t i = 0; i < G; i++) {
+      const uint64_t m = graphs[i].m;
+      if (!m) continue;
+      if (!graphs[i].src || !graphs[i].dst || !graphs[i].sign)
+        fail(STC_ERR_INVALID_ARGUMENT, "null edge array in graph " + std::to_string(i));
+      STC_CUDA(cudaMemcpyAsync(ds + off[i], graphs[i].src, m * sizeof(uint32_t), kind, st));
+      STC_CUDA(cudaMemcpyAsync(dd + off[i], graphs[i].dst, m * sizeof(uint32_t), kind, st));
+      STC_CUDA(cudaMemcpyAsync(dg + off[i], graphs[i].sign, m, kind, st));
+    }
+  });
+  if (s != STC_OK) return s;
+  stc_opts o2 = o ? *o : stc_opts{};
+  o2.flags |= STC_F_DEVICE_INPUT;
+  return stc_count_batch_packed(c, static_cast<const uint32_t*>(c->bufs[B_IN_SRC].p),
+                                static_cast<const uint32_t*>(c->bufs[B_IN_DST].p),
+                                static_cast<const int8_t*>(c->bufs[B_IN_SIGN].p), off.data(), G,
+                                &o2, outs);
 }
 
 stc_status stc_synth_rmat_device(stc_ctx* c, uint64_t seed, uint32_t scale, uint64_t n,

@@ -443,10 +443,44 @@ __device__ __forceinline__ void flush_counts(const TypeCounts& tc, unsigned long
   }
 }
 
-// Per-source counts of one vertex: vcounts[4 * id + type].
-template <int THREADS>
-__device__ __forceinline__ void block_vertex_flush(const TypeCounts& vc, uint32_t u, const Csr& g,
-                                                   unsigned long long* __restrict__ vcounts) {
+// Where per-vertex totals go when a kernel reports per vertex.
+struct TotalSink {  // only the four global counters
+  static constexpr bool kPerVertex = false;
+  __device__ void put(uint32_t, const unsigned long long*) const {}
+};
+struct VertexSink {  // per-source counts by original id: vcounts[4 * id + type]
+  static constexpr bool kPerVertex = true;
+  unsigned long long* vcounts;
+  const uint32_t* verts;
+  __device__ void put(uint32_t u, const unsigned long long* c) const {
+#pragma unroll
+    for (int k = 0; k < 4; k++) vcounts[4ull * verts[u] + (3 - k)] = c[k];
+  }
+};
+struct GraphSink {  // per-graph counts of a batch: gcounts[4 * graph + type]
+  static constexpr bool kPerVertex = true;
+  unsigned long long* gcounts;
+  const uint64_t* gbase;  // G + 1 rank boundaries (graphs are contiguous in rank space)
+  uint32_t G;
+  __device__ uint32_t graph_of(uint32_t u) const {
+    uint32_t lo = 0, hi = G;
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (gbase[mid] <= u) lo = mid; else hi = mid;
+    }
+    return lo;
+  }
+  __device__ void put(uint32_t u, const unsigned long long* c) const {
+    const uint32_t g = graph_of(u);
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      if (c[k]) atomicAdd(gcounts + 4ull * g + (3 - k), c[k]);
+  }
+};
+
+// Reduces one vertex's counters over the CTA and hands them to the sink.
+template <int THREADS, class Sink>
+__device__ __forceinline__ void block_vertex_flush(const TypeCounts& vc, uint32_t u, const Sink& sink) {
   __shared__ unsigned long long red[THREADS / 32][4];
   const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
 #pragma unroll
@@ -455,21 +489,22 @@ __device__ __forceinline__ void block_vertex_flush(const TypeCounts& vc, uint32_
     if (lane == 0) red[warp][k] = v;
   }
   __syncthreads();
-  if (threadIdx.x < 4) {
-    unsigned long long s = 0;
-    for (int w = 0; w < THREADS / 32; w++) s += red[w][threadIdx.x];
-    vcounts[4ull * g.verts[u] + (3 - threadIdx.x)] = s;
+  if (threadIdx.x == 0) {
+    unsigned long long s[4] = {0, 0, 0, 0};
+    for (int w = 0; w < THREADS / 32; w++)
+      for (int k = 0; k < 4; k++) s[k] += red[w][k];
+    sink.put(u, s);
   }
   __syncthreads();
 }
 
-__device__ __forceinline__ void warp_vertex_flush(const TypeCounts& vc, uint32_t u, const Csr& g,
-                                                  uint32_t lane, unsigned long long* __restrict__ vcounts) {
+template <class Sink>
+__device__ __forceinline__ void warp_vertex_flush(const TypeCounts& vc, uint32_t u, uint32_t lane,
+                                                  const Sink& sink) {
+  unsigned long long s[4];
 #pragma unroll
-  for (int k = 0; k < 4; k++) {
-    const unsigned long long s = warp_sum(vc.c[k]);
-    if (lane == 0) vcounts[4ull * g.verts[u] + (3 - k)] = s;
-  }
+  for (int k = 0; k < 4; k++) s[k] = warp_sum(vc.c[k]);
+  if (lane == 0) sink.put(u, s);
 }
 
 // ------------------------------------------------------------ classes ----
@@ -525,10 +560,10 @@ __global__ void k_classify_fill(const uint64_t* __restrict__ off, uint32_t n, Cl
 }
 
 // Tiny class: one thread per vertex, A in registers, B in global memory.
-template <int TMAX, bool kVC>
+template <int TMAX, class Sink>
 __global__ void __launch_bounds__(256) k_tiny(Csr g, const uint32_t* __restrict__ list, uint32_t cnt,
-                                              unsigned long long* __restrict__ ctr,
-                                              unsigned long long* __restrict__ vcounts) {
+                                              unsigned long long* __restrict__ ctr, Sink sink) {
+  constexpr bool kVC = Sink::kPerVertex;
   TypeCounts tc;
   for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < cnt; idx += gridDim.x * blockDim.x) {
     const uint32_t u = list[idx];
@@ -560,10 +595,7 @@ __global__ void __launch_bounds__(256) k_tiny(Csr g, const uint32_t* __restrict_
         }
       }
     }
-    if (kVC) {
-#pragma unroll
-      for (int k = 0; k < 4; k++) vcounts[4ull * g.verts[u] + (3 - k)] = vc.c[k];
-    }
+    if (kVC) sink.put(u, vc.c);
   }
   if (!kVC) flush_counts<256>(tc, ctr);
 }
@@ -573,11 +605,11 @@ __global__ void __launch_bounds__(256) k_tiny(Csr g, const uint32_t* __restrict_
 constexpr uint32_t kWarpBuckets = 2 * kWarpCap;
 constexpr size_t kWarpStageBytes = (StageMem::bytes(kWarpCap, kWarpBuckets) + 15) & ~size_t(15);
 
-template <bool kVC>
+template <class Sink>
 __global__ void __launch_bounds__(256) k_warp(Csr g, const uint32_t* __restrict__ list, uint32_t cnt,
-                                              unsigned long long* __restrict__ ctr,
-                                              unsigned long long* __restrict__ vcounts,
+                                              unsigned long long* __restrict__ ctr, Sink sink,
                                               const uint8_t* __restrict__ gtable) {
+  constexpr bool kVC = Sink::kPerVertex;
   constexpr int kWarps = 8;
   __shared__ __align__(16) unsigned char smem[kWarps * kWarpStageBytes];
   __shared__ uint8_t table[16][16];
@@ -604,7 +636,7 @@ __global__ void __launch_bounds__(256) k_warp(Csr g, const uint32_t* __restrict_
     stream_pass<kStreamUnroll>(g, m, d, 0, 1, lane, geo, pc, out);
     search_pass(g, m, d, 0, 1, lane, pc, out);
     pc.drain(out);
-    if (kVC) warp_vertex_flush(vc, u, g, lane, vcounts);
+    if (kVC) warp_vertex_flush(vc, u, lane, sink);
     __syncwarp();
   }
   if (!kVC) flush_counts<256>(tc, ctr);
@@ -615,13 +647,13 @@ __global__ void __launch_bounds__(256) k_warp(Csr g, const uint32_t* __restrict_
 // (nb >= 2 * cap, powers of two).
 inline size_t block_stage_bytes(uint32_t cap, uint32_t nb) { return StageMem::bytes(cap, nb); }
 
-template <int THREADS, bool kVC>
+template <int THREADS, class Sink>
 __global__ void __launch_bounds__(THREADS) k_block(Csr g, const uint32_t* __restrict__ list,
                                                    uint32_t cnt, uint32_t cap, uint32_t nb,
                                                    unsigned long long* __restrict__ queue,
-                                                   unsigned long long* __restrict__ ctr,
-                                                   unsigned long long* __restrict__ vcounts,
+                                                   unsigned long long* __restrict__ ctr, Sink sink,
                                                    const uint8_t* __restrict__ gtable) {
+  constexpr bool kVC = Sink::kPerVertex;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ uint8_t table[16][16];
   __shared__ uint32_t scan_tmp[THREADS / 32 + 1];
@@ -653,19 +685,19 @@ __global__ void __launch_bounds__(THREADS) k_block(Csr g, const uint32_t* __rest
     stream_pass<kStreamUnroll>(g, m, d, w, kWarps, lane, geo, pc, out);
     search_pass(g, m, d, w, kWarps, lane, pc, out);
     pc.drain(out);
-    if (kVC) block_vertex_flush<THREADS>(vc, u, g, vcounts);
+    if (kVC) block_vertex_flush<THREADS>(vc, u, sink);
   }
   if (!kVC) flush_counts<THREADS>(tc, ctr);
 }
 
 // Giant lists (d > kLargeCap): one CTA per vertex, A read from global memory,
 // one arc per warp; HASH falls back to MERGE (no staged hash).
-template <int THREADS, bool kVC>
+template <int THREADS, class Sink>
 __global__ void __launch_bounds__(THREADS) k_giant(Csr g, const uint32_t* __restrict__ list,
                                                    uint32_t cnt, unsigned long long* __restrict__ queue,
-                                                   unsigned long long* __restrict__ ctr,
-                                                   unsigned long long* __restrict__ vcounts,
+                                                   unsigned long long* __restrict__ ctr, Sink sink,
                                                    const uint8_t* __restrict__ gtable) {
+  constexpr bool kVC = Sink::kPerVertex;
   __shared__ uint8_t table[16][16];
   __shared__ uint32_t s_item;
   for (int i = threadIdx.x; i < 256; i += THREADS) (&table[0][0])[i] = gtable[i];
@@ -699,7 +731,7 @@ __global__ void __launch_bounds__(THREADS) k_giant(Csr g, const uint32_t* __rest
         arc_merge_global(a, s, k + 1, d, s[k] < 0, g.nbr + vb, g.sgn + vb, blen, lane, out);
       }
     }
-    if (kVC) block_vertex_flush<THREADS>(vc, u, g, vcounts);
+    if (kVC) block_vertex_flush<THREADS>(vc, u, sink);
   }
   if (!kVC) flush_counts<THREADS>(tc, ctr);
 }
@@ -716,6 +748,52 @@ void fixed_table(uint8_t t[16][16]) {
     }
 }
 
+// Launches the class kernels for one sink kind.
+template <class Sink>
+void launch_classes(cudaStream_t st, const Csr& csr, const uint32_t* lists, const uint32_t* counts,
+                    const uint32_t* starts, uint32_t max_fdeg, unsigned long long* ctr,
+                    const uint8_t* d_table, const Sink& sink, int& launches) {
+  if (counts[0]) {
+    const uint32_t grid = std::min<uint32_t>((counts[0] + 255) / 256, kSMs * 8);
+    k_tiny<kTinyMax, Sink><<<grid, 256, 0, st>>>(csr, lists + starts[0], counts[0], ctr, sink);
+    launches++;
+  }
+  if (counts[1]) {
+    const uint32_t grid = std::min<uint32_t>((counts[1] + 7) / 8, kSMs * 8);
+    k_warp<Sink><<<grid, 256, 0, st>>>(csr, lists + starts[1], counts[1], ctr, sink, d_table);
+    launches++;
+  }
+  if (counts[2]) {
+    const uint32_t cap = kBlockCap, nb = 4 * kBlockCap;
+    const size_t smem = block_stage_bytes(cap, nb);
+    STC_CUDA(cudaFuncSetAttribute(k_block<256, Sink>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem));
+    const uint32_t grid = std::min<uint32_t>(counts[2], kSMs * 8);
+    k_block<256, Sink><<<grid, 256, smem, st>>>(csr, lists + starts[2], counts[2], cap, nb,
+                                                 ctr + C_WORK + 0, ctr, sink, d_table);
+    launches++;
+  }
+  if (counts[3]) {
+    // Capacity: the class's largest list rounded up to a power of two.
+    uint32_t cap = kBlockCap;
+    while (cap < std::min<uint32_t>(max_fdeg, kLargeCap)) cap <<= 1;
+    const uint32_t nb = 2 * cap;
+    const size_t smem = block_stage_bytes(cap, nb);
+    STC_CUDA(cudaFuncSetAttribute(k_block<512, Sink>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem));
+    const uint32_t grid = std::min<uint32_t>(counts[3], kSMs * 2);
+    k_block<512, Sink><<<grid, 512, smem, st>>>(csr, lists + starts[3], counts[3], cap, nb,
+                                                 ctr + C_WORK + 1, ctr, sink, d_table);
+    launches++;
+  }
+  if (counts[4]) {
+    const uint32_t grid = std::min<uint32_t>(counts[4], kSMs * 2);
+    k_giant<512, Sink><<<grid, 512, 0, st>>>(csr, lists + starts[4], counts[4], ctr + C_WORK + 2,
+                                              ctr, sink, d_table);
+    launches++;
+  }
+}
+
 }  // namespace
 
 void count_triangles(stc_ctx* c, const DeviceGraph& g, const CountConfig& cfg) {
@@ -723,8 +801,6 @@ void count_triangles(stc_ctx* c, const DeviceGraph& g, const CountConfig& cfg) {
   cudaStream_t st = c->stream;
   Csr csr{g.off, g.nbr, g.sgn, g.verts, g.n};
   unsigned long long* ctr = (unsigned long long*)counters(c);
-  const bool vc = cfg.vertex_counts != nullptr;
-  unsigned long long* vcounts = (unsigned long long*)cfg.vertex_counts;
 
   // Dispatch table.
   uint8_t table[16][16];
@@ -760,47 +836,14 @@ void count_triangles(stc_ctx* c, const DeviceGraph& g, const CountConfig& cfg) {
   STC_CUDA(cudaMemsetAsync(counters(c) + C_WORK, 0, 8 * sizeof(uint64_t), st));
   c->launches += 2;
 
-  if (counts[0]) {
-    const uint32_t grid = std::min<uint32_t>((counts[0] + 255) / 256, kSMs * 8);
-    if (vc) k_tiny<kTinyMax, true><<<grid, 256, 0, st>>>(csr, lists + starts[0], counts[0], ctr, vcounts);
-    else k_tiny<kTinyMax, false><<<grid, 256, 0, st>>>(csr, lists + starts[0], counts[0], ctr, vcounts);
-    c->launches++;
-  }
-  if (counts[1]) {
-    const uint32_t grid = std::min<uint32_t>((counts[1] + 7) / 8, kSMs * 8);
-    if (vc) k_warp<true><<<grid, 256, 0, st>>>(csr, lists + starts[1], counts[1], ctr, vcounts, d_table);
-    else k_warp<false><<<grid, 256, 0, st>>>(csr, lists + starts[1], counts[1], ctr, vcounts, d_table);
-    c->launches++;
-  }
-  if (counts[2]) {
-    const uint32_t cap = kBlockCap, nb = 4 * kBlockCap;
-    const size_t smem = block_stage_bytes(cap, nb);
-    auto kern = vc ? k_block<256, true> : k_block<256, false>;
-    STC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const uint32_t grid = std::min<uint32_t>(counts[2], kSMs * 8);
-    kern<<<grid, 256, smem, st>>>(csr, lists + starts[2], counts[2], cap, nb, ctr + C_WORK + 0, ctr,
-                                  vcounts, d_table);
-    c->launches++;
-  }
-  if (counts[3]) {
-    // Capacity: the class's largest list rounded up to a power of two.
-    uint32_t cap = kBlockCap;
-    while (cap < std::min<uint32_t>(max_fdeg, kLargeCap)) cap <<= 1;
-    const uint32_t nb = 2 * cap;
-    const size_t smem = block_stage_bytes(cap, nb);
-    auto kern = vc ? k_block<512, true> : k_block<512, false>;
-    STC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const uint32_t grid = std::min<uint32_t>(counts[3], kSMs * 2);
-    kern<<<grid, 512, smem, st>>>(csr, lists + starts[3], counts[3], cap, nb, ctr + C_WORK + 1, ctr,
-                                  vcounts, d_table);
-    c->launches++;
-  }
-  if (counts[4]) {
-    auto kern = vc ? k_giant<512, true> : k_giant<512, false>;
-    const uint32_t grid = std::min<uint32_t>(counts[4], kSMs * 2);
-    kern<<<grid, 512, 0, st>>>(csr, lists + starts[4], counts[4], ctr + C_WORK + 2, ctr, vcounts,
-                               d_table);
-    c->launches++;
+  if (cfg.vertex_counts) {
+    const VertexSink sink{(unsigned long long*)cfg.vertex_counts, g.verts};
+    launch_classes(st, csr, lists, counts, starts, max_fdeg, ctr, d_table, sink, c->launches);
+  } else if (cfg.graph_counts) {
+    const GraphSink sink{(unsigned long long*)cfg.graph_counts, g.gbase, g.G};
+    launch_classes(st, csr, lists, counts, starts, max_fdeg, ctr, d_table, sink, c->launches);
+  } else {
+    launch_classes(st, csr, lists, counts, starts, max_fdeg, ctr, d_table, TotalSink{}, c->launches);
   }
   STC_CUDA(cudaGetLastError());
 }
@@ -939,36 +982,36 @@ extern "C" stc_status stc_count_oriented_csr_noalloc(const uint64_t* d_offsets,
   const uint8_t* d_table = scr->table;
   if (counts[0]) {
     const uint32_t grid = std::min<uint32_t>((counts[0] + 255) / 256, kSMs * 8);
-    k_tiny<kTinyMax, false><<<grid, 256, 0, st>>>(csr, lists + starts[0], counts[0], ctr, nullptr);
+    k_tiny<kTinyMax, TotalSink><<<grid, 256, 0, st>>>(csr, lists + starts[0], counts[0], ctr, TotalSink{});
   }
   if (counts[1]) {
     const uint32_t grid = std::min<uint32_t>((counts[1] + 7) / 8, kSMs * 8);
-    k_warp<false><<<grid, 256, 0, st>>>(csr, lists + starts[1], counts[1], ctr, nullptr, d_table);
+    k_warp<TotalSink><<<grid, 256, 0, st>>>(csr, lists + starts[1], counts[1], ctr, TotalSink{}, d_table);
   }
   if (counts[2]) {
     const uint32_t cap = kBlockCap, nb = 4 * kBlockCap;
     const size_t smem = block_stage_bytes(cap, nb);
-    STC_NA(cudaFuncSetAttribute(k_block<256, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    STC_NA(cudaFuncSetAttribute(k_block<256, TotalSink>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)smem));
     const uint32_t grid = std::min<uint32_t>(counts[2], kSMs * 8);
-    k_block<256, false><<<grid, 256, smem, st>>>(csr, lists + starts[2], counts[2], cap, nb,
-                                                  ctr + C_WORK + 0, ctr, nullptr, d_table);
+    k_block<256, TotalSink><<<grid, 256, smem, st>>>(csr, lists + starts[2], counts[2], cap, nb,
+                                                  ctr + C_WORK + 0, ctr, TotalSink{}, d_table);
   }
   if (counts[3]) {
     uint32_t cap = kBlockCap;
     while (cap < std::min<uint32_t>(max_fdeg, kLargeCap)) cap <<= 1;
     const uint32_t nb = 2 * cap;
     const size_t smem = block_stage_bytes(cap, nb);
-    STC_NA(cudaFuncSetAttribute(k_block<512, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    STC_NA(cudaFuncSetAttribute(k_block<512, TotalSink>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)smem));
     const uint32_t grid = std::min<uint32_t>(counts[3], kSMs * 2);
-    k_block<512, false><<<grid, 512, smem, st>>>(csr, lists + starts[3], counts[3], cap, nb,
-                                                  ctr + C_WORK + 1, ctr, nullptr, d_table);
+    k_block<512, TotalSink><<<grid, 512, smem, st>>>(csr, lists + starts[3], counts[3], cap, nb,
+                                                  ctr + C_WORK + 1, ctr, TotalSink{}, d_table);
   }
   if (counts[4]) {
     const uint32_t grid = std::min<uint32_t>(counts[4], kSMs * 2);
-    k_giant<512, false><<<grid, 512, 0, st>>>(csr, lists + starts[4], counts[4], ctr + C_WORK + 2,
-                                               ctr, nullptr, d_table);
+    k_giant<512, TotalSink><<<grid, 512, 0, st>>>(csr, lists + starts[4], counts[4], ctr + C_WORK + 2,
+                                               ctr, TotalSink{}, d_table);
   }
   STC_NA(cudaGetLastError());
   STC_NA(cudaMemcpyAsync(slots, ctr, sizeof(slots), cudaMemcpyDeviceToHost, st));

@@ -35,7 +35,7 @@ enum BufId {
   B_WORK2,
   B_EXPORT_OFF, B_EXPORT_FDEG,
   B_VCOUNTS,
-  B_BATCH_META,
+  B_BATCH_META, B_BATCH_SPACE, B_BATCH_COUNTS,
   B_COUNT_
 };
 
@@ -124,6 +124,10 @@ struct DeviceGraph {
   uint32_t* nbr = nullptr;    // arcs: head vertex (rank), sorted within each list
   int8_t* sgn = nullptr;      // arcs: +1 / -1
   uint32_t* fdeg = nullptr;   // out-degree by rank
+  // Batches: G graphs whose vertices (ids and ranks) are contiguous; graph
+  // g owns [gbase[g], gbase[g + 1]).  G == 0 for a single graph.
+  uint32_t G = 0;
+  uint64_t* gbase = nullptr;
 };
 
 // Stage timing helper: records an event when the context is timing.
@@ -136,6 +140,11 @@ void build_graph(stc_ctx* c, const uint32_t* d_src, const uint32_t* d_dst, const
 void graph_from_forward_csr(stc_ctx* c, uint32_t n, uint64_t m, const uint64_t* d_off,
                             const uint32_t* d_edges, const int8_t* d_signs, const uint32_t* d_rank,
                             DeviceGraph& g);
+// Batch of G graphs stored back to back (host edge offsets h_eoff, G + 1
+// entries): the disjoint union with graph-major ranks; sets g.G / g.gbase.
+void build_graph_batch(stc_ctx* c, const uint32_t* d_src, const uint32_t* d_dst,
+                       const int8_t* d_sign, uint64_t m, const uint64_t* h_eoff, uint32_t G,
+                       DeviceGraph& g);
 // Forward CSR in the reference's id-space layout, copied to host arrays.
 void export_forward_csr(stc_ctx* c, const DeviceGraph& g, stc_forward_csr* out);
 
@@ -143,7 +152,8 @@ void export_forward_csr(stc_ctx* c, const DeviceGraph& g, stc_forward_csr* out);
 struct CountConfig {
   uint32_t strategy = STC_STRATEGY_AUTO;
   uint32_t dispatch = STC_DISPATCH_FIXED;
-  uint64_t* vertex_counts = nullptr;  // optional per-source counts (rank space, 4 per vertex)
+  uint64_t* vertex_counts = nullptr;  // optional per-source counts, 4 per vertex id
+  uint64_t* graph_counts = nullptr;   // optional per-graph counts of a batch, 4 per graph
 };
 void count_triangles(stc_ctx* c, const DeviceGraph& g, const CountConfig& cfg);
 

@@ -547,6 +547,55 @@ int stc_synth_batch_graph(const stc_batch_spec* s, stc_synth_graph* out) {
   }
 }
 
+int stc_synth_batch_packed(const stc_batch_spec* specs, uint32_t g_begin, uint32_t g_end,
+                           stc_synth_graph* out, uint64_t* offsets) {
+  if (!specs || !out || !offsets || g_end < g_begin) return 1;
+  const uint32_t cnt = g_end - g_begin;
+  std::vector<stc_synth_graph> parts(cnt);
+  std::vector<int> rc(cnt, 0);
+  // Graphs in parallel, each generated single-threaded.
+  const uint32_t saved = g_threads.load();
+  g_threads.store(1);
+  {
+    std::atomic<uint32_t> next{0};
+    const uint32_t T = std::max(1u, saved ? saved : std::thread::hardware_concurrency());
+    std::vector<std::thread> th;
+    for (uint32_t t = 0; t < std::min(T, std::max(1u, cnt)); t++)
+      th.emplace_back([&] {
+        for (uint32_t i = next++; i < cnt; i = next++) {
+          memset(&parts[i], 0, sizeof(parts[i]));
+          rc[i] = stc_synth_batch_graph(&specs[g_begin + i], &parts[i]);
+        }
+      });
+    for (auto& x : th) x.join();
+  }
+  g_threads.store(saved);
+  int status = 0;
+  uint64_t total = 0;
+  for (uint32_t i = 0; i < cnt; i++) {
+    if (rc[i]) status = rc[i];
+    offsets[i] = total;
+    total += parts[i].m;
+  }
+  offsets[cnt] = total;
+  if (!status) {
+    if (!alloc_graph(out, 0, total)) {
+      status = 4;
+    } else {
+      uint64_t nmax = 0;
+      for (uint32_t i = 0; i < cnt; i++) {
+        std::memcpy(out->src + offsets[i], parts[i].src, parts[i].m * sizeof(uint32_t));
+        std::memcpy(out->dst + offsets[i], parts[i].dst, parts[i].m * sizeof(uint32_t));
+        std::memcpy(out->sign + offsets[i], parts[i].sign, parts[i].m);
+        nmax = std::max(nmax, parts[i].n);
+      }
+      out->n = nmax;
+    }
+  }
+  for (auto& pt : parts) stc_synth_free(&pt);
+  return status;
+}
+
 uint64_t stc_synth_workload_seed(int workload) { return 1000ull + (uint64_t)workload; }
 
 int stc_synth_workload(int workload, uint32_t shrink, stc_synth_graph* out) {

@@ -85,3 +85,26 @@ def batch_graph(spec: dict) -> EdgeList:
     s = _capi.stc_batch_spec(spec["seed"], spec["n"], spec["kind"], spec["rmat_scale"],
                              spec["m_target"], spec["p_pos"])
     return _call(lib().stc_synth_batch_graph, C.byref(s))
+
+
+def _spec_array(specs):
+    arr = (_capi.stc_batch_spec * max(1, len(specs)))()
+    for i, sp in enumerate(specs):
+        arr[i] = _capi.stc_batch_spec(sp["seed"], sp["n"], sp["kind"], sp["rmat_scale"],
+                                      sp["m_target"], sp["p_pos"])
+    return arr
+
+
+def batch_packed(specs: list, g_begin: int = 0, g_end: int | None = None):
+    """Graphs [g_begin, g_end) of a batch generated in parallel and packed back
+    to back: (EdgeList of all their edges, offsets with g_end - g_begin + 1
+    entries)."""
+    g_end = len(specs) if g_end is None else g_end
+    arr = _spec_array(specs)
+    offs = np.zeros(g_end - g_begin + 1, np.uint64)
+    g = _capi.stc_synth_graph()
+    st = lib().stc_synth_batch_packed(arr, g_begin, g_end, C.byref(g),
+                                      offs.ctypes.data_as(_capi.u64p))
+    if st != 0:
+        raise ValueError(f"batch generator failed (status {st})")
+    return _take(g), offs

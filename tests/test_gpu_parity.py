@@ -236,3 +236,68 @@ def test_cli_matches_reference_output(golden, text_dir):
             assert got[k] == s[k], (name, k)
         for k in ("balanced", "unbalanced", "total"):
             assert got[k] == mg[k], (name, k)
+
+
+def _mixed_batch(count: int):
+    graphs = []
+    for i in range(count):
+        kind = i % 7
+        if kind == 0:
+            el = synth.er(100 + i, 300 + 37 * i, 1500 + 90 * i, 0.3 + 0.01 * i)
+        elif kind == 1:
+            el = synth.rmat(100 + i, 9, 400 + i, 3000 + 50 * i, p_pos=0.5)
+        elif kind == 2:
+            el = synth.delaunay(100 + i, 500 + 40 * i, 0.2, 0.6)
+        elif kind == 3:
+            el = synth.skew(100 + i, 4096, 6000, 3, 100, 900, 0.8)
+        elif kind == 4:  # empty graph
+            el = stc.EdgeList(0, 0, np.zeros(0, np.uint32), np.zeros(0, np.uint32), np.zeros(0, np.int8))
+        elif kind == 5:  # self-loops only, large ids
+            ids = np.array([70000, 5, 9], np.uint32)
+            el = stc.EdgeList(70001, 3, ids, ids.copy(), np.array([1, -1, 1], np.int8))
+        else:  # reversed duplicates
+            b = synth.er(100 + i, 200, 1200, 0.5)
+            el = stc.EdgeList(b.n, 2 * b.m, np.concatenate([b.src, b.dst]),
+                              np.concatenate([b.dst, b.src]), np.concatenate([b.sign, b.sign]))
+        graphs.append(el)
+    return graphs
+
+
+def test_batch_packed_against_oracle(ctx):
+    graphs = _mixed_batch(63)
+    offs = np.zeros(len(graphs) + 1, np.uint64)
+    offs[1:] = np.cumsum([g.m for g in graphs])
+    src = np.concatenate([g.src for g in graphs]).astype(np.uint32)
+    dst = np.concatenate([g.dst for g in graphs]).astype(np.uint32)
+    sign = np.concatenate([g.sign for g in graphs]).astype(np.int8)
+    for strategy in STRATEGIES:
+        got = ctx.count_batch_packed(src, dst, sign, offs, strategy=strategy)
+        for g, c in zip(graphs, got):
+            assert c.as_tuple() == oracle.count_arrays(g.src, g.dst, g.sign), strategy
+
+
+def test_batch_workload_full(ctx, golden):
+    """The 4,096-graph workload against the reference's per-graph counts."""
+    import torch
+    b = golden.get("batch")
+    if b is None:
+        pytest.skip("no batch golden entry")
+    specs = synth.batch_specs(b["G"])
+    M = sum(b["m_input"])
+    src = torch.empty(M, dtype=torch.int32, device="cuda")
+    dst = torch.empty(M, dtype=torch.int32, device="cuda")
+    sign = torch.empty(M, dtype=torch.int8, device="cuda")
+    offs = np.zeros(b["G"] + 1, np.uint64)
+    pos = 0
+    for g0 in range(0, b["G"], 256):
+        g1 = min(b["G"], g0 + 256)
+        el, o = synth.batch_packed(specs, g0, g1)
+        offs[g0:g1 + 1] = o + pos
+        src[pos:pos + el.m] = torch.from_numpy(el.src.view(np.int32)).cuda()
+        dst[pos:pos + el.m] = torch.from_numpy(el.dst.view(np.int32)).cuda()
+        sign[pos:pos + el.m] = torch.from_numpy(el.sign).cuda()
+        pos += el.m
+    assert pos == M
+    assert [int(x) for x in np.diff(offs)] == b["m_input"]
+    got = ctx.count_batch_packed(src, dst, sign, offs)
+    assert [list(c.as_tuple()) for c in got] == b["t"]

@@ -241,3 +241,15 @@ def test_cli_missing_file():
     r = subprocess.run([str(CLI), "/nonexistent/g.txt"], capture_output=True, text=True)
     assert r.returncode == 1
     assert "/nonexistent/g.txt" in r.stderr
+
+
+def test_batch_packed_generator_matches_single_graphs():
+    specs = synth.batch_specs(64)
+    el, offs = synth.batch_packed(specs, 10, 22)
+    assert len(offs) == 13 and offs[0] == 0 and offs[-1] == el.m
+    for i, g in enumerate(range(10, 22)):
+        one = synth.batch_graph(specs[g])
+        a, b = int(offs[i]), int(offs[i + 1])
+        np.testing.assert_array_equal(el.src[a:b], one.src)
+        np.testing.assert_array_equal(el.dst[a:b], one.dst)
+        np.testing.assert_array_equal(el.sign[a:b], one.sign)
