@@ -239,6 +239,7 @@ def run_gpu(args) -> None:
     else:
         torch.cuda.set_device(local)
     ctx = stc.Context(local)
+    model = ctx.load_dispatch_model() if args.dispatch == "learned" else None
     stream = torch.cuda.current_stream(local)
     wl = make_device_workload(ctx, args.workload, rank, torch, args.rmat_scale)
     src, dst, sign = wl[:3]
@@ -369,7 +370,9 @@ def run_gpu(args) -> None:
                        f"RMAT scale {args.rmat_scale}, edge factor 16, (.57,.19,.19,.05), p(+)=0.5",
                        "m_input": m_input,
                        "m_unique": edges, "n": st.n, "strategy": args.strategy,
-                       "dispatch": args.dispatch, "l2": f"inputs {m_input * 9 / 1e9:.1f} GB > 126 MB L2, no flush",
+                       "dispatch": args.dispatch,
+                       "dispatch_model": model.get("trained_on") if model else None,
+                       "l2": f"inputs {m_input * 9 / 1e9:.1f} GB > 126 MB L2, no flush",
                        "parallelism": f"{world} rank(s), one graph instance each"},
             "exact": exact, "counts": counts_out,
             "stage_ms": {"dedup": st.ms_dedup, "orient": st.ms_orient, "csr": st.ms_csr,

@@ -225,6 +225,61 @@ stc_status stc_count_batch_packed(stc_ctx* ctx, const uint32_t* src, const uint3
                                   const int8_t* sign, const uint64_t* offsets, uint32_t G,
                                   const stc_opts* opts, stc_counts* outs);
 
+/* ----------------------------------------------------------- dispatcher ---- */
+/* No counterpart in the reference, whose programs each run one strategy
+ * (merge in MC/tc_merge_sign_enu.cpp, hash in MC/tc_hash_sign_enu.cpp).
+ * Every arc u -> v falls in a dispatch cell: the class of u's list (0 = warp,
+ * |N+(u)| <= 128; 1 = block, <= 1024; 2 = large, <= 4096; 3 = giant) and the
+ * buckets a = min(15, bit width of |A'|), b = min(15, bit width of |B|),
+ * where A' is the part of N+(u) after v and B = N+(v).  Cell index =
+ * 256 class + 16 a + b.  A dispatch table holds one stc_strategy per cell;
+ * all strategies give the same counts, so a table changes only speed. */
+#define STC_DISPATCH_CELLS 1024
+#define STC_DISPATCH_FEATURES 6
+#define STC_DISPATCH_MODEL_PARAMS 163
+
+/* Timing recorder: the whole path as stc_count (opts->strategy is usually
+ * forced to one strategy), with every arc of the staged and giant classes
+ * processed alone by one warp and timed.  cycles[cell] receives the SM
+ * cycles spent on the cell's arcs and arcs[cell] their number
+ * (STC_DISPATCH_CELLS words each).  Lists of 8 or fewer arcs, which are
+ * otherwise counted one thread per list, join the warp class here, so that
+ * runs with different forced strategies time the same arcs.  `out` receives
+ * the counts, which equal stc_count's. */
+stc_status stc_record_bucket_times(stc_ctx* ctx, const uint32_t* src, const uint32_t* dst,
+                                   const int8_t* sign, uint64_t m, const stc_opts* opts,
+                                   uint64_t* cycles, uint64_t* arcs, stc_counts* out);
+
+/* Input features of every cell (STC_DISPATCH_CELLS x STC_DISPATCH_FEATURES
+ * floats, row-major), computed on the host: the log-bucketed lengths a and
+ * b, their difference (the log of the |B| / |A'| ratio), a log-degree
+ * representative of u's class and its difference to b (the log of the
+ * deg(u) / deg(v) ratio), and whether the class stages a hash, each scaled
+ * to about [-1, 1]. */
+stc_status stc_dispatch_features(float* out);
+
+/* Trains the dispatcher's perceptron (STC_DISPATCH_FEATURES inputs, 16
+ * hidden ReLU units, one logit per strategy MERGE / HASH / SEARCH) on the
+ * device: full-batch Adam over `samples` rows of `features`, labels 0..2 (=
+ * strategy - 1) and non-negative weights, minimising the weighted softmax
+ * cross-entropy.  Deterministic for a given seed.  `params` receives the
+ * STC_DISPATCH_MODEL_PARAMS trained parameters (W1[16][6], b1[16], W2[3][16],
+ * b2[3]) and `loss` (optional) the final weighted loss.  samples <= 4096. */
+stc_status stc_dispatcher_train(stc_ctx* ctx, const float* features, const int32_t* labels,
+                                const float* weights, uint32_t samples, uint32_t epochs,
+                                float learning_rate, uint64_t seed, float* params, float* loss);
+
+/* Loads a trained model into the context: an inference kernel evaluates it
+ * on every cell and writes the learned tables on the device, which calls
+ * with dispatch STC_DISPATCH_LEARNED then use (the giant class, which stages
+ * no hash, never gets HASH).  NULL unloads it; without a model, LEARNED falls
+ * back to the fixed tables. */
+stc_status stc_ctx_set_dispatch_model(stc_ctx* ctx, const float* params);
+
+/* Copies to `out` (STC_DISPATCH_CELLS bytes) the tables a call with
+ * strategy AUTO and this dispatch would use on this context. */
+stc_status stc_dispatch_tables(stc_ctx* ctx, uint32_t dispatch, uint8_t* out);
+
 /* --------------------------------------------------- device generator ---- */
 /* Writes the RMAT samples of stc_synth_rmat (include/stc_synth.h) for the
  * same arguments directly into device arrays of `samples` elements. */

@@ -21,7 +21,7 @@ from ._capi import lib
 
 __all__ = [
     "GlobalTriCounts", "EdgeList", "ForwardCSR", "Stats", "StcError", "Context",
-    "load_graph", "parse_edge_text", "synth",
+    "load_graph", "parse_edge_text", "dispatch_features", "synth",
 ]
 
 
@@ -329,6 +329,67 @@ class Context:
                                             outs), self._h)
         return [GlobalTriCounts(x.t0, x.t1, x.t2, x.t3) for x in outs[:G]]
 
+    # ------------------------------------------------------------ dispatcher
+    def record_bucket_times(self, src, dst, sign, *, strategy="auto", dispatch="fixed"):
+        """Timing recorder: counts like ``count`` with every arc timed alone.
+
+        Returns (cycles, arcs, counts): per dispatch cell (``DISPATCH_CELLS``,
+        index 256 class + 16 bucket|A'| + bucket|B|) the SM cycles spent on its
+        arcs and their number, and the per-type counts."""
+        src, dst, sign = _host_arrays(src, dst, sign)
+        cycles = np.zeros(_capi.DISPATCH_CELLS, np.uint64)
+        arcs = np.zeros(_capi.DISPATCH_CELLS, np.uint64)
+        out = _capi.stc_counts()
+        o = self._opts(strategy, dispatch)
+        _check(lib().stc_record_bucket_times(self._h, _ptr(src), _ptr(dst), _ptr(sign), len(src),
+                                             C.byref(o), cycles.ctypes.data_as(_capi.u64p),
+                                             arcs.ctypes.data_as(_capi.u64p), C.byref(out)),
+               self._h)
+        return cycles, arcs, GlobalTriCounts(out.t0, out.t1, out.t2, out.t3)
+
+    def train_dispatcher(self, features, labels, weights, *, epochs=3000, lr=0.02, seed=1):
+        """Trains the dispatcher's perceptron on the device; returns
+        (parameters, final weighted loss)."""
+        X = np.ascontiguousarray(features, np.float32)
+        y = np.ascontiguousarray(labels, np.int32)
+        w = np.ascontiguousarray(weights, np.float32)
+        if X.ndim != 2 or X.shape[1] != _capi.DISPATCH_FEATURES or not (len(X) == len(y) == len(w)):
+            raise ValueError("features must be (samples, DISPATCH_FEATURES) with matching labels/weights")
+        params = np.zeros(_capi.DISPATCH_MODEL_PARAMS, np.float32)
+        loss = C.c_float()
+        _check(lib().stc_dispatcher_train(self._h, X.ctypes.data_as(_capi.f32p),
+                                          y.ctypes.data_as(_capi.i32p), w.ctypes.data_as(_capi.f32p),
+                                          len(X), epochs, lr, seed,
+                                          params.ctypes.data_as(_capi.f32p), C.byref(loss)), self._h)
+        return params, float(loss.value)
+
+    def set_dispatch_model(self, params) -> None:
+        """Loads a model (``DISPATCH_MODEL_PARAMS`` floats) for dispatch="learned";
+        None unloads it (learned then falls back to the fixed tables)."""
+        if params is None:
+            _check(lib().stc_ctx_set_dispatch_model(self._h, None), self._h)
+            return
+        p = np.ascontiguousarray(params, np.float32)
+        if p.shape != (_capi.DISPATCH_MODEL_PARAMS,):
+            raise ValueError(f"a model has {_capi.DISPATCH_MODEL_PARAMS} parameters")
+        _check(lib().stc_ctx_set_dispatch_model(self._h, p.ctypes.data_as(_capi.f32p)), self._h)
+
+    def load_dispatch_model(self, path=None) -> dict:
+        """Loads a model file written by ``dispatcher.save`` (default: the
+        model shipped with the package) and returns its metadata."""
+        from . import dispatcher
+        model = dispatcher.load(path)
+        self.set_dispatch_model(model["params"])
+        return model
+
+    def dispatch_tables(self, dispatch="fixed") -> np.ndarray:
+        """The tables (class, bucket|A'|, bucket|B|) -> strategy code that a call
+        with strategy="auto" and this dispatch uses, as a (4, 16, 16) array."""
+        t = np.zeros(_capi.DISPATCH_CELLS, np.uint8)
+        _check(lib().stc_dispatch_tables(self._h, _capi.DISPATCH[dispatch],
+                                         t.ctypes.data_as(_capi.u8p)), self._h)
+        return t.reshape(4, 16, 16)
+
     def last_stats(self) -> Stats:
         s = _capi.stc_stats()
         _check(lib().stc_ctx_last_stats(self._h, C.byref(s)))
@@ -339,6 +400,14 @@ class Context:
         """Fills device arrays (torch tensors) with stc_synth_rmat's samples."""
         _check(lib().stc_synth_rmat_device(self._h, seed, scale, n, samples, a, b, c, p_pos,
                                            _ptr(src), _ptr(dst), _ptr(sign)), self._h)
+
+
+def dispatch_features() -> np.ndarray:
+    """Features of every dispatch cell, (DISPATCH_CELLS, DISPATCH_FEATURES)
+    float32, as the dispatcher's inference kernel computes them."""
+    f = np.zeros((_capi.DISPATCH_CELLS, _capi.DISPATCH_FEATURES), np.float32)
+    _check(lib().stc_dispatch_features(f.ctypes.data_as(_capi.f32p)))
+    return f
 
 
 from . import synth  # noqa: E402  (needs the names above)

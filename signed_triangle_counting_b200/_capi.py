@@ -15,6 +15,8 @@ u8p = C.POINTER(C.c_uint8)
 u32p = C.POINTER(C.c_uint32)
 u64p = C.POINTER(C.c_uint64)
 i8p = C.POINTER(C.c_int8)
+i32p = C.POINTER(C.c_int32)
+f32p = C.POINTER(C.c_float)
 
 
 class stc_counts(C.Structure):
@@ -69,6 +71,9 @@ STC_ERR_NO_DEVICE = 7
 STC_ERR_INTERNAL = 8
 
 STRATEGY = {"auto": 0, "merge": 1, "hash": 2, "search": 3}
+DISPATCH_CELLS = 1024
+DISPATCH_FEATURES = 6
+DISPATCH_MODEL_PARAMS = 163
 DISPATCH = {"fixed": 0, "learned": 1}
 F_DEVICE_INPUT = 0x1
 F_TIMING = 0x2
@@ -103,6 +108,14 @@ SIGNATURES = [
                                          C.POINTER(stc_counts)]),
     ("stc_count_oriented_csr_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                                  C.c_uint64, C.c_void_p, C.POINTER(stc_counts)]),
+    ("stc_record_bucket_times", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_uint64, C.POINTER(stc_opts), u64p, u64p,
+                                          C.POINTER(stc_counts)]),
+    ("stc_dispatch_features", C.c_int, [f32p]),
+    ("stc_dispatcher_train", C.c_int, [C.c_void_p, f32p, i32p, f32p, C.c_uint32, C.c_uint32,
+                                       C.c_float, C.c_uint64, f32p, f32p]),
+    ("stc_ctx_set_dispatch_model", C.c_int, [C.c_void_p, f32p]),
+    ("stc_dispatch_tables", C.c_int, [C.c_void_p, C.c_uint32, u8p]),
     ("stc_synth_rmat_device", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint64,
                                         C.c_uint64, C.c_double, C.c_double, C.c_double,
                                         C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]),

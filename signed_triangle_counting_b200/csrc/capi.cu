@@ -466,6 +466,67 @@ stc_status stc_count_batch(stc_ctx* c, const stc_graph* graphs, uint32_t G, cons
                                 &o2, outs);
 }
 
+stc_status stc_record_bucket_times(stc_ctx* c, const uint32_t* src, const uint32_t* dst,
+                                   const int8_t* sign, uint64_t m, const stc_opts* o,
+                                   uint64_t* cycles, uint64_t* arcs, stc_counts* out) {
+  if (!c || !cycles || !arcs || !out) return STC_ERR_INVALID_ARGUMENT;
+  return guarded(c, [&] {
+    CountConfig cfg = count_config(o);
+    begin_call(c, o);
+    uint64_t* times = buffer<uint64_t>(c, B_TIMES, 2 * kTableBytes);
+    STC_CUDA(cudaMemsetAsync(times, 0, 2 * kTableBytes * sizeof(uint64_t), c->stream));
+    cfg.arc_cycles = times;
+    cfg.arc_counts = times + kTableBytes;
+    DeviceInput in = stage_input(c, src, dst, sign, m, o);
+    DeviceGraph g;
+    build_graph(c, in.src, in.dst, in.sign, m, g);
+    count_triangles(c, g, cfg);
+    mark(c, 5);
+    STC_CUDA(cudaMemcpyAsync(cycles, times, kTableBytes * sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                             c->stream));
+    STC_CUDA(cudaMemcpyAsync(arcs, times + kTableBytes, kTableBytes * sizeof(uint64_t),
+                             cudaMemcpyDeviceToHost, c->stream));
+    end_call(c, g, out);
+  });
+}
+
+stc_status stc_dispatch_features(float* out) {
+  if (!out) return STC_ERR_INVALID_ARGUMENT;
+  dispatch_features(out);
+  return STC_OK;
+}
+
+stc_status stc_dispatcher_train(stc_ctx* c, const float* features, const int32_t* labels,
+                                const float* weights, uint32_t samples, uint32_t epochs,
+                                float learning_rate, uint64_t seed, float* params, float* loss) {
+  if (!c) return STC_ERR_INVALID_ARGUMENT;
+  return guarded(c, [&] {
+    c->stream = c->own_stream;
+    train_dispatcher(c, features, labels, weights, samples, epochs, learning_rate, seed, params,
+                     loss);
+  });
+}
+
+stc_status stc_ctx_set_dispatch_model(stc_ctx* c, const float* params) {
+  if (!c) return STC_ERR_INVALID_ARGUMENT;
+  return guarded(c, [&] {
+    c->stream = c->own_stream;
+    load_dispatch_model(c, params);
+  });
+}
+
+stc_status stc_dispatch_tables(stc_ctx* c, uint32_t dispatch, uint8_t* out) {
+  if (!c || !out || dispatch > STC_DISPATCH_LEARNED) return STC_ERR_INVALID_ARGUMENT;
+  return guarded(c, [&] {
+    c->stream = c->own_stream;
+    CountConfig cfg;
+    cfg.dispatch = dispatch;
+    const uint8_t* t = dispatch_tables(c, cfg);
+    STC_CUDA(cudaMemcpyAsync(out, t, kTableBytes, cudaMemcpyDeviceToHost, c->stream));
+    STC_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
 stc_status stc_synth_rmat_device(stc_ctx* c, uint64_t seed, uint32_t scale, uint64_t n,
                                  uint64_t samples, double a, double b, double cc, double p_pos,
                                  uint32_t* d_src, uint32_t* d_dst, int8_t* d_sign) {

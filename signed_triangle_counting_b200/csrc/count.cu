@@ -18,11 +18,11 @@
 //   block  d <= 1024          one CTA per vertex      } shared memory
 //   large  d <= 4096          one 512-thread CTA      }
 //   giant  larger             one CTA per vertex, A read from global memory
-// A 16x16 dispatch table indexed by (bucket |A'|, bucket |B|) picks each
-// arc's strategy:
-//   HASH    B is streamed and every element is tested against a shared-memory
-//           bitmap filter of N+(u); the few that pass are checked exactly in
-//           a shared-memory hash of N+(u)
+// A 16x16 dispatch table per class (warp, block, large, giant) indexed by
+// (bucket |A'|, bucket |B|) picks each arc's strategy:
+//   HASH    B is streamed and every element is looked up in a shared-memory
+//           hash of N+(u) whose keys carry the sign, so one 8-byte bucket
+//           read answers membership and the A' sign together
 //   MERGE   B is streamed and each 16-byte chunk is located in the staged
 //           sorted A' by one binary search, its four keys merged forward
 //   SEARCH  a warp takes the arc: each lane holds one pivot of B, an A'
@@ -105,11 +105,7 @@ __device__ __forceinline__ uint32_t lower_bound(const uint32_t* a, uint32_t len,
   return lo;
 }
 
-// Bitmap filter index and hash slot use different multipliers so that a
-// filter false positive is not correlated with a hash collision.
-__device__ __forceinline__ uint32_t bit_index(uint32_t x, uint32_t shift) {
-  return (x * 0x9E3779B1u) >> shift;
-}
+// Multiplicative hash: the top bits of x * an odd constant.
 __device__ __forceinline__ uint32_t hash_slot(uint32_t x, uint32_t shift) {
   return (x * 0x85EBCA77u) >> shift;
 }
@@ -143,11 +139,12 @@ __device__ __forceinline__ void arc_search(const uint32_t* a, const int8_t* s, u
 
 // MERGE for one arc by one warp over B streamed in int4 chunks (giant lists,
 // whose A stays in global memory).
+template <class Counts>
 __device__ __forceinline__ void arc_merge_global(const uint32_t* a, const int8_t* s, uint32_t a0,
                                                  uint32_t d, uint32_t nuv,
                                                  const uint32_t* __restrict__ b,
                                                  const int8_t* __restrict__ sb, uint32_t blen,
-                                                 uint32_t lane, TypeCounts& tc) {
+                                                 uint32_t lane, Counts& tc) {
   const uint32_t alen = d - a0;
   const uint32_t alast = a[d - 1];
   for (uint32_t base = 0; base < blen; base += 128) {
@@ -307,6 +304,53 @@ __device__ __forceinline__ uint32_t pick4(const uint4& q, uint32_t e) {
   return (e & 2) ? hi : lo;
 }
 
+// Mask of the entries of int4 chunk ci (elements 4 ci .. 4 ci + 3) that lie
+// inside the arc's extent [lo, hi).
+__device__ __forceinline__ uint32_t chunk_mask(uint32_t ci, uint32_t lo, uint32_t hi) {
+  const uint32_t g0 = 4 * ci;
+  const uint32_t first = lo > g0 ? lo - g0 : 0;
+  const uint32_t last = min(hi - g0, 4u);
+  return ((1u << last) - 1) & ~((1u << first) - 1);
+}
+
+// One int4 chunk of B for arc k of a staged list: four ids q, their four sign
+// bytes sw, and the mask vm (non-zero) of the ids inside the arc.  HASH looks
+// every id up in the staged hash (one 8-byte bucket read gives membership and
+// the A' sign); MERGE locates the chunk in the sorted A' = a[k+1 ..) by one
+// binary search and merges its ascending ids forward.
+__device__ __forceinline__ void process_chunk(const StageMem& m, uint32_t d, const Geo& geo,
+                                              const uint4& q, uint32_t sw, uint32_t vm, uint32_t k,
+                                              uint32_t nuv, uint32_t st, PackedCounts& pc) {
+  if (st == STC_STRATEGY_HASH) {
+#pragma unroll
+    for (uint32_t e = 0; e < 4; e++) {
+      const uint32_t x = pick4(q, e);
+      const uint32_t b = hash_slot(x, geo.shift);
+      const uint2 w = *reinterpret_cast<const uint2*>(m.hk + 2 * b);
+      const bool m0 = (w.x & kIdMask) == x, m1 = (w.y & kIdMask) == x;
+      uint32_t hit = (m0 | m1) & (vm >> e) & 1u;
+      uint32_t na = (m0 ? w.x : w.y) >> 31;
+      if (!(m0 | m1) && w.y != kEmpty && ((vm >> e) & 1u)) {
+        const uint32_t r = probe_rest(m.hk, geo.nb, (b + 1) & (geo.nb - 1), x);
+        hit = r & 1u;
+        na = r >> 1;
+      }
+      const uint32_t nb = (sw >> (8 * e + 7)) & 1u;
+      if (hit) pc.add(nuv + na + nb);
+    }
+  } else {  // MERGE
+    const uint32_t a0 = k + 1, alen = d - a0;
+    const uint32_t* a = m.a + a0;
+    const uint32_t e0 = __ffs(vm) - 1;
+    uint32_t p = lower_bound(a, alen, pick4(q, e0));
+    for (uint32_t e = e0; e < 4 && ((vm >> e) & 1u); e++) {
+      const uint32_t x = pick4(q, e);
+      while (p < alen && a[p] < x) p++;
+      if (p < alen && a[p] == x) pc.add(nuv + (m.s[a0 + p] < 0) + ((sw >> (8 * e + 7)) & 1u));
+    }
+  }
+}
+
 // The streamed arcs of a staged list as one sequence of aligned int4
 // chunks.  Warp w takes a contiguous share of the sequence and its lanes
 // take consecutive chunks (coalesced); each lane keeps the extent of its
@@ -361,48 +405,15 @@ __device__ __forceinline__ void stream_pass(const Csr& g, const StageMem& m, uin
         const uint32_t ci = (alo >> 2) + (c - pk);
         q[u] = nbr4[ci];
         sw[u] = sgn4[ci];
-        const uint32_t g0 = 4 * ci;
-        const uint32_t first = alo > g0 ? alo - g0 : 0;
-        const uint32_t last = min(ahi - g0, 4u);
-        vm[u] = ((1u << last) - 1) & ~((1u << first) - 1);
+        vm[u] = chunk_mask(ci, alo, ahi);
         sk[u] = k;
         snuv[u] = anuv;
         sst[u] = ast;
       }
     }
 #pragma unroll
-    for (int u = 0; u < U; u++) {
-      if (vm[u] == 0) continue;
-      if (sst[u] == STC_STRATEGY_HASH) {
-#pragma unroll
-        for (uint32_t e = 0; e < 4; e++) {
-          const uint32_t x = pick4(q[u], e);
-          const uint32_t b = hash_slot(x, geo.shift);
-          const uint2 w = *reinterpret_cast<const uint2*>(m.hk + 2 * b);
-          const bool m0 = (w.x & kIdMask) == x, m1 = (w.y & kIdMask) == x;
-          uint32_t hit = (m0 | m1) & (vm[u] >> e) & 1u;
-          uint32_t na = (m0 ? w.x : w.y) >> 31;
-          if (!(m0 | m1) && w.y != kEmpty && ((vm[u] >> e) & 1u)) {
-            const uint32_t r = probe_rest(m.hk, geo.nb, (b + 1) & (geo.nb - 1), x);
-            hit = r & 1u;
-            na = r >> 1;
-          }
-          const uint32_t nb = (sw[u] >> (8 * e + 7)) & 1u;
-          if (hit) pc.add(snuv[u] + na + nb);
-        }
-      } else {  // MERGE: ids ascend within the chunk
-        const uint32_t a0 = sk[u] + 1, alen = d - a0;
-        const uint32_t* a = m.a + a0;
-        const uint32_t e0 = __ffs(vm[u]) - 1;
-        uint32_t p = lower_bound(a, alen, pick4(q[u], e0));
-        for (uint32_t e = e0; e < 4 && ((vm[u] >> e) & 1u); e++) {
-          const uint32_t x = pick4(q[u], e);
-          while (p < alen && a[p] < x) p++;
-          if (p < alen && a[p] == x)
-            pc.add(snuv[u] + (m.s[a0 + p] < 0) + ((sw[u] >> (8 * e + 7)) & 1u));
-        }
-      }
-    }
+    for (int u = 0; u < U; u++)
+      if (vm[u]) process_chunk(m, d, geo, q[u], sw[u], vm[u], sk[u], snuv[u], sst[u], pc);
     if (++rounds == 8000) {  // at most 4 * U adds per field per round
       pc.drain(tc);
       rounds = 0;
@@ -419,6 +430,72 @@ __device__ __forceinline__ void search_pass(const Csr& g, const StageMem& m, uin
     const uint32_t lo = m.lo[k];
     arc_search(m.a, m.s, k + 1, d, m.s[k] < 0, g.nbr + lo, g.sgn + lo, m.hi[k] - lo, lane, pc);
     pc.drain(tc);
+  }
+}
+
+// ------------------------------------------------------ arc timing ----
+// Timing recorder (CountConfig::arc_cycles): per dispatch cell
+// (class, bucket |A'|, bucket |B|), the SM cycles a warp spent on each arc
+// and the number of arcs.  In this mode every arc is processed alone by one
+// warp, timed from the first load of its B to the last count it adds, so
+// three runs with the strategy forced give every cell's cost under every
+// strategy: the training data of the learned dispatcher and the judge of a
+// dispatch table's regret.
+struct ArcTimes {
+  unsigned long long* cycles;  // kTableClasses * 256 cells
+  unsigned long long* arcs;
+};
+
+// SM clock read that the compiler cannot hoist above the computation of
+// `dep` (an input operand of the read).
+__device__ __forceinline__ long long clock_after(unsigned long long dep) {
+  long long t;
+  asm volatile("mov.u64 %0, %%clock64;" : "=l"(t) : "l"(dep) : "memory");
+  return t;
+}
+
+__device__ __forceinline__ void record_arc(const ArcTimes& at, uint32_t tclass, uint32_t alen,
+                                           uint32_t blen, unsigned cycles) {
+  const uint32_t cell = tclass * 256 + size_bucket(alen) * 16 + size_bucket(blen);
+  atomicAdd(at.cycles + cell, (unsigned long long)cycles);
+  atomicAdd(at.arcs + cell, 1ull);
+}
+
+// HASH or MERGE for arc k alone: the warp's lanes take consecutive int4
+// chunks of B.
+__device__ __forceinline__ void arc_stream(const Csr& g, const StageMem& m, uint32_t d, uint32_t k,
+                                           uint32_t lane, const Geo& geo, PackedCounts& pc) {
+  const uint4* __restrict__ nbr4 = reinterpret_cast<const uint4*>(g.nbr);
+  const uint32_t* __restrict__ sgn4 = reinterpret_cast<const uint32_t*>(g.sgn);
+  const uint32_t lo = m.lo[k], hi = m.hi[k], st = m.st[k], nuv = m.s[k] < 0;
+  const uint32_t c1 = (hi + 3) >> 2;
+  for (uint32_t ci = (lo >> 2) + lane; ci < c1; ci += 32) {
+    const uint4 q = nbr4[ci];
+    const uint32_t sw = sgn4[ci];
+    process_chunk(m, d, geo, q, sw, chunk_mask(ci, lo, hi), k, nuv, st, pc);
+  }
+}
+
+// All arcs of a staged list, one arc per warp at a time, each timed.
+__device__ __forceinline__ void timed_pass(const Csr& g, const StageMem& m, uint32_t d,
+                                           uint32_t warp, uint32_t warps, uint32_t lane,
+                                           const Geo& geo, PackedCounts& pc, TypeCounts& tc,
+                                           const ArcTimes& at, uint32_t tclass) {
+  for (uint32_t k = warp; k + 1 < d; k += warps) {
+    const uint32_t st = m.st[k];
+    if (st == kNoArc) continue;
+    const uint32_t lo = m.lo[k], blen = m.hi[k] - lo;
+    __syncwarp();
+    const long long t0 = clock_after(0);
+    if (st == STC_STRATEGY_SEARCH)
+      arc_search(m.a, m.s, k + 1, d, m.s[k] < 0, g.nbr + lo, g.sgn + lo, blen, lane, pc);
+    else
+      arc_stream(g, m, d, k, lane, geo, pc);
+    // The arc's time is the latest lane's (each lane stops its clock once its
+    // own counts are in).
+    const unsigned dt = __reduce_max_sync(kFull, (unsigned)(clock_after(pc.w) - t0));
+    pc.drain(tc);
+    if (lane == 0) record_arc(at, tclass, d - k - 1, blen, dt);
   }
 }
 
@@ -605,10 +682,10 @@ __global__ void __launch_bounds__(256) k_tiny(Csr g, const uint32_t* __restrict_
 constexpr uint32_t kWarpBuckets = 2 * kWarpCap;
 constexpr size_t kWarpStageBytes = (StageMem::bytes(kWarpCap, kWarpBuckets) + 15) & ~size_t(15);
 
-template <class Sink>
+template <class Sink, bool kTime>
 __global__ void __launch_bounds__(256) k_warp(Csr g, const uint32_t* __restrict__ list, uint32_t cnt,
                                               unsigned long long* __restrict__ ctr, Sink sink,
-                                              const uint8_t* __restrict__ gtable) {
+                                              const uint8_t* __restrict__ gtable, ArcTimes at) {
   constexpr bool kVC = Sink::kPerVertex;
   constexpr int kWarps = 8;
   __shared__ __align__(16) unsigned char smem[kWarps * kWarpStageBytes];
@@ -629,12 +706,16 @@ __global__ void __launch_bounds__(256) k_warp(Csr g, const uint32_t* __restrict_
     }
     const Geo geo = Geo::of(d, kWarpBuckets);
     stage<32>(g, ub, d, lane, m, geo, table, WarpSync{});
-    warp_chunk_scan(m, d, lane);
     TypeCounts vc;
     TypeCounts& out = kVC ? vc : tc;
     PackedCounts pc;
-    stream_pass<kStreamUnroll>(g, m, d, 0, 1, lane, geo, pc, out);
-    search_pass(g, m, d, 0, 1, lane, pc, out);
+    if (kTime) {
+      timed_pass(g, m, d, 0, 1, lane, geo, pc, out, at, kTableWarp);
+    } else {
+      warp_chunk_scan(m, d, lane);
+      stream_pass<kStreamUnroll>(g, m, d, 0, 1, lane, geo, pc, out);
+      search_pass(g, m, d, 0, 1, lane, pc, out);
+    }
     pc.drain(out);
     if (kVC) warp_vertex_flush(vc, u, lane, sink);
     __syncwarp();
@@ -647,12 +728,13 @@ __global__ void __launch_bounds__(256) k_warp(Csr g, const uint32_t* __restrict_
 // (nb >= 2 * cap, powers of two).
 inline size_t block_stage_bytes(uint32_t cap, uint32_t nb) { return StageMem::bytes(cap, nb); }
 
-template <int THREADS, class Sink>
+template <int THREADS, class Sink, bool kTime>
 __global__ void __launch_bounds__(THREADS) k_block(Csr g, const uint32_t* __restrict__ list,
                                                    uint32_t cnt, uint32_t cap, uint32_t nb,
                                                    unsigned long long* __restrict__ queue,
                                                    unsigned long long* __restrict__ ctr, Sink sink,
-                                                   const uint8_t* __restrict__ gtable) {
+                                                   const uint8_t* __restrict__ gtable, ArcTimes at,
+                                                   uint32_t tclass) {
   constexpr bool kVC = Sink::kPerVertex;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ uint8_t table[16][16];
@@ -678,12 +760,16 @@ __global__ void __launch_bounds__(THREADS) k_block(Csr g, const uint32_t* __rest
     }
     const Geo geo = Geo::of(d, nb);
     stage<THREADS>(g, ub, d, threadIdx.x, m, geo, table, BlockSync{});
-    block_chunk_scan<THREADS>(m, d, scan_tmp);
     TypeCounts vc;
     TypeCounts& out = kVC ? vc : tc;
     PackedCounts pc;
-    stream_pass<kStreamUnroll>(g, m, d, w, kWarps, lane, geo, pc, out);
-    search_pass(g, m, d, w, kWarps, lane, pc, out);
+    if (kTime) {
+      timed_pass(g, m, d, w, kWarps, lane, geo, pc, out, at, tclass);
+    } else {
+      block_chunk_scan<THREADS>(m, d, scan_tmp);
+      stream_pass<kStreamUnroll>(g, m, d, w, kWarps, lane, geo, pc, out);
+      search_pass(g, m, d, w, kWarps, lane, pc, out);
+    }
     pc.drain(out);
     if (kVC) block_vertex_flush<THREADS>(vc, u, sink);
   }
@@ -692,11 +778,11 @@ __global__ void __launch_bounds__(THREADS) k_block(Csr g, const uint32_t* __rest
 
 // Giant lists (d > kLargeCap): one CTA per vertex, A read from global memory,
 // one arc per warp; HASH falls back to MERGE (no staged hash).
-template <int THREADS, class Sink>
+template <int THREADS, class Sink, bool kTime>
 __global__ void __launch_bounds__(THREADS) k_giant(Csr g, const uint32_t* __restrict__ list,
                                                    uint32_t cnt, unsigned long long* __restrict__ queue,
                                                    unsigned long long* __restrict__ ctr, Sink sink,
-                                                   const uint8_t* __restrict__ gtable) {
+                                                   const uint8_t* __restrict__ gtable, ArcTimes at) {
   constexpr bool kVC = Sink::kPerVertex;
   __shared__ uint8_t table[16][16];
   __shared__ uint32_t s_item;
@@ -723,12 +809,21 @@ __global__ void __launch_bounds__(THREADS) k_giant(Csr g, const uint32_t* __rest
       const uint32_t blen = (uint32_t)(g.off[v + 1] - vb);
       if (blen == 0) continue;
       const uint32_t st = table[size_bucket(d - k - 1)][size_bucket(blen)];
-      if (st == STC_STRATEGY_SEARCH) {
-        PackedCounts pc;
-        arc_search(a, s, k + 1, d, s[k] < 0, g.nbr + vb, g.sgn + vb, blen, lane, pc);
-        pc.drain(out);
-      } else {
+      long long t0 = 0;
+      if (kTime) {
+        __syncwarp();
+        t0 = clock_after(0);
+      }
+      // 64-bit counters: a giant list may be long enough to overflow the
+      // packed 16-bit fields within one arc.
+      if (st == STC_STRATEGY_SEARCH)
+        arc_search(a, s, k + 1, d, s[k] < 0, g.nbr + vb, g.sgn + vb, blen, lane, out);
+      else
         arc_merge_global(a, s, k + 1, d, s[k] < 0, g.nbr + vb, g.sgn + vb, blen, lane, out);
+      if (kTime) {
+        const unsigned long long dep = out.c[0] + out.c[1] + out.c[2] + out.c[3];
+        const unsigned dt = __reduce_max_sync(kFull, (unsigned)(clock_after(dep) - t0));
+        if (lane == 0) record_arc(at, kTableGiant, d - k - 1, blen, dt);
       }
     }
     if (kVC) block_vertex_flush<THREADS>(vc, u, sink);
@@ -736,23 +831,12 @@ __global__ void __launch_bounds__(THREADS) k_giant(Csr g, const uint32_t* __rest
   if (!kVC) flush_counts<THREADS>(tc, ctr);
 }
 
-// Fixed degree-threshold dispatch: SEARCH when B is at least 16x longer than
-// A', MERGE when both are short, HASH otherwise.
-void fixed_table(uint8_t t[16][16]) {
-  for (int a = 0; a < 16; a++)
-    for (int b = 0; b < 16; b++) {
-      uint8_t s = STC_STRATEGY_HASH;
-      if (b >= a + 4) s = STC_STRATEGY_SEARCH;
-      else if (a <= 3 && b <= 5) s = STC_STRATEGY_MERGE;
-      t[a][b] = s;
-    }
-}
-
-// Launches the class kernels for one sink kind.
-template <class Sink>
+// Launches the class kernels for one sink kind.  `d_tables` holds one
+// 256-byte table per TableClass.
+template <class Sink, bool kTime>
 void launch_classes(cudaStream_t st, const Csr& csr, const uint32_t* lists, const uint32_t* counts,
                     const uint32_t* starts, uint32_t max_fdeg, unsigned long long* ctr,
-                    const uint8_t* d_table, const Sink& sink, int& launches) {
+                    const uint8_t* d_tables, const Sink& sink, const ArcTimes& at, int& launches) {
   if (counts[0]) {
     const uint32_t grid = std::min<uint32_t>((counts[0] + 255) / 256, kSMs * 8);
     k_tiny<kTinyMax, Sink><<<grid, 256, 0, st>>>(csr, lists + starts[0], counts[0], ctr, sink);
@@ -760,17 +844,20 @@ void launch_classes(cudaStream_t st, const Csr& csr, const uint32_t* lists, cons
   }
   if (counts[1]) {
     const uint32_t grid = std::min<uint32_t>((counts[1] + 7) / 8, kSMs * 8);
-    k_warp<Sink><<<grid, 256, 0, st>>>(csr, lists + starts[1], counts[1], ctr, sink, d_table);
+    k_warp<Sink, kTime><<<grid, 256, 0, st>>>(csr, lists + starts[1], counts[1], ctr, sink,
+                                               d_tables + 256 * kTableWarp, at);
     launches++;
   }
   if (counts[2]) {
     const uint32_t cap = kBlockCap, nb = 4 * kBlockCap;
     const size_t smem = block_stage_bytes(cap, nb);
-    STC_CUDA(cudaFuncSetAttribute(k_block<256, Sink>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem));
+    STC_CUDA(cudaFuncSetAttribute(k_block<256, Sink, kTime>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const uint32_t grid = std::min<uint32_t>(counts[2], kSMs * 8);
-    k_block<256, Sink><<<grid, 256, smem, st>>>(csr, lists + starts[2], counts[2], cap, nb,
-                                                 ctr + C_WORK + 0, ctr, sink, d_table);
+    k_block<256, Sink, kTime><<<grid, 256, smem, st>>>(csr, lists + starts[2], counts[2], cap, nb,
+                                                        ctr + C_WORK + 0, ctr, sink,
+                                                        d_tables + 256 * kTableBlock, at,
+                                                        kTableBlock);
     launches++;
   }
   if (counts[3]) {
@@ -779,42 +866,76 @@ void launch_classes(cudaStream_t st, const Csr& csr, const uint32_t* lists, cons
     while (cap < std::min<uint32_t>(max_fdeg, kLargeCap)) cap <<= 1;
     const uint32_t nb = 2 * cap;
     const size_t smem = block_stage_bytes(cap, nb);
-    STC_CUDA(cudaFuncSetAttribute(k_block<512, Sink>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem));
+    STC_CUDA(cudaFuncSetAttribute(k_block<512, Sink, kTime>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const uint32_t grid = std::min<uint32_t>(counts[3], kSMs * 2);
-    k_block<512, Sink><<<grid, 512, smem, st>>>(csr, lists + starts[3], counts[3], cap, nb,
-                                                 ctr + C_WORK + 1, ctr, sink, d_table);
+    k_block<512, Sink, kTime><<<grid, 512, smem, st>>>(csr, lists + starts[3], counts[3], cap, nb,
+                                                        ctr + C_WORK + 1, ctr, sink,
+                                                        d_tables + 256 * kTableLarge, at,
+                                                        kTableLarge);
     launches++;
   }
   if (counts[4]) {
     const uint32_t grid = std::min<uint32_t>(counts[4], kSMs * 2);
-    k_giant<512, Sink><<<grid, 512, 0, st>>>(csr, lists + starts[4], counts[4], ctr + C_WORK + 2,
-                                              ctr, sink, d_table);
+    k_giant<512, Sink, kTime><<<grid, 512, 0, st>>>(csr, lists + starts[4], counts[4],
+                                                     ctr + C_WORK + 2, ctr, sink,
+                                                     d_tables + 256 * kTableGiant, at);
     launches++;
   }
 }
 
 }  // namespace
 
+// Fixed degree-threshold dispatch, the same for every class: SEARCH when B
+// is at least 16x longer than A', MERGE when both are short, HASH otherwise
+// (the giant class, which stages no hash, merges instead of hashing).
+void fixed_dispatch_tables(uint8_t* out) {
+  for (int t = 0; t < kTableClasses; t++)
+    for (int a = 0; a < 16; a++)
+      for (int b = 0; b < 16; b++) {
+        uint8_t s = STC_STRATEGY_HASH;
+        if (b >= a + 4) s = STC_STRATEGY_SEARCH;
+        else if (a <= 3 && b <= 5) s = STC_STRATEGY_MERGE;
+        out[256 * t + 16 * a + b] = s;
+      }
+}
+
+// Device copy of the dispatch tables a call uses: a forced strategy fills
+// every cell; otherwise the learned tables when the context holds a model
+// and the call asks for them, else the fixed ones.
+const uint8_t* dispatch_tables(stc_ctx* c, const CountConfig& cfg) {
+  if (cfg.strategy != STC_STRATEGY_AUTO) {
+    uint8_t* t = buffer<uint8_t>(c, B_WORK2, kTableBytes);
+    STC_CUDA(cudaMemsetAsync(t, (int)cfg.strategy, kTableBytes, c->stream));
+    return t;
+  }
+  if (cfg.dispatch == STC_DISPATCH_LEARNED && c->model_loaded)
+    return buffer<uint8_t>(c, B_DISPATCH, kTableBytes);
+  if (!c->fixed_ready) {
+    uint8_t h[kTableBytes];
+    fixed_dispatch_tables(h);
+    uint8_t* t = buffer<uint8_t>(c, B_DISPATCH_FIXED, kTableBytes);
+    STC_CUDA(cudaMemcpyAsync(t, h, kTableBytes, cudaMemcpyHostToDevice, c->stream));
+    STC_CUDA(cudaStreamSynchronize(c->stream));  // `h` is pageable and leaves scope
+    c->fixed_ready = true;
+  }
+  return buffer<uint8_t>(c, B_DISPATCH_FIXED, kTableBytes);
+}
+
 void count_triangles(stc_ctx* c, const DeviceGraph& g, const CountConfig& cfg) {
   if (g.n == 0 || g.m_fwd == 0) return;
   cudaStream_t st = c->stream;
   Csr csr{g.off, g.nbr, g.sgn, g.verts, g.n};
   unsigned long long* ctr = (unsigned long long*)counters(c);
-
-  // Dispatch table.
-  uint8_t table[16][16];
-  if (cfg.strategy == STC_STRATEGY_AUTO) {
-    fixed_table(table);
-  } else {
-    memset(table, (int)cfg.strategy, sizeof(table));
-  }
-  uint8_t* d_table = buffer<uint8_t>(c, B_WORK2, 256);
-  STC_CUDA(cudaMemcpyAsync(d_table, table, 256, cudaMemcpyHostToDevice, st));
+  const uint8_t* d_table = dispatch_tables(c, cfg);
+  const bool timed = cfg.arc_cycles != nullptr;
+  const ArcTimes at{(unsigned long long*)cfg.arc_cycles, (unsigned long long*)cfg.arc_counts};
 
   // Vertex classes (a forced strategy disables the tiny class, which only
-  // implements the search form).
-  const bool tiny = cfg.strategy == STC_STRATEGY_AUTO || cfg.strategy == STC_STRATEGY_SEARCH;
+  // implements the search form; so does timing, so that every strategy's
+  // timings cover the same arcs).
+  const bool tiny =
+      !timed && (cfg.strategy == STC_STRATEGY_AUTO || cfg.strategy == STC_STRATEGY_SEARCH);
   const ClassBounds cb{tiny ? kTinyMax : 1u, kWarpCap, kBlockCap, kLargeCap};
   k_classify_count<<<kSMs * 4, 256, 0, st>>>(g.off, g.n, cb, ctr);
   STC_CUDA(cudaMemcpyAsync(c->h_pinned + C_WORK, counters(c) + C_WORK,
@@ -836,14 +957,20 @@ void count_triangles(stc_ctx* c, const DeviceGraph& g, const CountConfig& cfg) {
   STC_CUDA(cudaMemsetAsync(counters(c) + C_WORK, 0, 8 * sizeof(uint64_t), st));
   c->launches += 2;
 
-  if (cfg.vertex_counts) {
+  if (timed) {
+    launch_classes<TotalSink, true>(st, csr, lists, counts, starts, max_fdeg, ctr, d_table,
+                                    TotalSink{}, at, c->launches);
+  } else if (cfg.vertex_counts) {
     const VertexSink sink{(unsigned long long*)cfg.vertex_counts, g.verts};
-    launch_classes(st, csr, lists, counts, starts, max_fdeg, ctr, d_table, sink, c->launches);
+    launch_classes<VertexSink, false>(st, csr, lists, counts, starts, max_fdeg, ctr, d_table, sink,
+                                      at, c->launches);
   } else if (cfg.graph_counts) {
     const GraphSink sink{(unsigned long long*)cfg.graph_counts, g.gbase, g.G};
-    launch_classes(st, csr, lists, counts, starts, max_fdeg, ctr, d_table, sink, c->launches);
+    launch_classes<GraphSink, false>(st, csr, lists, counts, starts, max_fdeg, ctr, d_table, sink,
+                                     at, c->launches);
   } else {
-    launch_classes(st, csr, lists, counts, starts, max_fdeg, ctr, d_table, TotalSink{}, c->launches);
+    launch_classes<TotalSink, false>(st, csr, lists, counts, starts, max_fdeg, ctr, d_table,
+                                     TotalSink{}, at, c->launches);
   }
   STC_CUDA(cudaGetLastError());
 }
@@ -866,7 +993,7 @@ constexpr int kNoAllocMaxDevices = 64;
 
 struct NoAllocScratch {
   unsigned long long ctr[C_SLOTS];
-  uint8_t table[256];
+  uint8_t table[kTableBytes];
   uint32_t lists[kNoAllocMaxVertices + 8];
 };
 
@@ -957,8 +1084,8 @@ extern "C" stc_status stc_count_oriented_csr_noalloc(const uint64_t* d_offsets,
   if (slots[C_ERROR]) return STC_ERR_INVALID_ARGUMENT;
   if (m == 0) return STC_OK;
 
-  uint8_t table[16][16];
-  fixed_table(table);
+  uint8_t table[kTableBytes];
+  fixed_dispatch_tables(table);
   STC_NA(cudaMemcpyAsync(scr->table, table, sizeof(table), cudaMemcpyHostToDevice, st));
   const ClassBounds cb{kTinyMax, kWarpCap, kBlockCap, kLargeCap};
   k_classify_count<<<kSMs * 4, 256, 0, st>>>(d_offsets, n, cb, ctr);
@@ -979,39 +1106,13 @@ extern "C" stc_status stc_count_oriented_csr_noalloc(const uint64_t* d_offsets,
   STC_NA(cudaMemsetAsync(ctr + C_WORK, 0, 8 * sizeof(uint64_t), st));
 
   const Csr csr{d_offsets, d_heads, d_signs, nullptr, n};
-  const uint8_t* d_table = scr->table;
-  if (counts[0]) {
-    const uint32_t grid = std::min<uint32_t>((counts[0] + 255) / 256, kSMs * 8);
-    k_tiny<kTinyMax, TotalSink><<<grid, 256, 0, st>>>(csr, lists + starts[0], counts[0], ctr, TotalSink{});
-  }
-  if (counts[1]) {
-    const uint32_t grid = std::min<uint32_t>((counts[1] + 7) / 8, kSMs * 8);
-    k_warp<TotalSink><<<grid, 256, 0, st>>>(csr, lists + starts[1], counts[1], ctr, TotalSink{}, d_table);
-  }
-  if (counts[2]) {
-    const uint32_t cap = kBlockCap, nb = 4 * kBlockCap;
-    const size_t smem = block_stage_bytes(cap, nb);
-    STC_NA(cudaFuncSetAttribute(k_block<256, TotalSink>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem));
-    const uint32_t grid = std::min<uint32_t>(counts[2], kSMs * 8);
-    k_block<256, TotalSink><<<grid, 256, smem, st>>>(csr, lists + starts[2], counts[2], cap, nb,
-                                                  ctr + C_WORK + 0, ctr, TotalSink{}, d_table);
-  }
-  if (counts[3]) {
-    uint32_t cap = kBlockCap;
-    while (cap < std::min<uint32_t>(max_fdeg, kLargeCap)) cap <<= 1;
-    const uint32_t nb = 2 * cap;
-    const size_t smem = block_stage_bytes(cap, nb);
-    STC_NA(cudaFuncSetAttribute(k_block<512, TotalSink>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem));
-    const uint32_t grid = std::min<uint32_t>(counts[3], kSMs * 2);
-    k_block<512, TotalSink><<<grid, 512, smem, st>>>(csr, lists + starts[3], counts[3], cap, nb,
-                                                  ctr + C_WORK + 1, ctr, TotalSink{}, d_table);
-  }
-  if (counts[4]) {
-    const uint32_t grid = std::min<uint32_t>(counts[4], kSMs * 2);
-    k_giant<512, TotalSink><<<grid, 512, 0, st>>>(csr, lists + starts[4], counts[4], ctr + C_WORK + 2,
-                                               ctr, TotalSink{}, d_table);
+  int launches = 0;
+  try {
+    launch_classes<TotalSink, false>(st, csr, lists, counts, starts, max_fdeg, ctr, scr->table,
+                                     TotalSink{}, ArcTimes{nullptr, nullptr}, launches);
+  } catch (const Error& e) {
+    (void)cudaGetLastError();
+    return e.status;
   }
   STC_NA(cudaGetLastError());
   STC_NA(cudaMemcpyAsync(slots, ctr, sizeof(slots), cudaMemcpyDeviceToHost, st));

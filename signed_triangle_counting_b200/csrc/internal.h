@@ -36,6 +36,10 @@ enum BufId {
   B_EXPORT_OFF, B_EXPORT_FDEG,
   B_VCOUNTS,
   B_BATCH_META, B_BATCH_SPACE, B_BATCH_COUNTS,
+  B_DISPATCH,                     // learned dispatch tables (kTableBytes)
+  B_DISPATCH_FIXED,               // fixed dispatch tables (kTableBytes)
+  B_DISPATCH_TRAIN,               // dispatcher training samples and parameters
+  B_TIMES,                        // timing recorder: cycles and arcs per cell
   B_COUNT_
 };
 
@@ -63,6 +67,22 @@ enum CounterSlot {
 constexpr uint64_t kDeviceErrCsr = 1;
 constexpr uint64_t kDeviceErrTimeout = 2;
 
+// Dispatch tables: per list class that consults one, a 16 x 16 table
+// indexed by (bucket |A'|, bucket |B|), bucket(x) = min(15, bit width of x),
+// holding an stc_strategy.  Cell index = 256 * class + 16 * a + b.
+enum TableClass { kTableWarp = 0, kTableBlock = 1, kTableLarge = 2, kTableGiant = 3, kTableClasses = 4 };
+constexpr size_t kTableBytes = 256 * kTableClasses;
+static_assert(kTableBytes == STC_DISPATCH_CELLS, "one table byte per dispatch cell");
+
+// The dispatcher's multilayer perceptron: STC_DISPATCH_FEATURES inputs, one
+// hidden ReLU layer, one logit per strategy (MERGE, HASH, SEARCH).
+// Parameter layout: W1[hidden][in], b1[hidden], W2[out][hidden], b2[out].
+constexpr int kMlpIn = STC_DISPATCH_FEATURES;
+constexpr int kMlpHidden = 16;
+constexpr int kMlpOut = 3;
+constexpr int kMlpParams = kMlpHidden * kMlpIn + kMlpHidden + kMlpOut * kMlpHidden + kMlpOut;
+static_assert(kMlpParams == STC_DISPATCH_MODEL_PARAMS, "parameter count of the ABI");
+
 }  // namespace stc
 
 struct stc_ctx {
@@ -76,6 +96,8 @@ struct stc_ctx {
   cudaEvent_t ev[8] = {};
   bool timing = false;
   int launches = 0;
+  bool fixed_ready = false;   // B_DISPATCH_FIXED holds the fixed tables
+  bool model_loaded = false;  // B_DISPATCH holds the tables of a loaded model
 };
 
 namespace stc {
@@ -154,8 +176,23 @@ struct CountConfig {
   uint32_t dispatch = STC_DISPATCH_FIXED;
   uint64_t* vertex_counts = nullptr;  // optional per-source counts, 4 per vertex id
   uint64_t* graph_counts = nullptr;   // optional per-graph counts of a batch, 4 per graph
+  // Timing recorder (device arrays of kTableBytes words, or null): adds each
+  // arc's SM cycles and one arc to its dispatch cell.
+  uint64_t* arc_cycles = nullptr;
+  uint64_t* arc_counts = nullptr;
 };
 void count_triangles(stc_ctx* c, const DeviceGraph& g, const CountConfig& cfg);
+
+// Dispatch: the fixed tables (kTableBytes, host), the per-cell features
+// (kTableBytes x kMlpIn, host), the learned tables of a model computed on
+// the device into B_DISPATCH, and the on-device training of a model.
+void fixed_dispatch_tables(uint8_t* out);
+void dispatch_features(float* out);
+const uint8_t* dispatch_tables(stc_ctx* c, const CountConfig& cfg);
+void load_dispatch_model(stc_ctx* c, const float* params);
+void train_dispatcher(stc_ctx* c, const float* features, const int32_t* labels,
+                      const float* weights, uint32_t samples, uint32_t epochs, float lr,
+                      uint64_t seed, float* params, float* loss);
 
 uint64_t* counters(stc_ctx* c);
 

@@ -1,0 +1,206 @@
+"""Learned dispatcher: training data from the counter's own timings, training
+on the device, model files, and regret against exhaustive per-cell timing.
+
+The reference runs one intersection strategy per program (merge in
+"Signed_TC/Multicore Implementations/tc_merge_sign_enu.cpp:12-44", hash in
+"tc_hash_sign_enu.cpp:125-165"); this engine picks one per dispatch cell
+(class of u's list, bucket |A'|, bucket |B|).  All strategies give the same
+counts, so a dispatch table changes only speed.
+
+* ``record`` runs the timing recorder once per forced strategy: exhaustive
+  per-cell timing of one graph.
+* ``samples`` turns a recording into training rows: the cell's features, its
+  fastest strategy as the label, and the cycles at stake as the weight.
+* ``train`` fits the perceptron on the device (``stc_dispatcher_train``).
+* ``regret`` judges any table against a recording: the time it would spend
+  divided by the time of the per-cell best choice (1.0 = no regret).
+
+    python -m signed_triangle_counting_b200.dispatcher train [--out PATH]
+    python -m signed_triangle_counting_b200.dispatcher evaluate [--model PATH]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+from pathlib import Path
+
+import numpy as np
+
+from . import _capi, dispatch_features, synth
+
+STRATEGIES = ("merge", "hash", "search")  # label k is strategy code k + 1
+GIANT = 3                                  # class index whose lists stage no hash
+DEFAULT_MODEL = Path(__file__).resolve().parent / "dispatch_model.json"
+FORMAT_VERSION = 1
+
+
+def record(ctx, src, dst, sign) -> dict:
+    """Per-cell cycles of every strategy on one graph (three timed runs).
+
+    Returns {"cycles": (3, CELLS) float64, "arcs": (CELLS,) float64,
+    "counts": GlobalTriCounts}; raises if the strategies disagree on the
+    counts or on which arcs they timed."""
+    cycles, arcs, counts = [], None, None
+    for s in STRATEGIES:
+        cy, ar, c = ctx.record_bucket_times(src, dst, sign, strategy=s)
+        if counts is None:
+            counts, arcs = c, ar
+        elif c != counts or not np.array_equal(ar, arcs):
+            raise RuntimeError(f"strategy {s} disagrees: {c} vs {counts}")
+        cycles.append(cy.astype(np.float64))
+    return {"cycles": np.stack(cycles), "arcs": arcs.astype(np.float64), "counts": counts}
+
+
+def merge(records) -> dict:
+    """Sums recordings of several graphs (cycles and arcs per cell)."""
+    return {"cycles": sum(r["cycles"] for r in records), "arcs": sum(r["arcs"] for r in records)}
+
+
+def cell_costs(rec) -> np.ndarray:
+    """Mean cycles per arc, (3, CELLS); HASH is unavailable in the giant class
+    (its arcs run MERGE), so it costs infinity there; empty cells cost 0."""
+    arcs = rec["arcs"]
+    cost = np.divide(rec["cycles"], np.maximum(arcs, 1.0)[None, :])
+    cost[1, GIANT * 256:(GIANT + 1) * 256] = np.inf
+    return cost
+
+
+def samples(rec, min_arcs: int = 32):
+    """Training rows of a recording: (features, labels, weights, cells).
+
+    Only cells with at least ``min_arcs`` arcs are kept.  Label = fastest
+    strategy; weight = arcs x (slowest - fastest) mean cycles over the
+    available strategies, normalised to sum 1."""
+    arcs = rec["arcs"]
+    cost = cell_costs(rec)
+    cells = np.nonzero(arcs >= min_arcs)[0]
+    c = cost[:, cells]
+    labels = np.argmin(c, axis=0).astype(np.int32)
+    finite = np.where(np.isfinite(c), c, -np.inf)
+    stake = arcs[cells] * (finite.max(axis=0) - c.min(axis=0))
+    w = stake / stake.sum() if stake.sum() > 0 else np.full(len(cells), 1.0 / max(1, len(cells)))
+    X = dispatch_features()[cells]
+    return X, labels, w.astype(np.float32), cells
+
+
+def regret(rec, tables) -> dict:
+    """Cycles a dispatch table would spend on a recording, relative to the
+    per-cell best strategy.  ``tables``: strategy codes, (4, 16, 16) or flat."""
+    t = np.asarray(tables).reshape(-1).astype(np.int64)
+    arcs = rec["arcs"]
+    cost = cell_costs(rec)
+    k = t - 1
+    # The giant class runs MERGE where a table says HASH.
+    giant = np.arange(len(t)) // 256 == GIANT
+    k = np.where(giant & (k == 1), 0, k)
+    used = arcs > 0
+    chosen = cost[k, np.arange(len(t))]
+    spent = float((arcs * np.where(used, chosen, 0.0)).sum())
+    best = float((arcs * np.where(used, cost.min(axis=0), 0.0)).sum())
+    return {"cycles": spent, "best_cycles": best, "ratio": spent / best if best else 1.0}
+
+
+def train(ctx, rec, *, epochs: int = 3000, lr: float = 0.02, seed: int = 1, min_arcs: int = 32):
+    """Trains on a recording; returns (params, info)."""
+    X, y, w, cells = samples(rec, min_arcs)
+    params, loss = ctx.train_dispatcher(X, y, w, epochs=epochs, lr=lr, seed=seed)
+    ctx.set_dispatch_model(params)
+    pred = ctx.dispatch_tables("learned").reshape(-1)[cells].astype(np.int64) - 1
+    giant = cells // 256 == GIANT
+    pred = np.where(giant & (pred == 1), 0, pred)
+    acc = float((w * (pred == y)).sum())
+    info = {"samples": int(len(cells)), "loss": loss, "weighted_accuracy": acc,
+            "epochs": epochs, "lr": lr, "seed": seed, "min_arcs": min_arcs}
+    return params, info
+
+
+def save(path, params, meta: dict) -> None:
+    doc = {"format": FORMAT_VERSION, "kind": "stc-dispatch-mlp",
+           "layout": "W1[16][6], b1[16], W2[3][16], b2[3]",
+           "params": [float(x) for x in np.asarray(params, np.float32)]}
+    doc.update(meta)
+    Path(path).write_text(json.dumps(doc, indent=1) + "\n")
+
+
+def load(path=None) -> dict:
+    """Reads a model file; ``params`` comes back as a float32 array."""
+    doc = json.loads(Path(path or DEFAULT_MODEL).read_text())
+    if doc.get("format") != FORMAT_VERSION or doc.get("kind") != "stc-dispatch-mlp":
+        raise ValueError(f"{path or DEFAULT_MODEL}: not a dispatch model of format {FORMAT_VERSION}")
+    p = np.asarray(doc["params"], np.float32)
+    if p.shape != (_capi.DISPATCH_MODEL_PARAMS,):
+        raise ValueError("wrong number of model parameters")
+    doc["params"] = p
+    return doc
+
+
+def union(el, offsets, ns):
+    """One graph from graphs stored back to back (ids local to each graph):
+    graph g's ids are shifted by the vertex counts of the graphs before it."""
+    offsets = np.asarray(offsets, np.int64)
+    vbase = np.concatenate([[0], np.cumsum(np.asarray(ns, np.int64))[:-1]])
+    shift = np.repeat(vbase, np.diff(offsets)).astype(np.uint32)
+    return el.src + shift, el.dst + shift, el.sign
+
+
+def training_graphs(batch_graphs: int = 512):
+    """The training inputs: the Delaunay mesh (1M points, 20% deleted) and
+    the first ``batch_graphs`` graphs of the 4,096-graph batch as one union."""
+    d = synth.workload(2)
+    yield "workload2", (d.src, d.dst, d.sign)
+    specs = synth.batch_specs(4096)
+    el, offs = synth.batch_packed(specs, 0, batch_graphs)
+    yield f"workload4[0:{batch_graphs}]", union(el, offs, [s["n"] for s in specs[:batch_graphs]])
+
+
+def _main() -> None:
+    from . import Context
+    ap = argparse.ArgumentParser(prog="python -m signed_triangle_counting_b200.dispatcher")
+    ap.add_argument("mode", choices=["train", "evaluate"])
+    ap.add_argument("--out", default=str(DEFAULT_MODEL))
+    ap.add_argument("--model", default=None)
+    ap.add_argument("--workload", type=int, default=3)
+    ap.add_argument("--epochs", type=int, default=3000)
+    ap.add_argument("--batch-graphs", type=int, default=512)
+    ap.add_argument("--save-recording", default=None,
+                    help="write the per-cell recordings to this .npz file")
+    a = ap.parse_args()
+    ctx = Context(0)
+    import torch
+    gpu = torch.cuda.get_device_name(0) if torch.cuda.is_available() else "?"
+    if a.mode == "train":
+        recs, names = [], []
+        for name, (s, d, g) in training_graphs(a.batch_graphs):
+            t0 = time.time()
+            recs.append(record(ctx, s, d, g))
+            names.append(name)
+            print(json.dumps({"recorded": name, "m": int(len(s)), "s": round(time.time() - t0, 1)}),
+                  flush=True)
+        rec = merge(recs)
+        if a.save_recording:
+            np.savez(a.save_recording, names=np.array(names),
+                     cycles=np.stack([r["cycles"] for r in recs]),
+                     arcs=np.stack([r["arcs"] for r in recs]))
+        params, info = train(ctx, rec, epochs=a.epochs)
+        meta = {"gpu": gpu, "trained_on": names, **info,
+                "train_regret_fixed": regret(rec, ctx.dispatch_tables("fixed"))["ratio"],
+                "train_regret_learned": regret(rec, ctx.dispatch_tables("learned"))["ratio"]}
+        save(a.out, params, meta)
+        print(json.dumps(meta), flush=True)
+    else:
+        model = ctx.load_dispatch_model(a.model)
+        el = synth.workload(a.workload)
+        rec = record(ctx, el.src, el.dst, el.sign)
+        if a.save_recording:
+            np.savez(a.save_recording, names=np.array([f"workload{a.workload}"]),
+                     cycles=rec["cycles"][None], arcs=rec["arcs"][None])
+        out = {"gpu": gpu, "workload": a.workload, "model_trained_on": model.get("trained_on"),
+               "fixed": regret(rec, ctx.dispatch_tables("fixed")),
+               "learned": regret(rec, ctx.dispatch_tables("learned")),
+               "counts": rec["counts"].as_tuple()}
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    _main()

@@ -1,0 +1,188 @@
+"""GPU tests of the dispatcher: the timing recorder, on-device training and
+inference of the perceptron, and exactness of counts under any dispatch.
+
+All strategies must give identical counts, so every test that changes the
+dispatch also checks the counts bit for bit (against the oracle on small
+graphs, or a closed-form count on a dense clique)."""
+import numpy as np
+import pytest
+
+import oracle
+import signed_triangle_counting_b200 as stc
+from signed_triangle_counting_b200 import _capi, dispatcher, synth
+
+pytestmark = pytest.mark.gpu
+
+GRAPHS = {
+    "rmat": lambda: synth.rmat(3, 13, 1 << 13, 16 << 13, p_pos=0.5),
+    "rmat_dense": lambda: synth.rmat(4, 10, 1 << 10, 128 << 10, p_pos=0.4),
+    "delaunay": lambda: synth.delaunay(5, 20000, 0.2, 0.6),
+    "skew": lambda: synth.skew(6, 1 << 16, 1 << 17, 8, 2000, 20000, 0.8),
+}
+
+
+def bucket(x):
+    return np.minimum(15, np.floor(np.log2(np.maximum(x, 1))).astype(np.int64) + (x > 0))
+
+
+def expected_cells(el):
+    """Arcs per dispatch cell computed from the oracle's forward CSR: lists
+    in rank order, class by out-degree (lists of <= 8 join the warp class
+    when timing), A' = arcs after v in u's list, B = N+(v)."""
+    a = oracle.ForwardCSR(el.src, el.dst, el.sign).arrays()
+    off, edges, fdeg, rank = (a["offsets"].astype(np.int64), a["edges"].astype(np.int64),
+                              a["fdeg"].astype(np.int64), a["rank"].astype(np.int64))
+    n = len(fdeg)
+    tail = np.repeat(np.arange(n), np.diff(off))
+    order = np.lexsort((rank[edges], rank[tail]))
+    tail, head = tail[order], edges[order]
+    d = fdeg[tail]
+    start = np.repeat(np.cumsum(np.concatenate([[0], fdeg[np.argsort(rank)]]))[:-1],
+                      fdeg[np.argsort(rank)])
+    k = np.arange(len(head)) - start
+    alen, blen = d - k - 1, fdeg[head]
+    cls = np.select([d <= 128, d <= 1024, d <= 4096], [0, 1, 2], 3)
+    keep = (alen > 0) & (blen > 0) & (d >= 2)
+    cell = cls * 256 + bucket(alen) * 16 + bucket(blen)
+    return np.bincount(cell[keep], minlength=_capi.DISPATCH_CELLS)
+
+
+@pytest.mark.parametrize("name", sorted(GRAPHS))
+def test_recorder_counts_and_cells(ctx, name):
+    el = GRAPHS[name]()
+    want = oracle.count_arrays(el.src, el.dst, el.sign)
+    cells = expected_cells(el)
+    for s in ("merge", "hash", "search", "auto"):
+        cycles, arcs, c = ctx.record_bucket_times(el.src, el.dst, el.sign, strategy=s)
+        assert c.as_tuple() == want, s
+        np.testing.assert_array_equal(arcs, cells, err_msg=s)
+        assert (cycles[arcs > 0] > 0).all(), s
+        assert (cycles[arcs == 0] == 0).all(), s
+    assert ctx.count(el.src, el.dst, el.sign).as_tuple() == want
+
+
+def fixed_rule():
+    t = np.zeros((4, 16, 16), np.uint8)
+    for a in range(16):
+        for b in range(16):
+            t[:, a, b] = 3 if b >= a + 4 else (1 if a <= 3 and b <= 5 else 2)
+    return t
+
+
+def test_fixed_tables_and_fallback(ctx):
+    ctx.set_dispatch_model(None)
+    np.testing.assert_array_equal(ctx.dispatch_tables("fixed"), fixed_rule())
+    # No model loaded: "learned" falls back to the fixed tables.
+    np.testing.assert_array_equal(ctx.dispatch_tables("learned"), fixed_rule())
+
+
+def numpy_tables(params):
+    p = np.asarray(params, np.float64)
+    W1, b1 = p[:96].reshape(16, 6), p[96:112]
+    W2, b2 = p[112:160].reshape(3, 16), p[160:163]
+    X = stc.dispatch_features().astype(np.float64)
+    z = np.maximum(X @ W1.T + b1, 0) @ W2.T + b2
+    giant = np.arange(len(X)) // 256 == 3
+    z[giant, 1] = -np.inf
+    return np.argmax(z, axis=1) + 1, np.sort(z, axis=1)
+
+
+def test_inference_matches_numpy(ctx):
+    rng = np.random.default_rng(7)
+    for trial in range(4):
+        params = rng.normal(0, 1.0, _capi.DISPATCH_MODEL_PARAMS).astype(np.float32)
+        ctx.set_dispatch_model(params)
+        got = ctx.dispatch_tables("learned").reshape(-1)
+        want, zs = numpy_tables(params)
+        close = (zs[:, -1] - zs[:, -2]) < 1e-4  # near ties may round either way
+        assert ((got == want) | close).all(), trial
+        assert set(np.unique(got)) <= {1, 2, 3}
+        assert not (got[768:] == 2).any()  # giant: never HASH
+    ctx.set_dispatch_model(None)
+
+
+def rule_samples():
+    X = stc.dispatch_features()
+    y = (fixed_rule().reshape(-1) - 1).astype(np.int32)
+    cells = np.arange(768)  # staged classes, where all three strategies exist
+    w = np.full(len(cells), 1.0 / len(cells), np.float32)
+    return X[cells], y[cells], w
+
+
+def test_training_fits_and_is_deterministic(ctx):
+    X, y, w = rule_samples()
+    p1, loss1 = ctx.train_dispatcher(X, y, w, epochs=3000, lr=0.02, seed=3)
+    p2, loss2 = ctx.train_dispatcher(X, y, w, epochs=3000, lr=0.02, seed=3)
+    np.testing.assert_array_equal(p1, p2)
+    assert loss1 == loss2
+    _, loss0 = ctx.train_dispatcher(X, y, w, epochs=1, lr=0.02, seed=3)
+    assert loss1 < 0.3 * loss0
+    ctx.set_dispatch_model(p1)
+    pred = ctx.dispatch_tables("learned").reshape(-1)[:768] - 1
+    assert (pred == y).mean() > 0.95
+    ctx.set_dispatch_model(None)
+
+
+def test_training_rejects_bad_input(ctx):
+    X, y, w = rule_samples()
+    bad = y.copy()
+    bad[0] = 3
+    with pytest.raises(stc.StcError):
+        ctx.train_dispatcher(X, bad, w)
+    with pytest.raises(stc.StcError):
+        ctx.train_dispatcher(X, y, -w)
+    with pytest.raises(stc.StcError):
+        ctx.set_dispatch_model(np.full(_capi.DISPATCH_MODEL_PARAMS, np.nan, np.float32))
+
+
+@pytest.mark.parametrize("name", sorted(GRAPHS))
+def test_learned_dispatch_is_exact(ctx, name):
+    el = GRAPHS[name]()
+    want = oracle.count_arrays(el.src, el.dst, el.sign)
+    rng = np.random.default_rng(11)
+    for trial in range(3):  # random models: varied tables, same counts
+        ctx.set_dispatch_model(rng.normal(0, 1.0, _capi.DISPATCH_MODEL_PARAMS).astype(np.float32))
+        assert ctx.count(el.src, el.dst, el.sign, dispatch="learned").as_tuple() == want
+    ctx.set_dispatch_model(None)
+
+
+def test_shipped_model(ctx):
+    model = ctx.load_dispatch_model()
+    t = ctx.dispatch_tables("learned")
+    assert set(np.unique(t)) <= {1, 2, 3} and not (t[3] == 2).any()
+    assert model["weighted_accuracy"] > 0.9
+    el = GRAPHS["skew"]()
+    want = oracle.count_arrays(el.src, el.dst, el.sign)
+    assert ctx.count(el.src, el.dst, el.sign, dispatch="learned").as_tuple() == want
+    ctx.set_dispatch_model(None)
+
+
+def clique_counts(sign_matrix):
+    """Per-type counts of a signed complete graph from matrix traces: with P
+    and N the positive and negative adjacency, trace(P^3) / 6 triangles are
+    +++, trace(P P N) / 2 are ++-, trace(P N N) / 2 are +--, trace(N^3) / 6
+    are ---."""
+    P = (sign_matrix > 0).astype(np.float32)
+    N = (sign_matrix < 0).astype(np.float32)
+    PP, PN, NN = P @ P, P @ N, N @ N  # entries <= n: exact in float32
+    tr = lambda A, B: int(np.sum(A * B.T, dtype=np.float64))  # noqa: E731
+    return (tr(NN, N) // 6, tr(PN, N) // 2, tr(PP, N) // 2, tr(PP, P) // 6)
+
+
+def test_giant_class_dense_clique(ctx):
+    # K_4500: 403 lists longer than 4096 arcs take the giant class.
+    k = 4500
+    rng = np.random.default_rng(21)
+    a, b = np.triu_indices(k, 1)
+    s = np.where(rng.random(len(a)) < 0.5, 1, -1).astype(np.int8)
+    S = np.zeros((k, k), np.int8)
+    S[a, b] = s
+    S[b, a] = s
+    want = clique_counts(S)
+    perm = rng.permutation(k).astype(np.uint32)  # ids not in degree order
+    src, dst = perm[a], perm[b]
+    for strategy in ("auto", "merge", "hash", "search"):
+        assert ctx.count(src, dst, s, strategy=strategy).as_tuple() == want, strategy
+    _, arcs, c = ctx.record_bucket_times(src, dst, s, strategy="search")
+    assert c.as_tuple() == want
+    assert arcs.reshape(4, 256)[3].sum() > 0  # giant lists were timed
