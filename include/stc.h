@@ -258,21 +258,27 @@ stc_status stc_record_bucket_times(stc_ctx* ctx, const uint32_t* src, const uint
  * to about [-1, 1]. */
 stc_status stc_dispatch_features(float* out);
 
-/* Trains the dispatcher's perceptron (STC_DISPATCH_FEATURES inputs, 16
- * hidden ReLU units, one logit per strategy MERGE / HASH / SEARCH) on the
- * device: full-batch Adam over `samples` rows of `features`, labels 0..2 (=
- * strategy - 1) and non-negative weights, minimising the weighted softmax
- * cross-entropy.  Deterministic for a given seed.  `params` receives the
+/* Trains the dispatcher's perceptron on the device.  The perceptron has
+ * STC_DISPATCH_FEATURES inputs, 16 hidden ReLU units and one output per
+ * strategy (MERGE, HASH, SEARCH): the predicted log2 of the SM cycles one arc
+ * of the cell costs under that strategy.  Training is full-batch Adam over
+ * `samples` rows of `features`, `targets` (samples x 3 measured log2 cycles
+ * per arc, NaN where a strategy is unavailable) and non-negative `weights`,
+ * minimising the weighted squared error plus weight_decay / 2 times the
+ * squared weights.  Deterministic for a given seed.  `params` receives the
  * STC_DISPATCH_MODEL_PARAMS trained parameters (W1[16][6], b1[16], W2[3][16],
- * b2[3]) and `loss` (optional) the final weighted loss.  samples <= 4096. */
-stc_status stc_dispatcher_train(stc_ctx* ctx, const float* features, const int32_t* labels,
+ * b2[3]) and `loss` (optional) the final weighted squared error.
+ * samples <= 4096. */
+stc_status stc_dispatcher_train(stc_ctx* ctx, const float* features, const float* targets,
                                 const float* weights, uint32_t samples, uint32_t epochs,
-                                float learning_rate, uint64_t seed, float* params, float* loss);
+                                float learning_rate, float weight_decay, uint64_t seed,
+                                float* params, float* loss);
 
 /* Loads a trained model into the context: an inference kernel evaluates it
- * on every cell and writes the learned tables on the device, which calls
- * with dispatch STC_DISPATCH_LEARNED then use (the giant class, which stages
- * no hash, never gets HASH).  NULL unloads it; without a model, LEARNED falls
+ * on every cell and writes the learned tables on the device, each cell
+ * taking the strategy of least predicted cost (the giant class, which stages
+ * no hash, never gets HASH).  Calls with dispatch STC_DISPATCH_LEARNED then
+ * use these tables.  NULL unloads the model; without a model, LEARNED falls
  * back to the fixed tables. */
 stc_status stc_ctx_set_dispatch_model(stc_ctx* ctx, const float* params);
 

@@ -347,19 +347,23 @@ class Context:
                self._h)
         return cycles, arcs, GlobalTriCounts(out.t0, out.t1, out.t2, out.t3)
 
-    def train_dispatcher(self, features, labels, weights, *, epochs=3000, lr=0.02, seed=1):
-        """Trains the dispatcher's perceptron on the device; returns
-        (parameters, final weighted loss)."""
+    def train_dispatcher(self, features, targets, weights, *, epochs=3000, lr=0.02,
+                         weight_decay=1e-3, seed=1):
+        """Trains the dispatcher's perceptron on the device: features
+        (samples, DISPATCH_FEATURES), targets (samples, 3) measured log2
+        cycles per arc of MERGE / HASH / SEARCH (NaN = unavailable), weights
+        (samples,).  Returns (parameters, final weighted squared error)."""
         X = np.ascontiguousarray(features, np.float32)
-        y = np.ascontiguousarray(labels, np.int32)
+        T = np.ascontiguousarray(targets, np.float32)
         w = np.ascontiguousarray(weights, np.float32)
-        if X.ndim != 2 or X.shape[1] != _capi.DISPATCH_FEATURES or not (len(X) == len(y) == len(w)):
-            raise ValueError("features must be (samples, DISPATCH_FEATURES) with matching labels/weights")
+        if (X.ndim != 2 or X.shape[1] != _capi.DISPATCH_FEATURES or T.shape != (len(X), 3)
+                or w.shape != (len(X),)):
+            raise ValueError("features (S, DISPATCH_FEATURES), targets (S, 3), weights (S,)")
         params = np.zeros(_capi.DISPATCH_MODEL_PARAMS, np.float32)
         loss = C.c_float()
         _check(lib().stc_dispatcher_train(self._h, X.ctypes.data_as(_capi.f32p),
-                                          y.ctypes.data_as(_capi.i32p), w.ctypes.data_as(_capi.f32p),
-                                          len(X), epochs, lr, seed,
+                                          T.ctypes.data_as(_capi.f32p), w.ctypes.data_as(_capi.f32p),
+                                          len(X), epochs, lr, weight_decay, seed,
                                           params.ctypes.data_as(_capi.f32p), C.byref(loss)), self._h)
         return params, float(loss.value)
 

@@ -112,8 +112,8 @@ SIGNATURES = [
                                           C.c_uint64, C.POINTER(stc_opts), u64p, u64p,
                                           C.POINTER(stc_counts)]),
     ("stc_dispatch_features", C.c_int, [f32p]),
-    ("stc_dispatcher_train", C.c_int, [C.c_void_p, f32p, i32p, f32p, C.c_uint32, C.c_uint32,
-                                       C.c_float, C.c_uint64, f32p, f32p]),
+    ("stc_dispatcher_train", C.c_int, [C.c_void_p, f32p, f32p, f32p, C.c_uint32, C.c_uint32,
+                                       C.c_float, C.c_float, C.c_uint64, f32p, f32p]),
     ("stc_ctx_set_dispatch_model", C.c_int, [C.c_void_p, f32p]),
     ("stc_dispatch_tables", C.c_int, [C.c_void_p, C.c_uint32, u8p]),
     ("stc_synth_rmat_device", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint64,

@@ -496,14 +496,15 @@ stc_status stc_dispatch_features(float* out) {
   return STC_OK;
 }
 
-stc_status stc_dispatcher_train(stc_ctx* c, const float* features, const int32_t* labels,
+stc_status stc_dispatcher_train(stc_ctx* c, const float* features, const float* targets,
                                 const float* weights, uint32_t samples, uint32_t epochs,
-                                float learning_rate, uint64_t seed, float* params, float* loss) {
+                                float learning_rate, float weight_decay, uint64_t seed,
+                                float* params, float* loss) {
   if (!c) return STC_ERR_INVALID_ARGUMENT;
   return guarded(c, [&] {
     c->stream = c->own_stream;
-    train_dispatcher(c, features, labels, weights, samples, epochs, learning_rate, seed, params,
-                     loss);
+    train_dispatcher(c, features, targets, weights, samples, epochs, learning_rate, weight_decay,
+                     seed, params, loss);
   });
 }
 

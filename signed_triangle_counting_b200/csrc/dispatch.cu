@@ -4,10 +4,14 @@
 //
 // A dispatch cell is (class of u's list, bucket |A'|, bucket |B|); a table
 // maps every cell to MERGE, HASH or SEARCH.  All three give identical counts,
-// so the model decides only speed.  It is trained by weighted softmax
-// cross-entropy: the label of a cell is its fastest strategy under the timing
-// recorder, its weight the cycles at stake (arcs x (slowest - fastest)
-// cycles per arc), so cells that matter for the run time dominate the fit.
+// so the model decides only speed.  The model predicts, per strategy, the
+// log2 of the SM cycles an arc of the cell costs, and a cell's table entry
+// is the strategy of least predicted cost.  Training regresses the timing
+// recorder's measured log2 cycles per arc (weighted squared error, L2 weight
+// decay).  Log cost is close to linear in the log-bucketed lengths, which a
+// ReLU network extends linearly beyond the cells it was trained on: that is
+// what lets a model trained on small graphs place the HASH / SEARCH boundary
+// for the long lists of a power-law graph it has not seen.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -52,7 +56,8 @@ __host__ __device__ inline void cell_features(uint32_t cell, float* f) {
   f[5] = cls == kTableGiant ? 0.f : 1.f;
 }
 
-// Logits z of features f; h receives the hidden activations.
+// Outputs z (predicted log2 cycles per arc, one per strategy) of features f;
+// h receives the hidden activations.
 __device__ __forceinline__ void mlp_forward(const float* p, const float* f, float* h, float* z) {
 #pragma unroll
   for (int j = 0; j < kMlpHidden; j++) {
@@ -70,8 +75,8 @@ __device__ __forceinline__ void mlp_forward(const float* p, const float* f, floa
   }
 }
 
-// One thread per cell: the strategy of the largest logit (HASH excluded for
-// the giant class, which stages no hash).
+// One thread per cell: the strategy of least predicted cost (HASH excluded
+// for the giant class, which stages no hash).
 __global__ void k_mlp_tables(const float* __restrict__ params, uint8_t* __restrict__ tables) {
   __shared__ float p[kMlpParams];
   for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) p[i] = params[i];
@@ -85,7 +90,7 @@ __global__ void k_mlp_tables(const float* __restrict__ params, uint8_t* __restri
   int best = 0;
   for (int o = 1; o < kMlpOut; o++) {
     if (giant && o == STC_STRATEGY_HASH - 1) continue;
-    if (z[o] > z[best]) best = o;
+    if (z[o] < z[best]) best = o;
   }
   tables[cell] = (uint8_t)(best + 1);
 }
@@ -99,14 +104,18 @@ __device__ __forceinline__ void grad_add(float* row, int idx, float v, unsigned 
 
 // Full-batch Adam in one CTA.  Each warp takes 32 samples at a time (one per
 // lane) and reduces their gradient contributions with shuffles into its own
-// row of `gpart`; the rows are summed in warp order for the update.
+// row of `gpart`; the rows are summed in warp order for the update.  The
+// objective is sum_i w_i sum_o [T_io available] (z_io - T_io)^2 / sum_i w_i
+// plus wd / 2 times the squared weights (the reported loss is the first term
+// alone); targets are centred on their mean `mu` during training and `mu` is
+// folded into the output biases at the end.
 __global__ void __launch_bounds__(kTrainThreads)
-    k_mlp_train(const float* __restrict__ X, const int32_t* __restrict__ y,
-                const float* __restrict__ w, uint32_t S, uint32_t epochs, float lr, uint64_t seed,
-                float* __restrict__ params_out, float* __restrict__ loss_out) {
+    k_mlp_train(const float* __restrict__ X, const float* __restrict__ T,
+                const float* __restrict__ w, uint32_t S, uint32_t epochs, float lr, float wd,
+                uint64_t seed, float* __restrict__ params_out, float* __restrict__ loss_out) {
   __shared__ float p[kMlpParams], m1[kMlpParams], m2[kMlpParams];
   __shared__ float gpart[kTrainWarps][kMlpParams];
-  __shared__ float red[kTrainWarps];
+  __shared__ float red[3][kTrainWarps];
   const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
   for (int i = threadIdx.x; i < kMlpParams; i += kTrainThreads) {
     // Uniform in +-1/sqrt(fan_in) for weights, zero biases.
@@ -119,15 +128,35 @@ __global__ void __launch_bounds__(kTrainThreads)
     m2[i] = 0.f;
   }
   for (int i = threadIdx.x; i < kTrainWarps * kMlpParams; i += kTrainThreads) (&gpart[0][0])[i] = 0.f;
-  // Total weight, for the loss normalisation.
-  float ws = 0.f;
-  for (uint32_t i = threadIdx.x; i < S; i += kTrainThreads) ws += w[i];
+  // Total weight, and the mean of the available targets.
+  float ws = 0.f, ts = 0.f, tn = 0.f;
+  for (uint32_t i = threadIdx.x; i < S; i += kTrainThreads) {
+    ws += w[i];
+    for (int o = 0; o < kMlpOut; o++) {
+      const float t = T[(size_t)i * kMlpOut + o];
+      if (!isnan(t)) {
+        ts += t;
+        tn += 1.f;
+      }
+    }
+  }
   ws = warp_sum(ws);
-  if (lane == 0) red[warp] = ws;
+  ts = warp_sum(ts);
+  tn = warp_sum(tn);
+  if (lane == 0) {
+    red[0][warp] = ws;
+    red[1][warp] = ts;
+    red[2][warp] = tn;
+  }
   __syncthreads();
-  float wsum = 0.f;
-  for (int k = 0; k < kTrainWarps; k++) wsum += red[k];
+  float wsum = 0.f, tsum = 0.f, tcnt = 0.f;
+  for (int k = 0; k < kTrainWarps; k++) {
+    wsum += red[0][k];
+    tsum += red[1][k];
+    tcnt += red[2][k];
+  }
   const float inv_w = wsum > 0.f ? 1.f / wsum : 0.f;
+  const float mu = tcnt > 0.f ? tsum / tcnt : 0.f;
   __syncthreads();
 
   constexpr float kB1 = 0.9f, kB2 = 0.999f, kEps = 1e-8f;
@@ -139,25 +168,19 @@ __global__ void __launch_bounds__(kTrainThreads)
     for (uint32_t base = warp * 32; base < S; base += kTrainThreads) {
       const uint32_t i = base + lane;
       const bool valid = i < S;
-      float f[kMlpIn], h[kMlpHidden], z[kMlpOut];
+      float f[kMlpIn], h[kMlpHidden], z[kMlpOut], dz[kMlpOut];
 #pragma unroll
       for (int k = 0; k < kMlpIn; k++) f[k] = valid ? X[(size_t)i * kMlpIn + k] : 0.f;
-      const int label = valid ? y[i] : 0;
       const float wi = valid ? w[i] * inv_w : 0.f;
       mlp_forward(p, f, h, z);
-      const float zmax = fmaxf(z[0], fmaxf(z[1], z[2]));
-      float e[kMlpOut], es = 0.f;
 #pragma unroll
       for (int o = 0; o < kMlpOut; o++) {
-        e[o] = expf(z[o] - zmax);
-        es += e[o];
+        const float t = valid ? T[(size_t)i * kMlpOut + o] : NAN;
+        const float e = isnan(t) ? 0.f : z[o] - (t - mu);
+        loss += wi * e * e;
+        dz[o] = 2.f * wi * e;
       }
-      const float zl = label == 0 ? z[0] : label == 1 ? z[1] : z[2];
-      loss += wi * (logf(es) - (zl - zmax));
       if (last) continue;
-      float dz[kMlpOut];
-#pragma unroll
-      for (int o = 0; o < kMlpOut; o++) dz[o] = wi * (e[o] / es - (o == label ? 1.f : 0.f));
       float dh[kMlpHidden];
 #pragma unroll
       for (int j = 0; j < kMlpHidden; j++) {
@@ -181,11 +204,11 @@ __global__ void __launch_bounds__(kTrainThreads)
     }
     if (last) {
       loss = warp_sum(loss);
-      if (lane == 0) red[warp] = loss;
+      if (lane == 0) red[0][warp] = loss;
       __syncthreads();
       if (threadIdx.x == 0) {
         float t = 0.f;
-        for (int k = 0; k < kTrainWarps; k++) t += red[k];
+        for (int k = 0; k < kTrainWarps; k++) t += red[0][k];
         if (loss_out) *loss_out = t;
       }
       break;
@@ -199,6 +222,8 @@ __global__ void __launch_bounds__(kTrainThreads)
         g += gpart[k][i];
         gpart[k][i] = 0.f;
       }
+      const bool weight = i < kOffB1 || (i >= kOffW2 && i < kOffB2);
+      if (weight) g += wd * p[i];
       m1[i] = kB1 * m1[i] + (1.f - kB1) * g;
       m2[i] = kB2 * m2[i] + (1.f - kB2) * g * g;
       const float mh = m1[i] / (1.f - b1t), vh = m2[i] / (1.f - b2t);
@@ -206,7 +231,9 @@ __global__ void __launch_bounds__(kTrainThreads)
     }
     __syncthreads();
   }
-  for (int i = threadIdx.x; i < kMlpParams; i += kTrainThreads) params_out[i] = p[i];
+  __syncthreads();
+  for (int i = threadIdx.x; i < kMlpParams; i += kTrainThreads)
+    params_out[i] = i >= kOffB2 ? p[i] + mu : p[i];
 }
 
 }  // namespace
@@ -232,47 +259,53 @@ void load_dispatch_model(stc_ctx* c, const float* params) {
   c->model_loaded = true;
 }
 
-void train_dispatcher(stc_ctx* c, const float* features, const int32_t* labels,
-                      const float* weights, uint32_t samples, uint32_t epochs, float lr,
+void train_dispatcher(stc_ctx* c, const float* features, const float* targets,
+                      const float* weights, uint32_t samples, uint32_t epochs, float lr, float wd,
                       uint64_t seed, float* params, float* loss) {
-  if (!features || !labels || !weights || !params)
+  if (!features || !targets || !weights || !params)
     fail(STC_ERR_INVALID_ARGUMENT, "null training array");
   if (samples == 0 || samples > kMaxTrainSamples)
     fail(STC_ERR_INVALID_ARGUMENT, "samples must be in [1, " + std::to_string(kMaxTrainSamples) + "]");
   if (epochs == 0 || epochs > 1000000) fail(STC_ERR_INVALID_ARGUMENT, "epochs must be in [1, 1e6]");
   if (!(lr > 0.f) || !std::isfinite(lr)) fail(STC_ERR_INVALID_ARGUMENT, "learning rate must be > 0");
+  if (!(wd >= 0.f) || !std::isfinite(wd)) fail(STC_ERR_INVALID_ARGUMENT, "weight decay must be >= 0");
   double wsum = 0.0;
+  uint64_t available = 0;
   for (uint32_t i = 0; i < samples; i++) {
-    if (labels[i] < 0 || labels[i] >= kMlpOut) fail(STC_ERR_INVALID_ARGUMENT, "label out of range");
     if (!(weights[i] >= 0.f) || !std::isfinite(weights[i]))
       fail(STC_ERR_INVALID_ARGUMENT, "weights must be finite and >= 0");
     for (int k = 0; k < kMlpIn; k++)
       if (!std::isfinite(features[(size_t)i * kMlpIn + k]))
         fail(STC_ERR_INVALID_ARGUMENT, "feature is not finite");
+    for (int o = 0; o < kMlpOut; o++) {
+      const float t = targets[(size_t)i * kMlpOut + o];
+      if (std::isnan(t)) continue;
+      if (!std::isfinite(t)) fail(STC_ERR_INVALID_ARGUMENT, "target is infinite");
+      available++;
+    }
     wsum += weights[i];
   }
   if (!(wsum > 0.0)) fail(STC_ERR_INVALID_ARGUMENT, "total weight must be > 0");
-  // Device layout: X[samples][kMlpIn], w[samples], y[samples], params, loss.
-  const size_t nX = (size_t)samples * kMlpIn;
-  float* base = buffer<float>(c, B_DISPATCH_TRAIN, nX + 2 * (size_t)samples + kMlpParams + 1);
+  if (!available) fail(STC_ERR_INVALID_ARGUMENT, "no available target");
+  // Device layout: X[samples][kMlpIn], T[samples][kMlpOut], w[samples], params, loss.
+  const size_t nX = (size_t)samples * kMlpIn, nT = (size_t)samples * kMlpOut;
+  float* base = buffer<float>(c, B_DISPATCH_TRAIN, nX + nT + samples + kMlpParams + 1);
   float* dX = base;
-  float* dw = dX + nX;
-  int32_t* dy = reinterpret_cast<int32_t*>(dw + samples);
-  float* dp = reinterpret_cast<float*>(dy + samples);
+  float* dT = dX + nX;
+  float* dw = dT + nT;
+  float* dp = dw + samples;
   float* dl = dp + kMlpParams;
   cudaStream_t st = c->stream;
   STC_CUDA(cudaMemcpyAsync(dX, features, nX * sizeof(float), cudaMemcpyHostToDevice, st));
+  STC_CUDA(cudaMemcpyAsync(dT, targets, nT * sizeof(float), cudaMemcpyHostToDevice, st));
   STC_CUDA(cudaMemcpyAsync(dw, weights, samples * sizeof(float), cudaMemcpyHostToDevice, st));
-  STC_CUDA(cudaMemcpyAsync(dy, labels, samples * sizeof(int32_t), cudaMemcpyHostToDevice, st));
-  k_mlp_train<<<1, kTrainThreads, 0, st>>>(dX, dy, dw, samples, epochs, lr, seed, dp, dl);
+  k_mlp_train<<<1, kTrainThreads, 0, st>>>(dX, dT, dw, samples, epochs, lr, wd, seed, dp, dl);
   STC_CUDA(cudaGetLastError());
   float h_loss = 0.f;
   STC_CUDA(cudaMemcpyAsync(params, dp, kMlpParams * sizeof(float), cudaMemcpyDeviceToHost, st));
   STC_CUDA(cudaMemcpyAsync(&h_loss, dl, sizeof(float), cudaMemcpyDeviceToHost, st));
   STC_CUDA(cudaStreamSynchronize(st));
   if (loss) *loss = h_loss;
-  // The training buffer doubles as the model's parameter buffer: a loaded
-  // model's tables are already on the device and stay valid.
 }
 
 }  // namespace stc

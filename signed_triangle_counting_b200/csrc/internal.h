@@ -75,7 +75,8 @@ constexpr size_t kTableBytes = 256 * kTableClasses;
 static_assert(kTableBytes == STC_DISPATCH_CELLS, "one table byte per dispatch cell");
 
 // The dispatcher's multilayer perceptron: STC_DISPATCH_FEATURES inputs, one
-// hidden ReLU layer, one logit per strategy (MERGE, HASH, SEARCH).
+// hidden ReLU layer, one predicted log2 cost per strategy (MERGE, HASH,
+// SEARCH).
 // Parameter layout: W1[hidden][in], b1[hidden], W2[out][hidden], b2[out].
 constexpr int kMlpIn = STC_DISPATCH_FEATURES;
 constexpr int kMlpHidden = 16;
@@ -190,8 +191,8 @@ void fixed_dispatch_tables(uint8_t* out);
 void dispatch_features(float* out);
 const uint8_t* dispatch_tables(stc_ctx* c, const CountConfig& cfg);
 void load_dispatch_model(stc_ctx* c, const float* params);
-void train_dispatcher(stc_ctx* c, const float* features, const int32_t* labels,
-                      const float* weights, uint32_t samples, uint32_t epochs, float lr,
+void train_dispatcher(stc_ctx* c, const float* features, const float* targets,
+                      const float* weights, uint32_t samples, uint32_t epochs, float lr, float wd,
                       uint64_t seed, float* params, float* loss);
 
 uint64_t* counters(stc_ctx* c);

@@ -9,8 +9,9 @@ counts, so a dispatch table changes only speed.
 
 * ``record`` runs the timing recorder once per forced strategy: exhaustive
   per-cell timing of one graph.
-* ``samples`` turns a recording into training rows: the cell's features, its
-  fastest strategy as the label, and the cycles at stake as the weight.
+* ``samples`` turns a recording into training rows: the cell's features, the
+  measured log2 cycles per arc of each strategy as targets, and a weight that
+  grows with the cell's number of arcs.
 * ``train`` fits the perceptron on the device (``stc_dispatcher_train``).
 * ``regret`` judges any table against a recording: the time it would spend
   divided by the time of the per-cell best choice (1.0 = no regret).
@@ -32,7 +33,7 @@ from . import _capi, dispatch_features, synth
 STRATEGIES = ("merge", "hash", "search")  # label k is strategy code k + 1
 GIANT = 3                                  # class index whose lists stage no hash
 DEFAULT_MODEL = Path(__file__).resolve().parent / "dispatch_model.json"
-FORMAT_VERSION = 1
+FORMAT_VERSION = 2
 
 
 def record(ctx, src, dst, sign) -> dict:
@@ -66,22 +67,23 @@ def cell_costs(rec) -> np.ndarray:
     return cost
 
 
-def samples(rec, min_arcs: int = 32):
-    """Training rows of a recording: (features, labels, weights, cells).
+def samples(rec, min_arcs: int = 32, weight_power: float = 0.5):
+    """Training rows of a recording: (features, targets, weights, cells).
 
-    Only cells with at least ``min_arcs`` arcs are kept.  Label = fastest
-    strategy; weight = arcs x (slowest - fastest) mean cycles over the
-    available strategies, normalised to sum 1."""
+    Only cells with at least ``min_arcs`` arcs are kept.  Targets = measured
+    log2 cycles per arc of each strategy (NaN where unavailable); weight =
+    arcs ** ``weight_power``, normalised to sum 1 (0.5 keeps the busiest
+    cells first without letting a handful of them decide alone)."""
     arcs = rec["arcs"]
     cost = cell_costs(rec)
     cells = np.nonzero(arcs >= min_arcs)[0]
-    c = cost[:, cells]
-    labels = np.argmin(c, axis=0).astype(np.int32)
-    finite = np.where(np.isfinite(c), c, -np.inf)
-    stake = arcs[cells] * (finite.max(axis=0) - c.min(axis=0))
-    w = stake / stake.sum() if stake.sum() > 0 else np.full(len(cells), 1.0 / max(1, len(cells)))
+    c = cost[:, cells].T
+    with np.errstate(divide="ignore"):
+        targets = np.where(np.isfinite(c) & (c > 0), np.log2(np.where(c > 0, c, 1.0)), np.nan)
+    w = arcs[cells] ** weight_power
+    w = w / w.sum() if w.sum() > 0 else w
     X = dispatch_features()[cells]
-    return X, labels, w.astype(np.float32), cells
+    return X, targets.astype(np.float32), w.astype(np.float32), cells
 
 
 def regret(rec, tables) -> dict:
@@ -101,23 +103,29 @@ def regret(rec, tables) -> dict:
     return {"cycles": spent, "best_cycles": best, "ratio": spent / best if best else 1.0}
 
 
-def train(ctx, rec, *, epochs: int = 3000, lr: float = 0.02, seed: int = 1, min_arcs: int = 32):
-    """Trains on a recording; returns (params, info)."""
-    X, y, w, cells = samples(rec, min_arcs)
-    params, loss = ctx.train_dispatcher(X, y, w, epochs=epochs, lr=lr, seed=seed)
+def train(ctx, rec, *, epochs: int = 3000, lr: float = 0.02, weight_decay: float = 1e-3,
+          seed: int = 1, min_arcs: int = 32, weight_power: float = 0.5):
+    """Trains on a recording and loads the model into ``ctx``; returns
+    (params, info).  ``weighted_accuracy``: the weight of the training cells
+    whose table entry is their measured fastest strategy."""
+    X, T, w, cells = samples(rec, min_arcs, weight_power)
+    params, loss = ctx.train_dispatcher(X, T, w, epochs=epochs, lr=lr, weight_decay=weight_decay,
+                                        seed=seed)
     ctx.set_dispatch_model(params)
     pred = ctx.dispatch_tables("learned").reshape(-1)[cells].astype(np.int64) - 1
-    giant = cells // 256 == GIANT
-    pred = np.where(giant & (pred == 1), 0, pred)
-    acc = float((w * (pred == y)).sum())
+    best = np.argmin(np.where(np.isnan(T), np.inf, T), axis=1)
+    acc = float((w * (pred == best)).sum())
     info = {"samples": int(len(cells)), "loss": loss, "weighted_accuracy": acc,
-            "epochs": epochs, "lr": lr, "seed": seed, "min_arcs": min_arcs}
+            "objective": "log2 cycles per arc, weighted squared error", "epochs": epochs,
+            "lr": lr, "weight_decay": weight_decay, "seed": seed, "min_arcs": min_arcs,
+            "weight_power": weight_power}
     return params, info
 
 
 def save(path, params, meta: dict) -> None:
     doc = {"format": FORMAT_VERSION, "kind": "stc-dispatch-mlp",
-           "layout": "W1[16][6], b1[16], W2[3][16], b2[3]",
+           "layout": "W1[16][6], b1[16], W2[3][16], b2[3]; outputs: log2 cycles per arc "
+                     "of merge, hash, search",
            "params": [float(x) for x in np.asarray(params, np.float32)]}
     doc.update(meta)
     Path(path).write_text(json.dumps(doc, indent=1) + "\n")
@@ -144,14 +152,18 @@ def union(el, offsets, ns):
     return el.src + shift, el.dst + shift, el.sign
 
 
-def training_graphs(batch_graphs: int = 512):
+def training_graphs(batch_graphs: int = 4096, group: int = 512):
     """The training inputs: the Delaunay mesh (1M points, 20% deleted) and
-    the first ``batch_graphs`` graphs of the 4,096-graph batch as one union."""
+    the first ``batch_graphs`` graphs of the 4,096-graph batch, recorded as
+    unions of ``group`` graphs."""
     d = synth.workload(2)
     yield "workload2", (d.src, d.dst, d.sign)
+    del d
     specs = synth.batch_specs(4096)
-    el, offs = synth.batch_packed(specs, 0, batch_graphs)
-    yield f"workload4[0:{batch_graphs}]", union(el, offs, [s["n"] for s in specs[:batch_graphs]])
+    for g0 in range(0, batch_graphs, group):
+        g1 = min(batch_graphs, g0 + group)
+        el, offs = synth.batch_packed(specs, g0, g1)
+        yield f"workload4[{g0}:{g1}]", union(el, offs, [s["n"] for s in specs[g0:g1]])
 
 
 def _main() -> None:
@@ -162,7 +174,7 @@ def _main() -> None:
     ap.add_argument("--model", default=None)
     ap.add_argument("--workload", type=int, default=3)
     ap.add_argument("--epochs", type=int, default=3000)
-    ap.add_argument("--batch-graphs", type=int, default=512)
+    ap.add_argument("--batch-graphs", type=int, default=4096)
     ap.add_argument("--save-recording", default=None,
                     help="write the per-cell recordings to this .npz file")
     a = ap.parse_args()

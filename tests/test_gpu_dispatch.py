@@ -77,14 +77,16 @@ def test_fixed_tables_and_fallback(ctx):
 
 
 def numpy_tables(params):
+    """The inference kernel restated: least predicted cost, no HASH in the
+    giant class."""
     p = np.asarray(params, np.float64)
     W1, b1 = p[:96].reshape(16, 6), p[96:112]
     W2, b2 = p[112:160].reshape(3, 16), p[160:163]
     X = stc.dispatch_features().astype(np.float64)
     z = np.maximum(X @ W1.T + b1, 0) @ W2.T + b2
     giant = np.arange(len(X)) // 256 == 3
-    z[giant, 1] = -np.inf
-    return np.argmax(z, axis=1) + 1, np.sort(z, axis=1)
+    z[giant, 1] = np.inf
+    return np.argmin(z, axis=1) + 1, np.sort(z, axis=1)
 
 
 def test_inference_matches_numpy(ctx):
@@ -94,43 +96,55 @@ def test_inference_matches_numpy(ctx):
         ctx.set_dispatch_model(params)
         got = ctx.dispatch_tables("learned").reshape(-1)
         want, zs = numpy_tables(params)
-        close = (zs[:, -1] - zs[:, -2]) < 1e-4  # near ties may round either way
+        close = (zs[:, 1] - zs[:, 0]) < 1e-4  # near ties may round either way
         assert ((got == want) | close).all(), trial
         assert set(np.unique(got)) <= {1, 2, 3}
         assert not (got[768:] == 2).any()  # giant: never HASH
     ctx.set_dispatch_model(None)
 
 
-def rule_samples():
-    X = stc.dispatch_features()
-    y = (fixed_rule().reshape(-1) - 1).astype(np.int32)
-    cells = np.arange(768)  # staged classes, where all three strategies exist
-    w = np.full(len(cells), 1.0 / len(cells), np.float32)
-    return X[cells], y[cells], w
+def synthetic_costs():
+    """log2 cycles per arc of a made-up cost model over every cell:
+    merge ~ |A'| + |B|, hash ~ 2 |B|, search ~ 4 |A'| log |B|; HASH is
+    unavailable (NaN) in the giant class."""
+    cell = np.arange(_capi.DISPATCH_CELLS)
+    a, b = ((cell >> 4) & 15).astype(float), (cell & 15).astype(float)
+    T = np.stack([np.log2(2 ** a + 2 ** b), 1 + b, 2 + a + np.log2(1 + b)], axis=1)
+    T[768:, 1] = np.nan
+    return stc.dispatch_features(), T.astype(np.float32)
 
 
 def test_training_fits_and_is_deterministic(ctx):
-    X, y, w = rule_samples()
-    p1, loss1 = ctx.train_dispatcher(X, y, w, epochs=3000, lr=0.02, seed=3)
-    p2, loss2 = ctx.train_dispatcher(X, y, w, epochs=3000, lr=0.02, seed=3)
+    X, T = synthetic_costs()
+    w = np.full(len(X), 1.0 / len(X), np.float32)
+    p1, loss1 = ctx.train_dispatcher(X, T, w, epochs=3000, lr=0.02, seed=3)
+    p2, loss2 = ctx.train_dispatcher(X, T, w, epochs=3000, lr=0.02, seed=3)
     np.testing.assert_array_equal(p1, p2)
     assert loss1 == loss2
-    _, loss0 = ctx.train_dispatcher(X, y, w, epochs=1, lr=0.02, seed=3)
-    assert loss1 < 0.3 * loss0
+    _, loss0 = ctx.train_dispatcher(X, T, w, epochs=1, lr=0.02, seed=3)
+    assert loss1 < 0.05 * loss0
     ctx.set_dispatch_model(p1)
-    pred = ctx.dispatch_tables("learned").reshape(-1)[:768] - 1
-    assert (pred == y).mean() > 0.95
+    pred = ctx.dispatch_tables("learned").reshape(-1)
+    best = np.argmin(np.where(np.isnan(T), np.inf, T), axis=1) + 1
+    margin = np.sort(np.where(np.isnan(T), np.inf, T), axis=1)
+    clear = margin[:, 1] - margin[:, 0] > 0.25  # cells whose best strategy is clear
+    assert (pred[clear] == best[clear]).mean() > 0.97
+    assert not (pred[768:] == 2).any()
     ctx.set_dispatch_model(None)
 
 
 def test_training_rejects_bad_input(ctx):
-    X, y, w = rule_samples()
-    bad = y.copy()
-    bad[0] = 3
+    X, T = synthetic_costs()
+    w = np.full(len(X), 1.0 / len(X), np.float32)
+    bad = T.copy()
+    bad[0, 0] = np.inf
     with pytest.raises(stc.StcError):
         ctx.train_dispatcher(X, bad, w)
     with pytest.raises(stc.StcError):
-        ctx.train_dispatcher(X, y, -w)
+        ctx.train_dispatcher(X, T, -w)
+    with pytest.raises(stc.StcError):
+        ctx.train_dispatcher(np.zeros((5000, 6), np.float32), np.zeros((5000, 3), np.float32),
+                             np.ones(5000, np.float32))
     with pytest.raises(stc.StcError):
         ctx.set_dispatch_model(np.full(_capi.DISPATCH_MODEL_PARAMS, np.nan, np.float32))
 
@@ -150,7 +164,9 @@ def test_shipped_model(ctx):
     model = ctx.load_dispatch_model()
     t = ctx.dispatch_tables("learned")
     assert set(np.unique(t)) <= {1, 2, 3} and not (t[3] == 2).any()
-    assert model["weighted_accuracy"] > 0.9
+    # Judged by regret on its training recordings (near-ties make per-cell
+    # accuracy a poor measure): learned must beat the fixed tables.
+    assert model["train_regret_learned"] < model["train_regret_fixed"]
     el = GRAPHS["skew"]()
     want = oracle.count_arrays(el.src, el.dst, el.sign)
     assert ctx.count(el.src, el.dst, el.sign, dispatch="learned").as_tuple() == want
