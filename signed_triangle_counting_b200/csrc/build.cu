@@ -100,22 +100,68 @@ struct UniqueEmit {
   }
 };
 
-// Undirected degree over unique keys; the min endpoint arrives in runs (the
-// keys are sorted by it), so lanes sharing it add once.
-__global__ void k_degree(const uint64_t* __restrict__ keys, uint64_t mu, uint32_t bits,
-                         uint32_t* __restrict__ deg) {
+// Undirected degree of every vertex from the sorted unique keys
+// (min << bits | max).  The min endpoints of consecutive keys repeat, so a
+// warp adds each run with one atomic.  The max endpoints are scattered and a
+// few hubs may own millions of them, which would serialise on one address; so
+// each CTA counts them in a shared-memory table that it flushes every tile of
+// kDegTile keys, adding one global atomic per distinct vertex and tile (a
+// vertex that finds no free slot within kDegProbes probes is added directly).
+constexpr int kDegTile = 1024;
+constexpr int kDegSlots = 2048;  // load <= 1/2 per tile
+constexpr int kDegProbes = 8;
+
+__global__ void __launch_bounds__(kThreads) k_degree(const uint64_t* __restrict__ keys, uint64_t mu,
+                                                     uint32_t bits, uint32_t* __restrict__ deg) {
+  __shared__ uint32_t tkey[kDegSlots], tcnt[kDegSlots];
+  constexpr uint32_t kFree = 0xFFFFFFFFu;
+  for (int i = threadIdx.x; i < kDegSlots; i += kThreads) {
+    tkey[i] = kFree;
+    tcnt[i] = 0;
+  }
+  __syncthreads();
   const uint64_t idmask = (1ull << bits) - 1;
-  const uint64_t wstride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < mu;
-       base += wstride) {
-    const uint64_t i = base + lane_id();
-    const bool valid = i < mu;
-    const uint64_t k = valid ? keys[i] : 0;
-    const uint32_t a = valid ? (uint32_t)((k >> bits) & idmask) : 0xFFFFFFFFu;
-    const uint32_t b = (uint32_t)(k & idmask);
-    const unsigned peers = __match_any_sync(kFull, a);
-    if (valid && (peers & lanemask_lt()) == 0) atomicAdd(deg + a, (uint32_t)__popc(peers));
-    if (valid) atomicAdd(deg + b, 1u);
+  const uint64_t tiles = (mu + kDegTile - 1) / kDegTile;
+  for (uint64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+#pragma unroll
+    for (int r = 0; r < kDegTile / kThreads; r++) {
+      const uint64_t i = t * kDegTile + (uint64_t)r * kThreads + threadIdx.x;
+      const bool valid = i < mu;
+      const uint64_t k = valid ? keys[i] : 0;
+      const uint32_t a = valid ? (uint32_t)((k >> bits) & idmask) : kFree;
+      const uint32_t b = valid ? (uint32_t)(k & idmask) : kFree;
+      const unsigned pa = __match_any_sync(kFull, a);
+      if (valid && (pa & lanemask_lt()) == 0) atomicAdd(deg + a, (uint32_t)__popc(pa));
+      const unsigned pb = __match_any_sync(kFull, b);
+      if (valid && (pb & lanemask_lt()) == 0) {
+        const uint32_t add = (uint32_t)__popc(pb);
+        uint32_t slot = (b * 0x9E3779B1u) >> (32 - 11);
+        bool placed = false;
+        for (int p = 0; p < kDegProbes && !placed; p++) {
+          uint32_t cur = tkey[slot];
+          if (cur == kFree) {  // claim the slot, or see who claimed it first
+            const uint32_t old = atomicCAS(&tkey[slot], kFree, b);
+            cur = old == kFree ? b : old;
+          }
+          if (cur == b) {
+            atomicAdd(&tcnt[slot], add);
+            placed = true;
+          }
+          slot = (slot + 1) & (kDegSlots - 1);
+        }
+        if (!placed) atomicAdd(deg + b, add);
+      }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kDegSlots; i += kThreads) {
+      const uint32_t v = tkey[i];
+      if (v != kFree) {
+        atomicAdd(deg + v, tcnt[i]);
+        tkey[i] = kFree;
+        tcnt[i] = 0;
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -391,7 +437,7 @@ void build_graph(stc_ctx* c, const uint32_t* d_src, const uint32_t* d_dst, const
     STC_CUDA(cudaMemsetAsync(g.deg, 0, (size_t)g.n * sizeof(uint32_t), st));
     STC_CUDA(cudaMemsetAsync(g.fdeg, 0, (size_t)g.n * sizeof(uint32_t), st));
     if (g.m_unique) {
-      k_degree<<<grid_for(g.m_unique, 4), kThreads, 0, st>>>(g.ukeys, g.m_unique, g.bits, g.deg);
+      k_degree<<<grid_for(g.m_unique, 16), kThreads, 0, st>>>(g.ukeys, g.m_unique, g.bits, g.deg);
       c->launches++;
     }
     uint64_t* va = buffer<uint64_t>(c, B_VKEYS_A, g.n);
@@ -530,7 +576,7 @@ void build_graph_batch(stc_ctx* c, const uint32_t* d_src, const uint32_t* d_dst,
     STC_CUDA(cudaMemsetAsync(g.deg, 0, (size_t)g.n * sizeof(uint32_t), st));
     STC_CUDA(cudaMemsetAsync(g.fdeg, 0, (size_t)g.n * sizeof(uint32_t), st));
     if (g.m_unique) {
-      k_degree<<<grid_for(g.m_unique, 4), kThreads, 0, st>>>(g.ukeys, g.m_unique, g.bits, g.deg);
+      k_degree<<<grid_for(g.m_unique, 16), kThreads, 0, st>>>(g.ukeys, g.m_unique, g.bits, g.deg);
       c->launches++;
     }
     uint64_t* va = buffer<uint64_t>(c, B_VKEYS_A, g.n);

@@ -435,12 +435,16 @@ __device__ __forceinline__ void search_pass(const Csr& g, const StageMem& m, uin
 
 // ------------------------------------------------------ arc timing ----
 // Timing recorder (CountConfig::arc_cycles): per dispatch cell
-// (class, bucket |A'|, bucket |B|), the SM cycles a warp spent on each arc
-// and the number of arcs.  In this mode every arc is processed alone by one
-// warp, timed from the first load of its B to the last count it adds, so
-// three runs with the strategy forced give every cell's cost under every
-// strategy: the training data of the learned dispatcher and the judge of a
-// dispatch table's regret.
+// (class, bucket |A'|, bucket |B|), the SM cycles spent on its arcs and the
+// number of arcs.  In this mode every arc is processed alone by one warp,
+// timed from the first load of its B to the last count it adds, so three runs
+// with the strategy forced give every cell's cost under every strategy: the
+// training data of the learned dispatcher and the judge of a dispatch
+// table's regret.  The counting kernels proper pack the int4 chunks of all
+// HASH and MERGE arcs of a list into one stream that keeps every lane busy,
+// so such an arc of c chunks is charged its share of the lanes it would
+// occupy there, c / (32 ceil(c / 32)) of the warp's time; a SEARCH arc holds
+// a whole warp in both modes and is charged the warp's time.
 struct ArcTimes {
   unsigned long long* cycles;  // kTableClasses * 256 cells
   unsigned long long* arcs;
@@ -484,7 +488,7 @@ __device__ __forceinline__ void timed_pass(const Csr& g, const StageMem& m, uint
   for (uint32_t k = warp; k + 1 < d; k += warps) {
     const uint32_t st = m.st[k];
     if (st == kNoArc) continue;
-    const uint32_t lo = m.lo[k], blen = m.hi[k] - lo;
+    const uint32_t lo = m.lo[k], hi = m.hi[k], blen = hi - lo;
     __syncwarp();
     const long long t0 = clock_after(0);
     if (st == STC_STRATEGY_SEARCH)
@@ -493,9 +497,13 @@ __device__ __forceinline__ void timed_pass(const Csr& g, const StageMem& m, uint
       arc_stream(g, m, d, k, lane, geo, pc);
     // The arc's time is the latest lane's (each lane stops its clock once its
     // own counts are in).
-    const unsigned dt = __reduce_max_sync(kFull, (unsigned)(clock_after(pc.w) - t0));
+    unsigned dt = __reduce_max_sync(kFull, (unsigned)(clock_after(pc.w) - t0));
+    if (st != STC_STRATEGY_SEARCH) {  // lane share in the packed stream
+      const uint32_t chunks = ((hi + 3) >> 2) - (lo >> 2);
+      dt = (unsigned)((unsigned long long)dt * chunks / (32ull * ((chunks + 31) >> 5)));
+    }
     pc.drain(tc);
-    if (lane == 0) record_arc(at, tclass, d - k - 1, blen, dt);
+    if (lane == 0) record_arc(at, tclass, d - k - 1, blen, max(dt, 1u));
   }
 }
 

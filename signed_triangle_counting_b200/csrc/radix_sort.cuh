@@ -52,7 +52,7 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_upsweep(
   for (uint64_t base = begin + warp * 32; base < end; base += kSortThreads) {
     const uint64_t i = base + lane;
     const uint32_t d = i < end ? (uint32_t)(__ldcs(keys + i) >> shift) & dmask : kRadix;
-    const unsigned peers = __match_any_sync(kFull, d);
+    const unsigned peers = match_label<9>(d);
     if ((peers & lanemask_lt()) == 0) hist[warp][d] += __popc(peers);
     __syncwarp();
   }
@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_radix_downsweep(
     }
 #pragma unroll
     for (int j = 0; j < kSortItems; j++) {
-      const unsigned peers = __match_any_sync(kFull, dg[j]);
+      const unsigned peers = match_label<9>(dg[j]);
       const uint32_t base = whist[warp][dg[j]];
       const uint32_t below = __popc(peers & lt);
       __syncwarp();

@@ -55,6 +55,20 @@ __device__ __forceinline__ T block_exclusive_scan(T v, T* smem, T& total) {
   return r;
 }
 
+// Lanes of the warp holding the same BITS-bit label as this lane, computed
+// with one ballot per label bit (a cheaper warp multi-split than
+// __match_any_sync).  All 32 lanes must call it; labels must fit BITS bits.
+template <int BITS>
+__device__ __forceinline__ unsigned match_label(uint32_t label) {
+  unsigned peers = kFull;
+#pragma unroll
+  for (int b = 0; b < BITS; b++) {
+    const unsigned set = __ballot_sync(kFull, (label >> b) & 1u);
+    peers &= ((label >> b) & 1u) ? set : ~set;
+  }
+  return peers;
+}
+
 __host__ __device__ __forceinline__ uint32_t bit_width64(uint64_t x) {
   uint32_t b = 0;
   while (b < 64 && (x >> b) != 0) b++;
