@@ -163,6 +163,22 @@ stc_status stc_count(stc_ctx* ctx, const uint32_t* src, const uint32_t* dst,
                      const int8_t* sign, uint64_t m, const stc_opts* opts,
                      stc_counts* out);
 
+/* One shard of stc_count, for counting one graph on several GPUs (one
+ * process per GPU, each building the same forward CSR; no counterpart in the
+ * reference, whose programs use one machine).  Shard `shard` of `shards`
+ * (shards <= 65535) counts only the triangles whose lowest vertex in
+ * (degree, id) order has its rank in the shard's range; the ranges split
+ * rank space into contiguous pieces of about equal merge-model cost (vertex
+ * u costs 1 + the sum over its forward arcs u -> v of d+(u) + d+(v),
+ * saturated at 2^32 - 1; shard s starts at the first rank whose cost prefix
+ * reaches ceil(total * s / shards)).  The shards' counts add up to
+ * stc_count's, so the caller sums them across processes (one all-reduce of
+ * four words).  `range_out` (optional, 2 words) receives the shard's rank
+ * range [lo, hi). */
+stc_status stc_count_shard(stc_ctx* ctx, const uint32_t* src, const uint32_t* dst,
+                           const int8_t* sign, uint64_t m, const stc_opts* opts, uint32_t shard,
+                           uint32_t shards, stc_counts* out, uint64_t* range_out);
+
 /* build_forward_csr + sort_adj_lists (MC/graph_io.h:231-402,
  * MC/tc_serial.cpp:33-93) on the GPU; the result is returned in host memory
  * in the reference's layout.  Free with stc_free_forward_csr. */

@@ -231,6 +231,28 @@ class Context:
         _check(lib().stc_count(self._h, ps, pd, pg, m, C.byref(o), C.byref(out)), self._h)
         return GlobalTriCounts(out.t0, out.t1, out.t2, out.t3)
 
+    def count_shard(self, src, dst, sign, shard: int, shards: int, *, strategy="auto",
+                    dispatch="fixed", stream=None, timing=True):
+        """Shard ``shard`` of ``shards`` of ``count`` (one graph on several
+        GPUs): returns (counts, (lo, hi)), the counts of the triangles whose
+        lowest-ranked vertex has its rank in [lo, hi).  The shards' counts add
+        up to ``count``'s."""
+        dev = hasattr(src, "is_cuda") and src.is_cuda
+        if dev:
+            m = int(src.numel())
+            if stream is None:
+                import torch
+                stream = torch.cuda.current_stream(src.device).cuda_stream
+        else:
+            src, dst, sign = _host_arrays(src, dst, sign)
+            m = len(src)
+        out = _capi.stc_counts()
+        rng = (C.c_uint64 * 2)()
+        o = self._opts(strategy, dispatch, dev, timing, stream)
+        _check(lib().stc_count_shard(self._h, _ptr(src), _ptr(dst), _ptr(sign), m, C.byref(o),
+                                     shard, shards, C.byref(out), rng), self._h)
+        return GlobalTriCounts(out.t0, out.t1, out.t2, out.t3), (int(rng[0]), int(rng[1]))
+
     def count_edge_list(self, el: EdgeList, **kw) -> GlobalTriCounts:
         return self.count(el.src, el.dst, el.sign, **kw)
 

@@ -93,6 +93,9 @@ SIGNATURES = [
     ("stc_free_edge_list", None, [C.POINTER(stc_edge_list)]),
     ("stc_count", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64,
                             C.POINTER(stc_opts), C.POINTER(stc_counts)]),
+    ("stc_count_shard", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64,
+                                  C.POINTER(stc_opts), C.c_uint32, C.c_uint32,
+                                  C.POINTER(stc_counts), u64p]),
     ("stc_build_forward_csr", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_uint64, C.POINTER(stc_opts),
                                         C.POINTER(stc_forward_csr)]),

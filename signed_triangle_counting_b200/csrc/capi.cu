@@ -261,6 +261,30 @@ stc_status stc_count(stc_ctx* c, const uint32_t* src, const uint32_t* dst, const
   });
 }
 
+stc_status stc_count_shard(stc_ctx* c, const uint32_t* src, const uint32_t* dst,
+                           const int8_t* sign, uint64_t m, const stc_opts* o, uint32_t shard,
+                           uint32_t shards, stc_counts* out, uint64_t* range_out) {
+  if (!c || !out || shards == 0 || shards > 65535 || shard >= shards)
+    return STC_ERR_INVALID_ARGUMENT;
+  return guarded(c, [&] {
+    CountConfig cfg = count_config(o);
+    cfg.shard = shard;
+    cfg.shards = shards;
+    begin_call(c, o);
+    DeviceInput in = stage_input(c, src, dst, sign, m, o);
+    DeviceGraph g;
+    build_graph(c, in.src, in.dst, in.sign, m, g);
+    count_triangles(c, g, cfg);
+    mark(c, 5);
+    end_call(c, g, out);
+    if (range_out) {
+      const bool split = shards > 1 && g.n && g.m_fwd;
+      range_out[0] = split ? c->h_pinned[C_SHARD_LO] : (shard == 0 ? 0 : g.n);
+      range_out[1] = split ? c->h_pinned[C_SHARD_HI] : (shard == 0 ? g.n : g.n);
+    }
+  });
+}
+
 stc_status stc_build_forward_csr(stc_ctx* c, const uint32_t* src, const uint32_t* dst,
                                  const int8_t* sign, uint64_t m, const stc_opts* o,
                                  stc_forward_csr* out) {

@@ -40,6 +40,7 @@
 #include <mutex>
 
 #include "internal.h"
+#include "radix_sort.cuh"
 #include "stc_device.cuh"
 
 namespace stc {
@@ -606,11 +607,22 @@ struct ClassBounds {
 };
 constexpr int kClasses = 5;
 
+// Source vertices [range[0], range[1]) of rank space, or all n when `range`
+// is null (a sharded count reads its range from the counters).
+__device__ __forceinline__ void source_range(const unsigned long long* range, uint32_t n,
+                                             uint32_t& u0, uint32_t& u1) {
+  u0 = range ? (uint32_t)range[0] : 0u;
+  u1 = range ? (uint32_t)range[1] : n;
+}
+
 __global__ void k_classify_count(const uint64_t* __restrict__ off, uint32_t n, ClassBounds cb,
-                                 unsigned long long* __restrict__ ctr) {
+                                 unsigned long long* __restrict__ ctr,
+                                 const unsigned long long* __restrict__ range) {
   uint32_t cnt[kClasses] = {0, 0, 0, 0, 0};
   uint32_t dmax = 0;
-  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
+  uint32_t u0, u1;
+  source_range(range, n, u0, u1);
+  for (uint32_t u = u0 + blockIdx.x * blockDim.x + threadIdx.x; u < u1; u += gridDim.x * blockDim.x) {
     const uint32_t d = (uint32_t)(off[u + 1] - off[u]);
     const uint32_t c = cb.of(d);
     dmax = max(dmax, d);
@@ -630,11 +642,14 @@ __global__ void k_classify_count(const uint64_t* __restrict__ off, uint32_t n, C
 // counts are sums of integers).
 __global__ void k_classify_fill(const uint64_t* __restrict__ off, uint32_t n, ClassBounds cb,
                                 uint32_t* __restrict__ lists, const uint32_t* __restrict__ starts,
-                                unsigned long long* __restrict__ cursor) {
-  for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n;
+                                unsigned long long* __restrict__ cursor,
+                                const unsigned long long* __restrict__ range) {
+  uint32_t u0, u1;
+  source_range(range, n, u0, u1);
+  for (uint32_t base = u0 + blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < u1;
        base += gridDim.x * blockDim.x) {
     const uint32_t u = base + lane_id();
-    const uint32_t c = u < n ? cb.of((uint32_t)(off[u + 1] - off[u])) : 5u;
+    const uint32_t c = u < u1 ? cb.of((uint32_t)(off[u + 1] - off[u])) : 5u;
     const unsigned peers = __match_any_sync(kFull, c);
     const uint32_t leader = __ffs(peers) - 1;
     uint32_t pos = 0;
@@ -892,6 +907,63 @@ void launch_classes(cudaStream_t st, const Csr& csr, const uint32_t* lists, cons
   }
 }
 
+// ------------------------------------------------------------ shards ----
+// A shard of a count is a contiguous range of source vertices in rank space
+// chosen so that the shards carry about the same merge-model cost: vertex u
+// costs 1 + sum over v in N+(u) of (d+(u) + d+(v)), saturated at 2^32 - 1.
+// With P(r) the cost of the ranks below r, shard s of S starts at the first
+// rank r with P(r) >= ceil(P(n) s / S).  Every triangle is counted by the
+// shard of its lowest-ranked vertex, so the shards' counts add up to the
+// whole graph's.
+struct VertexCost {
+  const uint64_t* off;
+  const uint32_t* nbr;
+  __device__ uint32_t operator()(uint64_t u) const {
+    const uint64_t b = off[u], e = off[u + 1], du = e - b;
+    uint64_t cost = 1;
+    for (uint64_t i = b; i < e; i++) {
+      const uint32_t v = nbr[i];
+      cost += du + (off[v + 1] - off[v]);
+    }
+    return (uint32_t)(cost < 0xFFFFFFFFull ? cost : 0xFFFFFFFFull);
+  }
+};
+struct EmitPrefix {
+  uint64_t* pre;
+  __device__ void operator()(uint64_t i, uint64_t pos, uint32_t) const { pre[i] = pos; }
+};
+
+// Thread 0 writes the shard's first rank, thread 1 its end.
+__global__ void k_shard_bounds(const uint64_t* __restrict__ pre, uint32_t n, uint32_t shard,
+                               uint32_t shards, unsigned long long* __restrict__ ctr) {
+  if (threadIdx.x > 1) return;
+  const uint32_t s = shard + threadIdx.x;
+  uint32_t r = 0;
+  if (s >= shards) {
+    r = n;
+  } else if (s > 0) {
+    const uint64_t target = (pre[n] * s + shards - 1) / shards;
+    uint32_t lo = 0, hi = n;  // first r with pre[r] >= target (pre[n] = total)
+    while (lo < hi) {
+      const uint32_t mid = lo + ((hi - lo) >> 1);
+      if (pre[mid] < target) lo = mid + 1; else hi = mid;
+    }
+    r = lo;
+  }
+  ctr[C_SHARD_LO + threadIdx.x] = r;
+}
+
+// Writes the rank range of cfg.shard into the counters (device side only).
+void shard_range(stc_ctx* c, const DeviceGraph& g, uint32_t shard, uint32_t shards) {
+  uint64_t* pre = buffer<uint64_t>(c, B_SHARD_COST, (size_t)g.n + 1);
+  uint64_t* sums = buffer<uint64_t>(c, B_SCAN_SUMS, kMaxSortGrid + 1);
+  range_scan(VertexCost{g.off, g.nbr}, EmitPrefix{pre}, g.n, sums, c->stream, &c->launches);
+  STC_CUDA(cudaMemcpyAsync(pre + g.n, sums + range_partition(g.n, kScanTile, kMaxSortGrid).grid,
+                           sizeof(uint64_t), cudaMemcpyDeviceToDevice, c->stream));
+  k_shard_bounds<<<1, 32, 0, c->stream>>>(pre, g.n, shard, shards, (unsigned long long*)counters(c));
+  c->launches++;
+}
+
 }  // namespace
 
 // Fixed degree-threshold dispatch, the same for every class: SEARCH when B
@@ -938,6 +1010,11 @@ void count_triangles(stc_ctx* c, const DeviceGraph& g, const CountConfig& cfg) {
   const uint8_t* d_table = dispatch_tables(c, cfg);
   const bool timed = cfg.arc_cycles != nullptr;
   const ArcTimes at{(unsigned long long*)cfg.arc_cycles, (unsigned long long*)cfg.arc_counts};
+  const unsigned long long* range = nullptr;
+  if (cfg.shards > 1) {
+    shard_range(c, g, cfg.shard, cfg.shards);
+    range = ctr + C_SHARD_LO;
+  }
 
   // Vertex classes (a forced strategy disables the tiny class, which only
   // implements the search form; so does timing, so that every strategy's
@@ -945,7 +1022,7 @@ void count_triangles(stc_ctx* c, const DeviceGraph& g, const CountConfig& cfg) {
   const bool tiny =
       !timed && (cfg.strategy == STC_STRATEGY_AUTO || cfg.strategy == STC_STRATEGY_SEARCH);
   const ClassBounds cb{tiny ? kTinyMax : 1u, kWarpCap, kBlockCap, kLargeCap};
-  k_classify_count<<<kSMs * 4, 256, 0, st>>>(g.off, g.n, cb, ctr);
+  k_classify_count<<<kSMs * 4, 256, 0, st>>>(g.off, g.n, cb, ctr, range);
   STC_CUDA(cudaMemcpyAsync(c->h_pinned + C_WORK, counters(c) + C_WORK,
                            (C_MAX_FDEG + 1 - C_WORK) * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
   STC_CUDA(cudaStreamSynchronize(st));
@@ -961,7 +1038,7 @@ void count_triangles(stc_ctx* c, const DeviceGraph& g, const CountConfig& cfg) {
   STC_CUDA(cudaMemcpyAsync(d_starts, starts, kClasses * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
   // Cursors of the fill, then the dynamic queues, live in C_WORK ...
   STC_CUDA(cudaMemsetAsync(counters(c) + C_WORK, 0, 8 * sizeof(uint64_t), st));
-  k_classify_fill<<<kSMs * 4, 256, 0, st>>>(g.off, g.n, cb, lists, d_starts, ctr + C_WORK);
+  k_classify_fill<<<kSMs * 4, 256, 0, st>>>(g.off, g.n, cb, lists, d_starts, ctr + C_WORK, range);
   STC_CUDA(cudaMemsetAsync(counters(c) + C_WORK, 0, 8 * sizeof(uint64_t), st));
   c->launches += 2;
 
@@ -1096,7 +1173,7 @@ extern "C" stc_status stc_count_oriented_csr_noalloc(const uint64_t* d_offsets,
   fixed_dispatch_tables(table);
   STC_NA(cudaMemcpyAsync(scr->table, table, sizeof(table), cudaMemcpyHostToDevice, st));
   const ClassBounds cb{kTinyMax, kWarpCap, kBlockCap, kLargeCap};
-  k_classify_count<<<kSMs * 4, 256, 0, st>>>(d_offsets, n, cb, ctr);
+  k_classify_count<<<kSMs * 4, 256, 0, st>>>(d_offsets, n, cb, ctr, nullptr);
   STC_NA(cudaMemcpyAsync(slots, ctr, sizeof(slots), cudaMemcpyDeviceToHost, st));
   STC_NA(cudaStreamSynchronize(st));
   const uint32_t max_fdeg = (uint32_t)slots[C_MAX_FDEG];
@@ -1110,7 +1187,8 @@ extern "C" stc_status stc_count_oriented_csr_noalloc(const uint64_t* d_offsets,
   uint32_t* d_starts = lists + starts[kClasses];
   STC_NA(cudaMemcpyAsync(d_starts, starts, kClasses * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
   STC_NA(cudaMemsetAsync(ctr + C_WORK, 0, 8 * sizeof(uint64_t), st));
-  k_classify_fill<<<kSMs * 4, 256, 0, st>>>(d_offsets, n, cb, lists, d_starts, ctr + C_WORK);
+  k_classify_fill<<<kSMs * 4, 256, 0, st>>>(d_offsets, n, cb, lists, d_starts, ctr + C_WORK,
+                                            nullptr);
   STC_NA(cudaMemsetAsync(ctr + C_WORK, 0, 8 * sizeof(uint64_t), st));
 
   const Csr csr{d_offsets, d_heads, d_signs, nullptr, n};

@@ -40,6 +40,7 @@ enum BufId {
   B_DISPATCH_FIXED,               // fixed dispatch tables (kTableBytes)
   B_DISPATCH_TRAIN,               // dispatcher training samples and parameters
   B_TIMES,                        // timing recorder: cycles and arcs per cell
+  B_SHARD_COST,                   // cost prefix of a sharded count (n + 1 words)
   B_COUNT_
 };
 
@@ -58,6 +59,8 @@ enum CounterSlot {
   C_WORK = 8,                  // dynamic work counters (8 slots)
   C_ERROR = 16,                // device error word (0 = ok)
   C_MAX_FDEG = 17,             // largest out-degree of the forward CSR
+  C_SHARD_LO = 18,             // rank range [lo, hi) of a sharded count
+  C_SHARD_HI = 19,
   C_SLOTS = 32
 };
 
@@ -181,6 +184,11 @@ struct CountConfig {
   // arc's SM cycles and one arc to its dispatch cell.
   uint64_t* arc_cycles = nullptr;
   uint64_t* arc_counts = nullptr;
+  // Sharded count: only source vertices of shard `shard` of `shards` (equal
+  // merge-model cost ranges of rank space); the range lands in
+  // C_SHARD_LO / C_SHARD_HI.
+  uint32_t shard = 0;
+  uint32_t shards = 1;
 };
 void count_triangles(stc_ctx* c, const DeviceGraph& g, const CountConfig& cfg);
 

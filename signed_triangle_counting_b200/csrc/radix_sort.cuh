@@ -1,10 +1,13 @@
 // Stable LSD radix sort of 64-bit keys over a bit window [lo, hi), plus the
-// range-partitioned scans the graph build uses.
+// range-partitioned scans the graph build and the sharded count use.  The
+// kernels have internal linkage: every translation unit that includes this
+// header gets its own copy.
 //
 // Design (B200): every pass is a reduce-then-scan over a fixed grid of
 // CTA-contiguous key ranges (4 CTAs per SM), so no kernel ever waits on
 // another CTA:
-//   upsweep   per-CTA digit histogram of its range      (reads 8 B/key)
+//   upsweep   per-CTA digit histogram of its range      (reads 8 B/key;
+//             per-warp shared-memory atomics)
 //   scan      one CTA turns [digit][cta] counts into offsets
 //   downsweep per 4096-key tile: warp-striped match.any ranking (stable),
 //             tile-local reorder through shared memory, coalesced scatter
@@ -25,6 +28,7 @@ constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys
 constexpr int kRadix = 256;
 constexpr int kMaxSortGrid = kSMs * 4;
+constexpr int kUpItems = 8;  // keys per thread per upsweep iteration
 
 struct RangePartition {
   uint32_t grid;     // CTAs
@@ -40,7 +44,7 @@ inline RangePartition range_partition(uint64_t m, uint64_t tile, uint32_t max_gr
   return RangePartition{(uint32_t)grid, per * tile};
 }
 
-__global__ void __launch_bounds__(kSortThreads) k_radix_upsweep(
+static __global__ void __launch_bounds__(kSortThreads) k_radix_upsweep(
     const uint64_t* __restrict__ keys, uint64_t m, uint64_t per_cta, int shift,
     uint32_t dmask, uint32_t* __restrict__ counts, uint32_t grid) {
   __shared__ uint32_t hist[kSortWarps][kRadix + 1];
@@ -49,12 +53,18 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_upsweep(
   __syncthreads();
   const uint64_t begin = (uint64_t)blockIdx.x * per_cta;
   const uint64_t end = begin + per_cta < m ? begin + per_cta : m;
-  for (uint64_t base = begin + warp * 32; base < end; base += kSortThreads) {
-    const uint64_t i = base + lane;
-    const uint32_t d = i < end ? (uint32_t)(__ldcs(keys + i) >> shift) & dmask : kRadix;
-    const unsigned peers = match_label<9>(d);
-    if ((peers & lanemask_lt()) == 0) hist[warp][d] += __popc(peers);
-    __syncwarp();
+  // kUpItems independent loads in flight per thread, then one shared-memory
+  // atomic per key into the warp's own histogram.
+  for (uint64_t base = begin + warp * 32 * kUpItems; base < end; base += kSortThreads * kUpItems) {
+    uint32_t d[kUpItems];
+#pragma unroll
+    for (int j = 0; j < kUpItems; j++) {
+      const uint64_t i = base + j * 32 + lane;
+      d[j] = i < end ? (uint32_t)(__ldcs(keys + i) >> shift) & dmask : kRadix;
+    }
+#pragma unroll
+    for (int j = 0; j < kUpItems; j++)
+      if (d[j] != kRadix) atomicAdd(&hist[warp][d[j]], 1u);
   }
   __syncthreads();
   for (unsigned d = tid; d < kRadix; d += kSortThreads) {
@@ -66,7 +76,7 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_upsweep(
 }
 
 // Exclusive scan of `n` 32-bit counts in place by one CTA of 1024 threads.
-__global__ void __launch_bounds__(1024) k_scan_counts(uint32_t* __restrict__ a, uint32_t n) {
+static __global__ void __launch_bounds__(1024) k_scan_counts(uint32_t* __restrict__ a, uint32_t n) {
   __shared__ uint32_t tmp[33];
   const uint32_t per = (n + 1023) / 1024;
   const uint32_t b = threadIdx.x * per, e = b + per < n ? b + per : n;
@@ -81,7 +91,7 @@ __global__ void __launch_bounds__(1024) k_scan_counts(uint32_t* __restrict__ a, 
   }
 }
 
-__global__ void __launch_bounds__(kSortThreads, 2) k_radix_downsweep(
+static __global__ void __launch_bounds__(kSortThreads, 2) k_radix_downsweep(
     const uint64_t* __restrict__ in, uint64_t* __restrict__ out, uint64_t m, uint64_t per_cta,
     int shift, uint32_t dmask, const uint32_t* __restrict__ offsets, uint32_t grid) {
   __shared__ uint64_t sbuf[kSortTile];
@@ -201,7 +211,7 @@ __global__ void __launch_bounds__(kScanThreads) k_range_reduce(F f, uint64_t n, 
 }
 
 // Exclusive scan of a[0, n) in place; a[n] receives the total.
-__global__ void __launch_bounds__(1024) k_scan_small(uint64_t* __restrict__ a, uint32_t n) {
+static __global__ void __launch_bounds__(1024) k_scan_small(uint64_t* __restrict__ a, uint32_t n) {
   __shared__ uint64_t tmp[33];
   const uint32_t per = (n + 1023) / 1024;
   const uint32_t b = threadIdx.x * per, e = b + per < n ? b + per : n;
