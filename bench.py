@@ -258,7 +258,9 @@ def run_gpu(args) -> None:
         offs_run = offs
     torch.cuda.synchronize()
     m_input = src.numel()
-    kw = dict(strategy=args.strategy, dispatch=args.dispatch, stream=stream.cuda_stream)
+    persistent = args.engine == "persistent" or (args.engine == "auto" and offs is not None)
+    kw = dict(strategy=args.strategy, dispatch=args.dispatch, stream=stream.cuda_stream,
+              persistent=persistent)
 
     def step():
         if offs_run is not None:
@@ -266,7 +268,8 @@ def run_gpu(args) -> None:
             if world > 1:
                 c = distributed.gather_batch(c, mine, G, device=dev)
         elif world > 1:
-            c = distributed.count(ctx, src, dst, sign, device=dev, **kw)
+            c = distributed.count(ctx, src, dst, sign, device=dev,
+                                  **{k: v for k, v in kw.items() if k != "persistent"})
         else:
             c = ctx.count(src, dst, sign, **kw)
         return c, ctx.last_stats()
@@ -325,7 +328,8 @@ def run_gpu(args) -> None:
     h_src, h_dst, h_sign = host_copy(src), host_copy(dst), host_copy(sign)
     pinned = h_src.is_pinned()
     torch.cuda.synchronize()
-    o = stc.Context._opts(args.strategy, args.dispatch, False, True, stream.cuda_stream)
+    o = stc.Context._opts(args.strategy, args.dispatch, False, True, stream.cuda_stream,
+                          persistent)
     G_run = len(offs_run) - 1 if offs_run is not None else 1
     out = (_capi.stc_counts * max(1, G_run))()
     ptrs = [C.c_void_p(h.data_ptr()) for h in (h_src, h_dst, h_sign)]
@@ -396,6 +400,7 @@ def run_gpu(args) -> None:
                        "m_unique": edges, "n": st.n if offs is None else None,
                        "strategy": args.strategy, "dispatch": args.dispatch,
                        "dispatch_model": model.get("trained_on") if model else None,
+                       "engine": "persistent (CUDA graph)" if persistent else "class kernels",
                        "l2": f"inputs {m_input * 9 / 1e9:.1f} GB per rank > 126 MB L2, no flush",
                        "parallelism": par},
             "exact": exact, "counts": counts_out,
@@ -429,6 +434,8 @@ def main() -> None:
     ap.add_argument("--strategy", default="auto", choices=["auto", "merge", "hash", "search"])
     ap.add_argument("--dispatch", default="fixed", choices=["fixed", "learned"])
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--engine", default="auto", choices=["auto", "persistent", "classes"],
+                    help="counting engine (auto: persistent for the batch, class kernels else)")
     ap.add_argument("--rmat-scale", type=int, default=24,
                     help="RMAT scale of workload 3 (24 = the benchmark; smaller for profiling)")
     args = ap.parse_args()

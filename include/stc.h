@@ -103,7 +103,11 @@ typedef enum stc_dispatch {
 /* Option flags. */
 #define STC_F_DEVICE_INPUT 0x1u /* input pointers are device pointers */
 #define STC_F_TIMING 0x2u       /* record per-stage device times (stc_ctx_last_stats) */
-#define STC_F_NO_SYNC 0x4u      /* leave results on device; stc_ctx_counts_device */
+#define STC_F_PERSISTENT 0x8u   /* count with the persistent engine: the device plans the
+                                   class worklists and one persistent kernel pulls lists
+                                   from a device work queue; the sequence is captured in a
+                                   CUDA graph once per set of buffers and replayed (on the
+                                   legacy default stream it is launched directly) */
 
 typedef struct stc_opts {
   uint32_t strategy; /* stc_strategy */

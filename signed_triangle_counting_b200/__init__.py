@@ -201,20 +201,22 @@ class Context:
 
     @staticmethod
     def _opts(strategy="auto", dispatch="fixed", device_input=False, timing=True,
-              stream: Optional[int] = None) -> _capi.stc_opts:
+              stream: Optional[int] = None, persistent=False) -> _capi.stc_opts:
         o = _capi.stc_opts()
         o.strategy = _capi.STRATEGY[strategy]
         o.dispatch = _capi.DISPATCH[dispatch]
-        o.flags = (_capi.F_DEVICE_INPUT if device_input else 0) | (_capi.F_TIMING if timing else 0)
+        o.flags = ((_capi.F_DEVICE_INPUT if device_input else 0) | (_capi.F_TIMING if timing else 0)
+                   | (_capi.F_PERSISTENT if persistent else 0))
         o.stream = C.c_void_p(stream) if stream else None
         return o
 
     def count(self, src, dst, sign, *, strategy="auto", dispatch="fixed", stream=None,
-              timing=True) -> GlobalTriCounts:
+              timing=True, persistent=False) -> GlobalTriCounts:
         """Whole path (dedup, orientation, CSR, intersection) on the GPU.
 
         Host numpy arrays are copied to the device; torch CUDA tensors
-        (uint32/int32 ids, int8 signs) are used in place."""
+        (uint32/int32 ids, int8 signs) are used in place.  ``persistent``
+        counts with the persistent engine replayed from a CUDA graph."""
         dev = hasattr(src, "is_cuda") and src.is_cuda
         if dev:
             m = int(src.numel())
@@ -227,7 +229,7 @@ class Context:
             m = len(src)
             ps, pd, pg = _ptr(src), _ptr(dst), _ptr(sign)
         out = _capi.stc_counts()
-        o = self._opts(strategy, dispatch, dev, timing, stream)
+        o = self._opts(strategy, dispatch, dev, timing, stream, persistent)
         _check(lib().stc_count(self._h, ps, pd, pg, m, C.byref(o), C.byref(out)), self._h)
         return GlobalTriCounts(out.t0, out.t1, out.t2, out.t3)
 
@@ -295,11 +297,11 @@ class Context:
         _check(lib().stc_count_forward_csr(self._h, C.byref(c), C.byref(o), C.byref(out)), self._h)
         return GlobalTriCounts(out.t0, out.t1, out.t2, out.t3)
 
-    def vertex_counts(self, src, dst, sign, *, strategy="auto") -> np.ndarray:
+    def vertex_counts(self, src, dst, sign, *, strategy="auto", persistent=False) -> np.ndarray:
         """Per-source counts cnt[4n] (tc_serial.cpp:141-158) as an (n, 4) array."""
         src, dst, sign = _host_arrays(src, dst, sign)
         n_out = C.c_uint32()
-        o = self._opts(strategy)
+        o = self._opts(strategy, persistent=persistent)
         n_bound = int(max(src.max(initial=0), dst.max(initial=0))) + 1 if len(src) else 0
         buf = np.zeros(4 * max(n_bound, 1), np.uint64)
         _check(lib().stc_vertex_counts(self._h, _ptr(src), _ptr(dst), _ptr(sign), len(src),
@@ -308,7 +310,7 @@ class Context:
         return buf[: 4 * n_out.value].reshape(-1, 4)
 
     def count_batch(self, graphs: Sequence[tuple], *, strategy="auto", dispatch="fixed",
-                    stream=None) -> list:
+                    stream=None, persistent=True) -> list:
         """Counts independent graphs given as (src, dst, sign) triples."""
         keep = []
         arr = (_capi.stc_graph * max(1, len(graphs)))()
@@ -326,12 +328,12 @@ class Context:
         if dev and stream is None:
             import torch
             stream = torch.cuda.current_stream(keep[0][0].device).cuda_stream
-        o = self._opts(strategy, dispatch, dev, True, stream)
+        o = self._opts(strategy, dispatch, dev, True, stream, persistent)
         _check(lib().stc_count_batch(self._h, arr, len(graphs), C.byref(o), outs), self._h)
         return [GlobalTriCounts(x.t0, x.t1, x.t2, x.t3) for x in outs[: len(graphs)]]
 
     def count_batch_packed(self, src, dst, sign, offsets, *, strategy="auto", dispatch="fixed",
-                           stream=None, timing=True) -> list:
+                           stream=None, timing=True, persistent=True) -> list:
         """Counts graphs stored back to back (graph g owns entries
         [offsets[g], offsets[g + 1]), ids local to the graph); numpy arrays
         are host input, torch CUDA tensors device input."""
@@ -345,7 +347,7 @@ class Context:
         else:
             src, dst, sign = _host_arrays(src, dst, sign)
         outs = (_capi.stc_counts * max(1, G))()
-        o = self._opts(strategy, dispatch, dev, timing, stream)
+        o = self._opts(strategy, dispatch, dev, timing, stream, persistent)
         _check(lib().stc_count_batch_packed(self._h, _ptr(src), _ptr(dst), _ptr(sign),
                                             offsets.ctypes.data_as(_capi.u64p), G, C.byref(o),
                                             outs), self._h)

@@ -77,7 +77,7 @@ DISPATCH_MODEL_PARAMS = 163
 DISPATCH = {"fixed": 0, "learned": 1}
 F_DEVICE_INPUT = 0x1
 F_TIMING = 0x2
-F_NO_SYNC = 0x4
+F_PERSISTENT = 0x8
 
 # (name, restype, argtypes) for every exported function of include/*.h.
 SIGNATURES = [

@@ -138,6 +138,7 @@ CountConfig count_config(const stc_opts* o) {
     if (o->dispatch > STC_DISPATCH_LEARNED) fail(STC_ERR_INVALID_ARGUMENT, "unknown dispatch");
     cfg.strategy = o->strategy;
     cfg.dispatch = o->dispatch;
+    cfg.persistent = (o->flags & STC_F_PERSISTENT) != 0;
   }
   return cfg;
 }
@@ -216,6 +217,7 @@ void stc_ctx_destroy(stc_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->own_stream) cudaStreamSynchronize(c->own_stream);
+  if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
   for (auto& b : c->bufs)
     if (b.p) cudaFree(b.p);
   for (auto& e : c->ev)
@@ -238,6 +240,10 @@ stc_status stc_ctx_trim(stc_ctx* c) {
   if (!c) return STC_ERR_INVALID_ARGUMENT;
   return guarded(c, [&] {
     STC_CUDA(cudaStreamSynchronize(c->own_stream));
+    if (c->graph_exec) {  // it refers to the buffers released below
+      STC_CUDA(cudaGraphExecDestroy(c->graph_exec));
+      c->graph_exec = nullptr;
+    }
     for (int i = 0; i < B_COUNT_; i++) {
       if (i == B_COUNTERS) continue;
       if (c->bufs[i].p) STC_CUDA(cudaFree(c->bufs[i].p));

@@ -37,6 +37,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstring>
 #include <mutex>
 
 #include "internal.h"
@@ -606,6 +607,10 @@ struct ClassBounds {
   }
 };
 constexpr int kClasses = 5;
+// Device plan of a persistent count: plan[c] = first list entry of class c
+// (plan[kClasses] = total), plan[kPlanCounts + c] = its vertex count.
+constexpr uint32_t kPlanCounts = 8;
+constexpr uint32_t kPlanWords = kPlanCounts + kClasses;
 
 // Source vertices [range[0], range[1]) of rank space, or all n when `range`
 // is null (a sharded count reads its range from the counters).
@@ -660,50 +665,87 @@ __global__ void k_classify_fill(const uint64_t* __restrict__ off, uint32_t n, Cl
 }
 
 // Tiny class: one thread per vertex, A in registers, B in global memory.
+// One tiny list (one thread): A in registers, a monotone binary search of
+// each later A' element in B.
+template <int TMAX, class Sink>
+__device__ __forceinline__ void tiny_vertex(const Csr& g, uint32_t u, const Sink& sink,
+                                            TypeCounts& tc) {
+  constexpr bool kVC = Sink::kPerVertex;
+  const uint64_t ub = g.off[u];
+  const uint32_t d = (uint32_t)(g.off[u + 1] - ub);
+  uint32_t a[TMAX];
+  uint32_t neg[TMAX];
+#pragma unroll
+  for (int i = 0; i < TMAX; i++) {
+    a[i] = i < (int)d ? g.nbr[ub + i] : kEmpty;
+    neg[i] = i < (int)d ? (g.sgn[ub + i] < 0) : 0u;
+  }
+  TypeCounts vc;
+#pragma unroll
+  for (int k = 0; k < TMAX - 1; k++) {
+    if (k + 1 >= (int)d) break;
+    const uint64_t vb = g.off[a[k]];
+    const uint32_t blen = (uint32_t)(g.off[a[k] + 1] - vb);
+    const uint32_t* b = g.nbr + vb;
+    uint32_t pos = 0;
+#pragma unroll
+    for (int i = k + 1; i < TMAX; i++) {
+      if (i >= (int)d || pos >= blen) break;
+      pos += lower_bound(b + pos, blen - pos, a[i]);
+      if (pos < blen && b[pos] == a[i]) {
+        const uint32_t t = neg[k] + neg[i] + (g.sgn[vb + pos] < 0);
+        if (kVC) vc.add(t); else tc.add(t);
+        pos++;
+      }
+    }
+  }
+  if (kVC) sink.put(u, vc.c);
+}
+
+// Tiny class: one thread per vertex, A in registers, B in global memory.
 template <int TMAX, class Sink>
 __global__ void __launch_bounds__(256) k_tiny(Csr g, const uint32_t* __restrict__ list, uint32_t cnt,
                                               unsigned long long* __restrict__ ctr, Sink sink) {
-  constexpr bool kVC = Sink::kPerVertex;
   TypeCounts tc;
-  for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < cnt; idx += gridDim.x * blockDim.x) {
-    const uint32_t u = list[idx];
-    const uint64_t ub = g.off[u];
-    const uint32_t d = (uint32_t)(g.off[u + 1] - ub);
-    uint32_t a[TMAX];
-    uint32_t neg[TMAX];
-#pragma unroll
-    for (int i = 0; i < TMAX; i++) {
-      a[i] = i < (int)d ? g.nbr[ub + i] : kEmpty;
-      neg[i] = i < (int)d ? (g.sgn[ub + i] < 0) : 0u;
-    }
-    TypeCounts vc;
-#pragma unroll
-    for (int k = 0; k < TMAX - 1; k++) {
-      if (k + 1 >= (int)d) break;
-      const uint64_t vb = g.off[a[k]];
-      const uint32_t blen = (uint32_t)(g.off[a[k] + 1] - vb);
-      const uint32_t* b = g.nbr + vb;
-      uint32_t pos = 0;
-#pragma unroll
-      for (int i = k + 1; i < TMAX; i++) {
-        if (i >= (int)d || pos >= blen) break;
-        pos += lower_bound(b + pos, blen - pos, a[i]);
-        if (pos < blen && b[pos] == a[i]) {
-          const uint32_t t = neg[k] + neg[i] + (g.sgn[vb + pos] < 0);
-          if (kVC) vc.add(t); else tc.add(t);
-          pos++;
-        }
-      }
-    }
-    if (kVC) sink.put(u, vc.c);
-  }
-  if (!kVC) flush_counts<256>(tc, ctr);
+  for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < cnt; idx += gridDim.x * blockDim.x)
+    tiny_vertex<TMAX>(g, list[idx], sink, tc);
+  if (!Sink::kPerVertex) flush_counts<256>(tc, ctr);
 }
 
 // Warp class: one warp per vertex, staged in the warp's slice of shared
 // memory (256 hash buckets).
 constexpr uint32_t kWarpBuckets = 2 * kWarpCap;
 constexpr size_t kWarpStageBytes = (StageMem::bytes(kWarpCap, kWarpBuckets) + 15) & ~size_t(15);
+
+// One warp-class list, staged in the warp's shared-memory slice `m`.
+template <class Sink, bool kTime>
+__device__ __forceinline__ void warp_vertex(const Csr& g, uint32_t u, uint32_t lane,
+                                            const StageMem& m, const uint8_t (*table)[16],
+                                            unsigned long long* __restrict__ ctr, const Sink& sink,
+                                            const ArcTimes& at, TypeCounts& tc) {
+  constexpr bool kVC = Sink::kPerVertex;
+  const uint64_t ub = g.off[u];
+  const uint32_t d = (uint32_t)(g.off[u + 1] - ub);
+  if (d > kWarpCap) {  // uniform over the warp
+    if (lane == 0) atomicExch(ctr + C_ERROR, kErrStageCapacity);
+    return;
+  }
+  const Geo geo = Geo::of(d, kWarpBuckets);
+  stage<32>(g, ub, d, lane, m, geo, table, WarpSync{});
+  TypeCounts vc;
+  TypeCounts& out = kVC ? vc : tc;
+  PackedCounts pc;
+  if (kTime) {
+    timed_pass(g, m, d, 0, 1, lane, geo, pc, out, at, kTableWarp);
+  } else {
+    warp_chunk_scan(m, d, lane);
+    stream_pass<kStreamUnroll>(g, m, d, 0, 1, lane, geo, pc, out);
+    search_pass(g, m, d, 0, 1, lane, pc, out);
+  }
+  pc.drain(out);
+  if (kVC) warp_vertex_flush(vc, u, lane, sink);
+  __syncwarp();
+}
 
 template <class Sink, bool kTime>
 __global__ void __launch_bounds__(256) k_warp(Csr g, const uint32_t* __restrict__ list, uint32_t cnt,
@@ -719,30 +761,8 @@ __global__ void __launch_bounds__(256) k_warp(Csr g, const uint32_t* __restrict_
   const StageMem m = StageMem::carve(smem + w * kWarpStageBytes, kWarpCap, kWarpBuckets);
   TypeCounts tc;
   const uint32_t warps = gridDim.x * kWarps;
-  for (uint32_t idx = blockIdx.x * kWarps + w; idx < cnt; idx += warps) {
-    const uint32_t u = list[idx];
-    const uint64_t ub = g.off[u];
-    const uint32_t d = (uint32_t)(g.off[u + 1] - ub);
-    if (d > kWarpCap) {  // uniform over the warp
-      if (lane == 0) atomicExch(ctr + C_ERROR, kErrStageCapacity);
-      continue;
-    }
-    const Geo geo = Geo::of(d, kWarpBuckets);
-    stage<32>(g, ub, d, lane, m, geo, table, WarpSync{});
-    TypeCounts vc;
-    TypeCounts& out = kVC ? vc : tc;
-    PackedCounts pc;
-    if (kTime) {
-      timed_pass(g, m, d, 0, 1, lane, geo, pc, out, at, kTableWarp);
-    } else {
-      warp_chunk_scan(m, d, lane);
-      stream_pass<kStreamUnroll>(g, m, d, 0, 1, lane, geo, pc, out);
-      search_pass(g, m, d, 0, 1, lane, pc, out);
-    }
-    pc.drain(out);
-    if (kVC) warp_vertex_flush(vc, u, lane, sink);
-    __syncwarp();
-  }
+  for (uint32_t idx = blockIdx.x * kWarps + w; idx < cnt; idx += warps)
+    warp_vertex<Sink, kTime>(g, list[idx], lane, m, table, ctr, sink, at, tc);
   if (!kVC) flush_counts<256>(tc, ctr);
 }
 
@@ -751,22 +771,58 @@ __global__ void __launch_bounds__(256) k_warp(Csr g, const uint32_t* __restrict_
 // (nb >= 2 * cap, powers of two).
 inline size_t block_stage_bytes(uint32_t cap, uint32_t nb) { return StageMem::bytes(cap, nb); }
 
+// One block-class list (the whole CTA), staged in `m` of capacity `cap`
+// with `nb` hash buckets.
+template <int THREADS, class Sink, bool kTime>
+__device__ __forceinline__ void block_vertex(const Csr& g, uint32_t u, uint32_t cap, uint32_t nb,
+                                             const StageMem& m, const uint8_t (*table)[16],
+                                             uint32_t* scan_tmp, unsigned long long* __restrict__ ctr,
+                                             const Sink& sink, const ArcTimes& at, uint32_t tclass,
+                                             TypeCounts& tc) {
+  constexpr bool kVC = Sink::kPerVertex;
+  constexpr uint32_t kWarps = THREADS / 32;
+  const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
+  const uint64_t ub = g.off[u];
+  const uint32_t d = (uint32_t)(g.off[u + 1] - ub);
+  if (d > cap) {  // uniform over the CTA
+    if (threadIdx.x == 0) atomicExch(ctr + C_ERROR, kErrStageCapacity);
+    return;
+  }
+  const Geo geo = Geo::of(d, nb);
+  stage<THREADS>(g, ub, d, threadIdx.x, m, geo, table, BlockSync{});
+  TypeCounts vc;
+  TypeCounts& out = kVC ? vc : tc;
+  PackedCounts pc;
+  if (kTime) {
+    timed_pass(g, m, d, w, kWarps, lane, geo, pc, out, at, tclass);
+  } else {
+    block_chunk_scan<THREADS>(m, d, scan_tmp);
+    stream_pass<kStreamUnroll>(g, m, d, w, kWarps, lane, geo, pc, out);
+    search_pass(g, m, d, w, kWarps, lane, pc, out);
+  }
+  pc.drain(out);
+  if (kVC) block_vertex_flush<THREADS>(vc, u, sink);
+}
+
 template <int THREADS, class Sink, bool kTime>
 __global__ void __launch_bounds__(THREADS) k_block(Csr g, const uint32_t* __restrict__ list,
                                                    uint32_t cnt, uint32_t cap, uint32_t nb,
                                                    unsigned long long* __restrict__ queue,
                                                    unsigned long long* __restrict__ ctr, Sink sink,
                                                    const uint8_t* __restrict__ gtable, ArcTimes at,
-                                                   uint32_t tclass) {
+                                                   uint32_t tclass, const uint32_t* __restrict__ plan,
+                                                   uint32_t pclass) {
   constexpr bool kVC = Sink::kPerVertex;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ uint8_t table[16][16];
   __shared__ uint32_t scan_tmp[THREADS / 32 + 1];
   __shared__ uint32_t s_item;
   for (int i = threadIdx.x; i < 256; i += THREADS) (&table[0][0])[i] = gtable[i];
+  if (plan) {  // list and count planned on the device
+    list += plan[pclass];
+    cnt = plan[kPlanCounts + pclass];
+  }
   const StageMem m = StageMem::carve(smem, cap, nb);
-  constexpr uint32_t kWarps = THREADS / 32;
-  const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
   TypeCounts tc;
   while (true) {
     __syncthreads();
@@ -774,27 +830,8 @@ __global__ void __launch_bounds__(THREADS) k_block(Csr g, const uint32_t* __rest
     __syncthreads();
     const uint32_t item = s_item;
     if (item >= cnt) break;
-    const uint32_t u = list[item];
-    const uint64_t ub = g.off[u];
-    const uint32_t d = (uint32_t)(g.off[u + 1] - ub);
-    if (d > cap) {  // uniform over the CTA
-      if (threadIdx.x == 0) atomicExch(ctr + C_ERROR, kErrStageCapacity);
-      continue;
-    }
-    const Geo geo = Geo::of(d, nb);
-    stage<THREADS>(g, ub, d, threadIdx.x, m, geo, table, BlockSync{});
-    TypeCounts vc;
-    TypeCounts& out = kVC ? vc : tc;
-    PackedCounts pc;
-    if (kTime) {
-      timed_pass(g, m, d, w, kWarps, lane, geo, pc, out, at, tclass);
-    } else {
-      block_chunk_scan<THREADS>(m, d, scan_tmp);
-      stream_pass<kStreamUnroll>(g, m, d, w, kWarps, lane, geo, pc, out);
-      search_pass(g, m, d, w, kWarps, lane, pc, out);
-    }
-    pc.drain(out);
-    if (kVC) block_vertex_flush<THREADS>(vc, u, sink);
+    block_vertex<THREADS, Sink, kTime>(g, list[item], cap, nb, m, table, scan_tmp, ctr, sink, at,
+                                       tclass, tc);
   }
   if (!kVC) flush_counts<THREADS>(tc, ctr);
 }
@@ -805,11 +842,16 @@ template <int THREADS, class Sink, bool kTime>
 __global__ void __launch_bounds__(THREADS) k_giant(Csr g, const uint32_t* __restrict__ list,
                                                    uint32_t cnt, unsigned long long* __restrict__ queue,
                                                    unsigned long long* __restrict__ ctr, Sink sink,
-                                                   const uint8_t* __restrict__ gtable, ArcTimes at) {
+                                                   const uint8_t* __restrict__ gtable, ArcTimes at,
+                                                   const uint32_t* __restrict__ plan, uint32_t pclass) {
   constexpr bool kVC = Sink::kPerVertex;
   __shared__ uint8_t table[16][16];
   __shared__ uint32_t s_item;
   for (int i = threadIdx.x; i < 256; i += THREADS) (&table[0][0])[i] = gtable[i];
+  if (plan) {  // list and count planned on the device
+    list += plan[pclass];
+    cnt = plan[kPlanCounts + pclass];
+  }
   constexpr uint32_t kWarps = THREADS / 32;
   const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
   TypeCounts tc;
@@ -880,7 +922,7 @@ void launch_classes(cudaStream_t st, const Csr& csr, const uint32_t* lists, cons
     k_block<256, Sink, kTime><<<grid, 256, smem, st>>>(csr, lists + starts[2], counts[2], cap, nb,
                                                         ctr + C_WORK + 0, ctr, sink,
                                                         d_tables + 256 * kTableBlock, at,
-                                                        kTableBlock);
+                                                        kTableBlock, nullptr, 0);
     launches++;
   }
   if (counts[3]) {
@@ -895,16 +937,166 @@ void launch_classes(cudaStream_t st, const Csr& csr, const uint32_t* lists, cons
     k_block<512, Sink, kTime><<<grid, 512, smem, st>>>(csr, lists + starts[3], counts[3], cap, nb,
                                                         ctr + C_WORK + 1, ctr, sink,
                                                         d_tables + 256 * kTableLarge, at,
-                                                        kTableLarge);
+                                                        kTableLarge, nullptr, 0);
     launches++;
   }
   if (counts[4]) {
     const uint32_t grid = std::min<uint32_t>(counts[4], kSMs * 2);
     k_giant<512, Sink, kTime><<<grid, 512, 0, st>>>(csr, lists + starts[4], counts[4],
                                                      ctr + C_WORK + 2, ctr, sink,
-                                                     d_tables + 256 * kTableGiant, at);
+                                                     d_tables + 256 * kTableGiant, at, nullptr, 0);
     launches++;
   }
+}
+
+// ------------------------------------------------------- persistent ----
+// The persistent engine: the whole count as one sequence without host
+// synchronisation, so that it can be captured once in a CUDA graph and
+// replayed.  The class lists are planned on the device (k_plan); one
+// persistent kernel of 256-thread CTAs then drains two device work queues:
+// first the block-class lists, one per CTA at a time; then, with no further
+// CTA barriers, each warp takes a warp-class list or 32 tiny lists (one per
+// lane) at a time.  Large and giant lists, rare in the small graphs a batch
+// holds, keep their own kernels, which read their counts from the plan.
+__global__ void k_plan(unsigned long long* __restrict__ ctr, uint32_t* __restrict__ plan) {
+  if (threadIdx.x != 0) return;
+  uint32_t start = 0;
+  for (int c = 0; c < kClasses; c++) {
+    const uint32_t cnt = (uint32_t)ctr[C_WORK + c];
+    plan[c] = start;
+    plan[kPlanCounts + c] = cnt;
+    start += cnt;
+  }
+  plan[kClasses] = start;
+  for (int i = 0; i < 8; i++) ctr[C_WORK + i] = 0;  // fill cursors and work queues
+  ctr[C_QUEUE_WARP] = 0;
+}
+
+constexpr size_t kPersistentSmem =
+    StageMem::bytes(kBlockCap, 4 * kBlockCap) > 8 * kWarpStageBytes
+        ? StageMem::bytes(kBlockCap, 4 * kBlockCap)
+        : 8 * kWarpStageBytes;
+
+template <class Sink>
+__global__ void __launch_bounds__(256, 4) k_persistent(Csr g, const uint32_t* __restrict__ lists,
+                                                       const uint32_t* __restrict__ plan,
+                                                       unsigned long long* __restrict__ ctr, Sink sink,
+                                                       const uint8_t* __restrict__ gtables) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ uint8_t tw[16][16], tb[16][16];
+  __shared__ uint32_t scan_tmp[256 / 32 + 1];
+  __shared__ uint32_t s_item;
+  (&tw[0][0])[threadIdx.x] = gtables[256 * kTableWarp + threadIdx.x];
+  (&tb[0][0])[threadIdx.x] = gtables[256 * kTableBlock + threadIdx.x];
+  const uint32_t nt = plan[kPlanCounts + 0], nw = plan[kPlanCounts + 1], nb = plan[kPlanCounts + 2];
+  const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
+  TypeCounts tc;
+  // Phase 1: block-class lists, the whole CTA on each.
+  const StageMem mb = StageMem::carve(smem, kBlockCap, 4 * kBlockCap);
+  while (true) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_item = (uint32_t)atomicAdd(ctr + C_WORK + 5, 1ull);
+    __syncthreads();
+    const uint32_t item = s_item;
+    if (item >= nb) break;
+    block_vertex<256, Sink, false>(g, lists[plan[2] + item], kBlockCap, 4 * kBlockCap, mb, tb,
+                                   scan_tmp, ctr, sink, ArcTimes{nullptr, nullptr}, kTableBlock, tc);
+  }
+  // Phase 2: warp-granular items.  Every warp of the CTA has left phase 1
+  // (the exit above is uniform), so the slices no longer alias mb in use.
+  const StageMem mw = StageMem::carve(smem + w * kWarpStageBytes, kWarpCap, kWarpBuckets);
+  const uint32_t total = nw + (nt + 31) / 32;
+  while (true) {
+    uint32_t item = 0;
+    if (lane == 0) item = (uint32_t)atomicAdd(ctr + C_QUEUE_WARP, 1ull);
+    item = __shfl_sync(kFull, item, 0);
+    if (item >= total) break;
+    if (item < nw) {
+      warp_vertex<Sink, false>(g, lists[plan[1] + item], lane, mw, tw, ctr, sink,
+                               ArcTimes{nullptr, nullptr}, tc);
+    } else {
+      const uint32_t idx = (item - nw) * 32 + lane;
+      if (idx < nt) tiny_vertex<kTinyMax>(g, lists[plan[0] + idx], sink, tc);
+    }
+  }
+  if (!Sink::kPerVertex) flush_counts<256>(tc, ctr);
+}
+
+// Enqueues the persistent sequence on `st` (no host synchronisation).
+template <class Sink>
+void enqueue_persistent(cudaStream_t st, const Csr& csr, const ClassBounds& cb, uint32_t* lists,
+                        uint32_t* plan, unsigned long long* ctr, const uint8_t* d_tables,
+                        const Sink& sink) {
+  const ArcTimes none{nullptr, nullptr};
+  STC_CUDA(cudaMemsetAsync(ctr + C_WORK, 0, 8 * sizeof(uint64_t), st));
+  k_classify_count<<<kSMs * 4, 256, 0, st>>>(csr.off, csr.n, cb, ctr, nullptr);
+  k_plan<<<1, 32, 0, st>>>(ctr, plan);
+  k_classify_fill<<<kSMs * 4, 256, 0, st>>>(csr.off, csr.n, cb, lists, plan, ctr + C_WORK, nullptr);
+  k_persistent<Sink><<<kSMs * 4, 256, kPersistentSmem, st>>>(csr, lists, plan, ctr, sink,
+                                                             d_tables);
+  k_block<512, Sink, false><<<kSMs, 512, StageMem::bytes(kLargeCap, 2 * kLargeCap), st>>>(
+      csr, lists, 0, kLargeCap, 2 * kLargeCap, ctr + C_WORK + 6, ctr, sink,
+      d_tables + 256 * kTableLarge, none, kTableLarge, plan, 3);
+  k_giant<512, Sink, false><<<kSMs * 2, 512, 0, st>>>(csr, lists, 0, ctr + C_WORK + 7, ctr, sink,
+                                                      d_tables + 256 * kTableGiant, none, plan, 4);
+  STC_CUDA(cudaGetLastError());
+}
+
+// Identity of a captured persistent sequence: every pointer and size its
+// kernels were given.
+struct PersistentKey {
+  const void* p[9];
+  uint64_t v[4];
+  bool operator==(const PersistentKey& o) const { return memcmp(this, &o, sizeof(*this)) == 0; }
+};
+
+template <class Sink>
+void count_persistent(stc_ctx* c, const Csr& csr, const ClassBounds& cb, uint32_t* lists,
+                      uint32_t* plan, unsigned long long* ctr, const uint8_t* d_tables,
+                      const Sink& sink, const void* s0, const void* s1, uint64_t s2) {
+  cudaStream_t st = c->stream;
+  STC_CUDA(cudaFuncSetAttribute(k_persistent<Sink>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kPersistentSmem));
+  STC_CUDA(cudaFuncSetAttribute(k_block<512, Sink, false>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)StageMem::bytes(kLargeCap, 2 * kLargeCap)));
+  c->launches += 6;
+  // The legacy default stream cannot be captured: launch directly there.
+  if (st == nullptr || st == cudaStreamLegacy || st == cudaStreamPerThread) {
+    enqueue_persistent(st, csr, cb, lists, plan, ctr, d_tables, sink);
+    return;
+  }
+  PersistentKey key{};
+  const void* ptrs[9] = {csr.off, csr.nbr, csr.sgn, csr.verts, lists, plan, ctr, d_tables, s0};
+  memcpy(key.p, ptrs, sizeof(ptrs));
+  key.v[0] = csr.n;
+  key.v[1] = cb.tiny_max;
+  key.v[2] = s2;
+  key.v[3] = reinterpret_cast<uint64_t>(s1);
+  static_assert(sizeof(PersistentKey) <= sizeof(c->graph_key), "graph key size");
+  if (c->graph_exec && memcmp(c->graph_key, &key, sizeof(key)) == 0) {
+    STC_CUDA(cudaGraphLaunch(c->graph_exec, st));
+    return;
+  }
+  if (c->graph_exec) {
+    STC_CUDA(cudaGraphExecDestroy(c->graph_exec));
+    c->graph_exec = nullptr;
+  }
+  cudaGraph_t graph = nullptr;
+  STC_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  try {
+    enqueue_persistent(st, csr, cb, lists, plan, ctr, d_tables, sink);
+  } catch (...) {
+    cudaStreamEndCapture(st, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    throw;
+  }
+  STC_CUDA(cudaStreamEndCapture(st, &graph));
+  const cudaError_t e = cudaGraphInstantiate(&c->graph_exec, graph, 0);
+  cudaGraphDestroy(graph);
+  STC_CUDA(e);
+  memcpy(c->graph_key, &key, sizeof(key));
+  STC_CUDA(cudaGraphLaunch(c->graph_exec, st));
 }
 
 // ------------------------------------------------------------ shards ----
@@ -1022,6 +1214,22 @@ void count_triangles(stc_ctx* c, const DeviceGraph& g, const CountConfig& cfg) {
   const bool tiny =
       !timed && (cfg.strategy == STC_STRATEGY_AUTO || cfg.strategy == STC_STRATEGY_SEARCH);
   const ClassBounds cb{tiny ? kTinyMax : 1u, kWarpCap, kBlockCap, kLargeCap};
+
+  if (cfg.persistent && !timed && cfg.shards <= 1) {
+    uint32_t* lists = buffer<uint32_t>(c, B_WORK, (size_t)g.n + kPlanWords + 8);
+    uint32_t* plan = lists + g.n + 4;
+    if (cfg.vertex_counts) {
+      const VertexSink sink{(unsigned long long*)cfg.vertex_counts, g.verts};
+      count_persistent(c, csr, cb, lists, plan, ctr, d_table, sink, sink.vcounts, nullptr, 1);
+    } else if (cfg.graph_counts) {
+      const GraphSink sink{(unsigned long long*)cfg.graph_counts, g.gbase, g.G};
+      count_persistent(c, csr, cb, lists, plan, ctr, d_table, sink, sink.gcounts, sink.gbase,
+                       2 + ((uint64_t)g.G << 8));
+    } else {
+      count_persistent(c, csr, cb, lists, plan, ctr, d_table, TotalSink{}, nullptr, nullptr, 0);
+    }
+    return;
+  }
   k_classify_count<<<kSMs * 4, 256, 0, st>>>(g.off, g.n, cb, ctr, range);
   STC_CUDA(cudaMemcpyAsync(c->h_pinned + C_WORK, counters(c) + C_WORK,
                            (C_MAX_FDEG + 1 - C_WORK) * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));

@@ -61,6 +61,7 @@ enum CounterSlot {
   C_MAX_FDEG = 17,             // largest out-degree of the forward CSR
   C_SHARD_LO = 18,             // rank range [lo, hi) of a sharded count
   C_SHARD_HI = 19,
+  C_QUEUE_WARP = 20,           // warp-granular work queue of the persistent engine
   C_SLOTS = 32
 };
 
@@ -102,6 +103,10 @@ struct stc_ctx {
   int launches = 0;
   bool fixed_ready = false;   // B_DISPATCH_FIXED holds the fixed tables
   bool model_loaded = false;  // B_DISPATCH holds the tables of a loaded model
+  // The persistent count captured in a CUDA graph, and the pointers and
+  // sizes it was captured with (replayed while they stay the same).
+  cudaGraphExec_t graph_exec = nullptr;
+  uint64_t graph_key[16] = {};
 };
 
 namespace stc {
@@ -189,6 +194,8 @@ struct CountConfig {
   // C_SHARD_LO / C_SHARD_HI.
   uint32_t shard = 0;
   uint32_t shards = 1;
+  // Persistent engine captured in a CUDA graph (STC_F_PERSISTENT).
+  bool persistent = false;
 };
 void count_triangles(stc_ctx* c, const DeviceGraph& g, const CountConfig& cfg);
 
