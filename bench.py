@@ -227,6 +227,51 @@ def run_reference(args) -> None:
     print(json.dumps(out))
 
 
+def compare_forms(ctx, args, src, dst, sign, offs, stream, torch, edges) -> dict:
+    """The metric's comparison on resident inputs, one process, one GPU:
+    the plain fixed form (one graph per call, per-class kernels, fixed
+    dispatch) against the learned + batched form (the whole batch in one
+    call on the persistent engine, learned dispatch; for a single graph,
+    learned dispatch alone).  Each form: one warm-up pass, then `steps`
+    timed passes with CUDA events."""
+    ctx.load_dispatch_model()
+    spans = ([(int(offs[g]), int(offs[g + 1])) for g in range(len(offs) - 1)]
+             if offs is not None else [(0, int(src.numel()))])
+    kw = dict(stream=stream.cuda_stream)
+
+    def plain():
+        for b, e in spans:
+            if e > b:
+                ctx.count(src[b:e], dst[b:e], sign[b:e], dispatch="fixed", persistent=False, **kw)
+
+    def learned():
+        if offs is not None:
+            ctx.count_batch_packed(src, dst, sign, offs, dispatch="learned", persistent=True, **kw)
+        else:
+            ctx.count(src, dst, sign, dispatch="learned", persistent=False, **kw)
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / args.steps
+
+    ms_plain, ms_learned = timed(plain), timed(learned)
+    ctx.set_dispatch_model(None)
+    return {"plain_fixed": {"edges_per_s": edges / (ms_plain / 1e3), "ms": ms_plain,
+                            "form": "one graph per call, per-class kernels, fixed dispatch"},
+            "learned_batched": {"edges_per_s": edges / (ms_learned / 1e3), "ms": ms_learned,
+                                "form": ("whole batch in one call, persistent engine (CUDA graph), "
+                                         "learned dispatch") if offs is not None else
+                                        "learned dispatch, per-class kernels"},
+            "ratio": ms_plain / ms_learned}
+
+
 def run_gpu(args) -> None:
     import ctypes as C
 
@@ -243,6 +288,10 @@ def run_gpu(args) -> None:
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
     ctx = stc.Context(local)
     model = ctx.load_dispatch_model() if args.dispatch == "learned" else None
+    from signed_triangle_counting_b200 import autotune
+    tuning = None if args.no_tuning else autotune.tuning_for(args.workload)
+    if tuning:
+        ctx.set_tuning(tuning)
     stream = torch.cuda.current_stream(local)
     # Every rank generates the same workload; with N > 1 ranks a single graph
     # is split into N shards of equal merge-model cost, a batch into N sets of
@@ -369,6 +418,8 @@ def run_gpu(args) -> None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
     e2e_value = edges * e2e_steps / (e2e_ms / 1e3)
+    forms = (compare_forms(ctx, args, src, dst, sign, offs_run, stream, torch, edges)
+             if args.compare_forms and world == 1 else None)
 
     if rank == 0:
         peaks = load_peaks()
@@ -401,6 +452,7 @@ def run_gpu(args) -> None:
                        "strategy": args.strategy, "dispatch": args.dispatch,
                        "dispatch_model": model.get("trained_on") if model else None,
                        "engine": "persistent (CUDA graph)" if persistent else "class kernels",
+                       "tuning": tuning,
                        "l2": f"inputs {m_input * 9 / 1e9:.1f} GB per rank > 126 MB L2, no flush",
                        "parallelism": par},
             "exact": exact, "counts": counts_out,
@@ -418,6 +470,8 @@ def run_gpu(args) -> None:
             "gpu_launches": launches,
             "clocks": clocks,
         }
+        if forms:
+            res["forms"] = forms
         print(json.dumps(res))
     ctx.close()
     if world > 1:
@@ -434,6 +488,10 @@ def main() -> None:
     ap.add_argument("--strategy", default="auto", choices=["auto", "merge", "hash", "search"])
     ap.add_argument("--dispatch", default="fixed", choices=["fixed", "learned"])
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--no-tuning", action="store_true",
+                    help="untuned launch parameters instead of the workload's autotuned ones")
+    ap.add_argument("--compare-forms", action="store_true",
+                    help="also time the plain fixed form against the learned + batched form")
     ap.add_argument("--engine", default="auto", choices=["auto", "persistent", "classes"],
                     help="counting engine (auto: persistent for the batch, class kernels else)")
     ap.add_argument("--rmat-scale", type=int, default=24,

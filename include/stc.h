@@ -306,6 +306,35 @@ stc_status stc_ctx_set_dispatch_model(stc_ctx* ctx, const float* params);
  * strategy AUTO and this dispatch would use on this context. */
 stc_status stc_dispatch_tables(stc_ctx* ctx, uint32_t dispatch, uint8_t* out);
 
+/* ------------------------------------------------------------ autotuner ---- */
+/* No counterpart in the reference.  Launch parameters of the three staged
+ * list classes (index 0 = warp class, |N+(u)| <= 128; 1 = block, <= 1024;
+ * 2 = large, <= 4096), used by the per-class kernels (not by the persistent
+ * engine, which keeps the defaults). */
+typedef struct stc_tuning {
+  uint32_t block_threads;  /* CTA threads of the block class: 128, 256 (default) or 512 */
+  uint32_t hash_factor[3]; /* hash buckets (of two keys) per staged element: 2, 4 or 8;
+                              defaults 4, 4, 2; lowered where the table would not fit
+                              a CTA's shared memory */
+  uint32_t unroll[3];      /* int4 chunks of B in flight per lane in the stream pass
+                              (the merge tile width): 1, 2 (default) or 4 */
+} stc_tuning;
+
+/* Sets the context's tuning (NULL restores the defaults); values outside the
+ * lists above return STC_ERR_INVALID_ARGUMENT. */
+stc_status stc_ctx_set_tuning(stc_ctx* ctx, const stc_tuning* tuning);
+stc_status stc_ctx_get_tuning(const stc_ctx* ctx, stc_tuning* out);
+
+/* Autotuner: builds the graph of (src, dst, sign) once, then, class by class
+ * (warp, block, large), counts that class alone under every candidate
+ * setting (hash factor x unroll, and for the block class x block threads),
+ * `reps` times each, timed with CUDA events, and keeps the fastest.  Every
+ * candidate must give the same counts (else STC_ERR_INTERNAL).  The result
+ * is set on the context and copied to `out`. */
+stc_status stc_autotune(stc_ctx* ctx, const uint32_t* src, const uint32_t* dst,
+                        const int8_t* sign, uint64_t m, const stc_opts* opts, uint32_t reps,
+                        stc_tuning* out);
+
 /* --------------------------------------------------- device generator ---- */
 /* Writes the RMAT samples of stc_synth_rmat (include/stc_synth.h) for the
  * same arguments directly into device arrays of `samples` elements. */

@@ -418,6 +418,37 @@ class Context:
                                          t.ctypes.data_as(_capi.u8p)), self._h)
         return t.reshape(4, 16, 16)
 
+    # ------------------------------------------------------------- tuning
+    def set_tuning(self, tuning: Optional[dict]) -> None:
+        """Sets the staged classes' launch parameters (a dict with
+        block_threads, hash_factor[3], unroll[3]); None restores the defaults."""
+        if tuning is None:
+            _check(lib().stc_ctx_set_tuning(self._h, None), self._h)
+            return
+        t = _capi.stc_tuning()
+        t.block_threads = int(tuning["block_threads"])
+        for i in range(3):
+            t.hash_factor[i] = int(tuning["hash_factor"][i])
+            t.unroll[i] = int(tuning["unroll"][i])
+        _check(lib().stc_ctx_set_tuning(self._h, C.byref(t)), self._h)
+
+    def get_tuning(self) -> dict:
+        t = _capi.stc_tuning()
+        _check(lib().stc_ctx_get_tuning(self._h, C.byref(t)), self._h)
+        return {"block_threads": t.block_threads, "hash_factor": list(t.hash_factor),
+                "unroll": list(t.unroll)}
+
+    def autotune(self, src, dst, sign, *, reps=3, strategy="auto", dispatch="fixed") -> dict:
+        """Runs the autotuner on one graph (host arrays); the result is set on
+        the context and returned."""
+        src, dst, sign = _host_arrays(src, dst, sign)
+        t = _capi.stc_tuning()
+        o = self._opts(strategy, dispatch, timing=False)
+        _check(lib().stc_autotune(self._h, _ptr(src), _ptr(dst), _ptr(sign), len(src), C.byref(o),
+                                  reps, C.byref(t)), self._h)
+        return {"block_threads": t.block_threads, "hash_factor": list(t.hash_factor),
+                "unroll": list(t.unroll)}
+
     def last_stats(self) -> Stats:
         s = _capi.stc_stats()
         _check(lib().stc_ctx_last_stats(self._h, C.byref(s)))

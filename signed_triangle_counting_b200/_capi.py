@@ -50,6 +50,11 @@ class stc_stats(C.Structure):
                 ("kernel_launches", C.c_uint32), ("reserved", C.c_uint32)]
 
 
+class stc_tuning(C.Structure):
+    _fields_ = [("block_threads", C.c_uint32), ("hash_factor", C.c_uint32 * 3),
+                ("unroll", C.c_uint32 * 3)]
+
+
 class stc_synth_graph(C.Structure):
     _fields_ = [("n", C.c_uint64), ("m", C.c_uint64), ("src", u32p), ("dst", u32p), ("sign", i8p)]
 
@@ -119,6 +124,10 @@ SIGNATURES = [
                                        C.c_float, C.c_float, C.c_uint64, f32p, f32p]),
     ("stc_ctx_set_dispatch_model", C.c_int, [C.c_void_p, f32p]),
     ("stc_dispatch_tables", C.c_int, [C.c_void_p, C.c_uint32, u8p]),
+    ("stc_ctx_set_tuning", C.c_int, [C.c_void_p, C.POINTER(stc_tuning)]),
+    ("stc_ctx_get_tuning", C.c_int, [C.c_void_p, C.POINTER(stc_tuning)]),
+    ("stc_autotune", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64,
+                               C.POINTER(stc_opts), C.c_uint32, C.POINTER(stc_tuning)]),
     ("stc_synth_rmat_device", C.c_int, [C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint64,
                                         C.c_uint64, C.c_double, C.c_double, C.c_double,
                                         C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]),

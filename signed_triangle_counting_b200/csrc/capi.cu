@@ -4,6 +4,7 @@
 
 #include <cstdlib>
 #include <cstring>
+#include <initializer_list>
 #include <new>
 #include <string>
 #include <vector>
@@ -554,6 +555,138 @@ stc_status stc_dispatch_tables(stc_ctx* c, uint32_t dispatch, uint8_t* out) {
     cfg.dispatch = dispatch;
     const uint8_t* t = dispatch_tables(c, cfg);
     STC_CUDA(cudaMemcpyAsync(out, t, kTableBytes, cudaMemcpyDeviceToHost, c->stream));
+    STC_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
+namespace {
+
+bool valid_tuning(const stc_tuning& t) {
+  auto in = [](uint32_t v, std::initializer_list<uint32_t> ok) {
+    for (uint32_t x : ok)
+      if (v == x) return true;
+    return false;
+  };
+  if (!in(t.block_threads, {128, 256, 512})) return false;
+  for (int i = 0; i < 3; i++)
+    if (!in(t.hash_factor[i], {2, 4, 8}) || !in(t.unroll[i], {1, 2, 4})) return false;
+  return true;
+}
+
+stc_tuning to_abi(const Tuning& t) {
+  stc_tuning o;
+  o.block_threads = t.block_threads;
+  for (int i = 0; i < 3; i++) {
+    o.hash_factor[i] = t.hash_factor[i];
+    o.unroll[i] = t.unroll[i];
+  }
+  return o;
+}
+
+Tuning from_abi(const stc_tuning& o) {
+  Tuning t;
+  t.block_threads = o.block_threads;
+  for (int i = 0; i < 3; i++) {
+    t.hash_factor[i] = o.hash_factor[i];
+    t.unroll[i] = o.unroll[i];
+  }
+  return t;
+}
+
+}  // namespace
+
+stc_status stc_ctx_set_tuning(stc_ctx* c, const stc_tuning* t) {
+  if (!c) return STC_ERR_INVALID_ARGUMENT;
+  if (!t) {
+    c->tuning = Tuning{};
+    return STC_OK;
+  }
+  if (!valid_tuning(*t)) return STC_ERR_INVALID_ARGUMENT;
+  c->tuning = from_abi(*t);
+  return STC_OK;
+}
+
+stc_status stc_ctx_get_tuning(const stc_ctx* c, stc_tuning* out) {
+  if (!c || !out) return STC_ERR_INVALID_ARGUMENT;
+  *out = to_abi(c->tuning);
+  return STC_OK;
+}
+
+stc_status stc_autotune(stc_ctx* c, const uint32_t* src, const uint32_t* dst, const int8_t* sign,
+                        uint64_t m, const stc_opts* o, uint32_t reps, stc_tuning* out) {
+  if (!c || !out || reps == 0 || reps > 100) return STC_ERR_INVALID_ARGUMENT;
+  return guarded(c, [&] {
+    CountConfig cfg = count_config(o);
+    cfg.persistent = false;
+    begin_call(c, o);
+    DeviceInput in = stage_input(c, src, dst, sign, m, o);
+    DeviceGraph g;
+    build_graph(c, in.src, in.dst, in.sign, m, g);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    STC_CUDA(cudaEventCreate(&e0));
+    STC_CUDA(cudaEventCreate(&e1));
+    Tuning best = c->tuning;
+    try {
+      // One class at a time; candidates of the other classes do not matter
+      // to its time.  Index into the class mask: warp = 1, block = 2, large = 3.
+      for (int k = 0; k < 3; k++) {
+        std::vector<Tuning> cands;
+        const uint32_t hfs[3] = {2, 4, 8};
+        const uint32_t us[3] = {1, 2, 4};
+        const uint32_t ts[3] = {128, 256, 512};
+        for (uint32_t hf : hfs)
+          for (uint32_t u : us)
+            for (int ti = 0; ti < (k == 1 ? 3 : 1); ti++) {
+              Tuning t = best;
+              t.hash_factor[k] = hf;
+              t.unroll[k] = u;
+              if (k == 1) t.block_threads = ts[ti];
+              cands.push_back(t);
+            }
+        cfg.class_mask = 1u << (k + 1);
+        float best_ms = 0.f;
+        bool first = true;
+        uint64_t want[4] = {0, 0, 0, 0};
+        for (const Tuning& t : cands) {
+          c->tuning = t;
+          float t_min = 0.f;
+          for (uint32_t r = 0; r < reps; r++) {
+            STC_CUDA(cudaMemsetAsync(counters(c), 0, 4 * sizeof(uint64_t), c->stream));
+            STC_CUDA(cudaEventRecord(e0, c->stream));
+            count_triangles(c, g, cfg);
+            STC_CUDA(cudaEventRecord(e1, c->stream));
+            STC_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            STC_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (r == 0 || ms < t_min) t_min = ms;
+          }
+          uint64_t got[C_SLOTS];
+          STC_CUDA(cudaMemcpy(got, counters(c), sizeof(got), cudaMemcpyDeviceToHost));
+          if (got[C_ERROR])
+            fail(STC_ERR_INTERNAL, "device reported error word " + std::to_string(got[C_ERROR]));
+          if (first) {
+            memcpy(want, got, sizeof(want));
+          } else if (memcmp(want, got, sizeof(want)) != 0) {
+            fail(STC_ERR_INTERNAL, "autotuner: a candidate setting changed the counts");
+          }
+          if (first || t_min < best_ms) {
+            best_ms = t_min;
+            best.hash_factor[k] = t.hash_factor[k];
+            best.unroll[k] = t.unroll[k];
+            if (k == 1) best.block_threads = t.block_threads;
+          }
+          first = false;
+        }
+      }
+    } catch (...) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->tuning = best;
+    *out = to_abi(best);
     STC_CUDA(cudaStreamSynchronize(c->stream));
   });
 }

@@ -204,14 +204,14 @@ struct StageMem {
   }
 };
 
-// Hash geometry for a list of length d: next_pow2(4 d) buckets of two keys
-// (load <= 1/8), at most `nb_cap` buckets (load <= 1/4 when capped).
+// Hash geometry for a list of length d: next_pow2(hf d) buckets of two keys
+// (hf = 4: load <= 1/8), at most `nb_cap` buckets.
 struct Geo {
   uint32_t nb, shift;
-  __device__ static Geo of(uint32_t d, uint32_t nb_cap) {
+  __device__ static Geo of(uint32_t d, uint32_t nb_cap, uint32_t hf) {
     Geo g;
     g.nb = 4;
-    while (g.nb < 4 * d && g.nb < nb_cap) g.nb <<= 1;
+    while (g.nb < hf * d && g.nb < nb_cap) g.nb <<= 1;
     g.shift = 32 - (31 - __clz(g.nb));
     return g;
   }
@@ -717,12 +717,13 @@ __global__ void __launch_bounds__(256) k_tiny(Csr g, const uint32_t* __restrict_
 constexpr uint32_t kWarpBuckets = 2 * kWarpCap;
 constexpr size_t kWarpStageBytes = (StageMem::bytes(kWarpCap, kWarpBuckets) + 15) & ~size_t(15);
 
-// One warp-class list, staged in the warp's shared-memory slice `m`.
-template <class Sink, bool kTime>
+// One warp-class list, staged in the warp's shared-memory slice `m` with
+// up to hf hash buckets per element; U int4 chunks in flight per lane.
+template <class Sink, bool kTime, int U>
 __device__ __forceinline__ void warp_vertex(const Csr& g, uint32_t u, uint32_t lane,
                                             const StageMem& m, const uint8_t (*table)[16],
-                                            unsigned long long* __restrict__ ctr, const Sink& sink,
-                                            const ArcTimes& at, TypeCounts& tc) {
+                                            uint32_t hf, unsigned long long* __restrict__ ctr,
+                                            const Sink& sink, const ArcTimes& at, TypeCounts& tc) {
   constexpr bool kVC = Sink::kPerVertex;
   const uint64_t ub = g.off[u];
   const uint32_t d = (uint32_t)(g.off[u + 1] - ub);
@@ -730,7 +731,7 @@ __device__ __forceinline__ void warp_vertex(const Csr& g, uint32_t u, uint32_t l
     if (lane == 0) atomicExch(ctr + C_ERROR, kErrStageCapacity);
     return;
   }
-  const Geo geo = Geo::of(d, kWarpBuckets);
+  const Geo geo = Geo::of(d, kWarpBuckets, hf);
   stage<32>(g, ub, d, lane, m, geo, table, WarpSync{});
   TypeCounts vc;
   TypeCounts& out = kVC ? vc : tc;
@@ -739,7 +740,7 @@ __device__ __forceinline__ void warp_vertex(const Csr& g, uint32_t u, uint32_t l
     timed_pass(g, m, d, 0, 1, lane, geo, pc, out, at, kTableWarp);
   } else {
     warp_chunk_scan(m, d, lane);
-    stream_pass<kStreamUnroll>(g, m, d, 0, 1, lane, geo, pc, out);
+    stream_pass<U>(g, m, d, 0, 1, lane, geo, pc, out);
     search_pass(g, m, d, 0, 1, lane, pc, out);
   }
   pc.drain(out);
@@ -747,10 +748,11 @@ __device__ __forceinline__ void warp_vertex(const Csr& g, uint32_t u, uint32_t l
   __syncwarp();
 }
 
-template <class Sink, bool kTime>
+template <class Sink, bool kTime, int U>
 __global__ void __launch_bounds__(256) k_warp(Csr g, const uint32_t* __restrict__ list, uint32_t cnt,
                                               unsigned long long* __restrict__ ctr, Sink sink,
-                                              const uint8_t* __restrict__ gtable, ArcTimes at) {
+                                              const uint8_t* __restrict__ gtable, ArcTimes at,
+                                              uint32_t hf) {
   constexpr bool kVC = Sink::kPerVertex;
   constexpr int kWarps = 8;
   __shared__ __align__(16) unsigned char smem[kWarps * kWarpStageBytes];
@@ -762,7 +764,7 @@ __global__ void __launch_bounds__(256) k_warp(Csr g, const uint32_t* __restrict_
   TypeCounts tc;
   const uint32_t warps = gridDim.x * kWarps;
   for (uint32_t idx = blockIdx.x * kWarps + w; idx < cnt; idx += warps)
-    warp_vertex<Sink, kTime>(g, list[idx], lane, m, table, ctr, sink, at, tc);
+    warp_vertex<Sink, kTime, U>(g, list[idx], lane, m, table, hf, ctr, sink, at, tc);
   if (!kVC) flush_counts<256>(tc, ctr);
 }
 
@@ -770,12 +772,14 @@ __global__ void __launch_bounds__(256) k_warp(Csr g, const uint32_t* __restrict_
 // dynamic shared memory of capacity `cap` with `nb` hash buckets
 // (nb >= 2 * cap, powers of two).
 inline size_t block_stage_bytes(uint32_t cap, uint32_t nb) { return StageMem::bytes(cap, nb); }
+constexpr size_t kMaxStageSmem = 220 * 1024;  // dynamic shared memory a staged CTA may use
 
 // One block-class list (the whole CTA), staged in `m` of capacity `cap`
 // with `nb` hash buckets.
-template <int THREADS, class Sink, bool kTime>
+template <int THREADS, class Sink, bool kTime, int U>
 __device__ __forceinline__ void block_vertex(const Csr& g, uint32_t u, uint32_t cap, uint32_t nb,
-                                             const StageMem& m, const uint8_t (*table)[16],
+                                             uint32_t hf, const StageMem& m,
+                                             const uint8_t (*table)[16],
                                              uint32_t* scan_tmp, unsigned long long* __restrict__ ctr,
                                              const Sink& sink, const ArcTimes& at, uint32_t tclass,
                                              TypeCounts& tc) {
@@ -788,7 +792,7 @@ __device__ __forceinline__ void block_vertex(const Csr& g, uint32_t u, uint32_t 
     if (threadIdx.x == 0) atomicExch(ctr + C_ERROR, kErrStageCapacity);
     return;
   }
-  const Geo geo = Geo::of(d, nb);
+  const Geo geo = Geo::of(d, nb, hf);
   stage<THREADS>(g, ub, d, threadIdx.x, m, geo, table, BlockSync{});
   TypeCounts vc;
   TypeCounts& out = kVC ? vc : tc;
@@ -797,16 +801,16 @@ __device__ __forceinline__ void block_vertex(const Csr& g, uint32_t u, uint32_t 
     timed_pass(g, m, d, w, kWarps, lane, geo, pc, out, at, tclass);
   } else {
     block_chunk_scan<THREADS>(m, d, scan_tmp);
-    stream_pass<kStreamUnroll>(g, m, d, w, kWarps, lane, geo, pc, out);
+    stream_pass<U>(g, m, d, w, kWarps, lane, geo, pc, out);
     search_pass(g, m, d, w, kWarps, lane, pc, out);
   }
   pc.drain(out);
   if (kVC) block_vertex_flush<THREADS>(vc, u, sink);
 }
 
-template <int THREADS, class Sink, bool kTime>
+template <int THREADS, class Sink, bool kTime, int U>
 __global__ void __launch_bounds__(THREADS) k_block(Csr g, const uint32_t* __restrict__ list,
-                                                   uint32_t cnt, uint32_t cap, uint32_t nb,
+                                                   uint32_t cnt, uint32_t cap, uint32_t nb, uint32_t hf,
                                                    unsigned long long* __restrict__ queue,
                                                    unsigned long long* __restrict__ ctr, Sink sink,
                                                    const uint8_t* __restrict__ gtable, ArcTimes at,
@@ -830,8 +834,8 @@ __global__ void __launch_bounds__(THREADS) k_block(Csr g, const uint32_t* __rest
     __syncthreads();
     const uint32_t item = s_item;
     if (item >= cnt) break;
-    block_vertex<THREADS, Sink, kTime>(g, list[item], cap, nb, m, table, scan_tmp, ctr, sink, at,
-                                       tclass, tc);
+    block_vertex<THREADS, Sink, kTime, U>(g, list[item], cap, nb, hf, m, table, scan_tmp, ctr,
+                                          sink, at, tclass, tc);
   }
   if (!kVC) flush_counts<THREADS>(tc, ctr);
 }
@@ -896,51 +900,96 @@ __global__ void __launch_bounds__(THREADS) k_giant(Csr g, const uint32_t* __rest
   if (!kVC) flush_counts<THREADS>(tc, ctr);
 }
 
+// Compile-time choices of the tuned kernels, selected at run time.
+template <int V> struct Int { static constexpr int value = V; };
+template <class F> void with_unroll(uint32_t u, F&& f) {
+  if (u == 1) f(Int<1>{});
+  else if (u == 4) f(Int<4>{});
+  else f(Int<2>{});
+}
+template <class F> void with_block_threads(uint32_t t, F&& f) {
+  if (t == 128) f(Int<128>{});
+  else if (t == 512) f(Int<512>{});
+  else f(Int<256>{});
+}
+
+// Largest hash factor whose staged image of `cap` entries fits the
+// shared memory of one CTA.
+inline uint32_t fit_hash_factor(uint32_t hf, uint32_t cap) {
+  while (hf > 1 && StageMem::bytes(cap, hf * cap) > kMaxStageSmem) hf >>= 1;
+  return hf;
+}
+
 // Launches the class kernels for one sink kind.  `d_tables` holds one
-// 256-byte table per TableClass.
+// 256-byte table per TableClass; `tu` gives the tuned block size, hash
+// factors and stream widths; classes outside `mask` are skipped.  The timing
+// recorder (kTime) uses the default widths and block size, which its
+// per-arc passes do not depend on.
 template <class Sink, bool kTime>
 void launch_classes(cudaStream_t st, const Csr& csr, const uint32_t* lists, const uint32_t* counts,
                     const uint32_t* starts, uint32_t max_fdeg, unsigned long long* ctr,
-                    const uint8_t* d_tables, const Sink& sink, const ArcTimes& at, int& launches) {
-  if (counts[0]) {
+                    const uint8_t* d_tables, const Sink& sink, const ArcTimes& at,
+                    const Tuning& tu, uint32_t mask, int& launches) {
+  if (counts[0] && (mask & 1u)) {
     const uint32_t grid = std::min<uint32_t>((counts[0] + 255) / 256, kSMs * 8);
     k_tiny<kTinyMax, Sink><<<grid, 256, 0, st>>>(csr, lists + starts[0], counts[0], ctr, sink);
     launches++;
   }
-  if (counts[1]) {
+  if (counts[1] && (mask & 2u)) {
     const uint32_t grid = std::min<uint32_t>((counts[1] + 7) / 8, kSMs * 8);
-    k_warp<Sink, kTime><<<grid, 256, 0, st>>>(csr, lists + starts[1], counts[1], ctr, sink,
-                                               d_tables + 256 * kTableWarp, at);
+    const uint32_t u = kTime ? kStreamUnroll : tu.unroll[0];
+    with_unroll(u, [&](auto U) {
+      if constexpr (!kTime || decltype(U)::value == kStreamUnroll)
+        k_warp<Sink, kTime, decltype(U)::value><<<grid, 256, 0, st>>>(
+            csr, lists + starts[1], counts[1], ctr, sink, d_tables + 256 * kTableWarp, at,
+            tu.hash_factor[0]);
+    });
     launches++;
   }
-  if (counts[2]) {
-    const uint32_t cap = kBlockCap, nb = 4 * kBlockCap;
+  if (counts[2] && (mask & 4u)) {
+    const uint32_t cap = kBlockCap;
+    const uint32_t hf = fit_hash_factor(tu.hash_factor[1], cap);
+    const uint32_t nb = hf * cap;
     const size_t smem = block_stage_bytes(cap, nb);
-    STC_CUDA(cudaFuncSetAttribute(k_block<256, Sink, kTime>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const uint32_t grid = std::min<uint32_t>(counts[2], kSMs * 8);
-    k_block<256, Sink, kTime><<<grid, 256, smem, st>>>(csr, lists + starts[2], counts[2], cap, nb,
-                                                        ctr + C_WORK + 0, ctr, sink,
-                                                        d_tables + 256 * kTableBlock, at,
-                                                        kTableBlock, nullptr, 0);
+    const uint32_t threads = kTime ? 256 : tu.block_threads;
+    const uint32_t u = kTime ? kStreamUnroll : tu.unroll[1];
+    with_block_threads(threads, [&](auto T) {
+      with_unroll(u, [&](auto U) {
+        constexpr int kT = decltype(T)::value, kU = decltype(U)::value;
+        if constexpr (!kTime || (kT == 256 && kU == kStreamUnroll)) {
+          STC_CUDA(cudaFuncSetAttribute(k_block<kT, Sink, kTime, kU>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+          const uint32_t grid = std::min<uint32_t>(counts[2], kSMs * 8);
+          k_block<kT, Sink, kTime, kU><<<grid, kT, smem, st>>>(
+              csr, lists + starts[2], counts[2], cap, nb, hf, ctr + C_WORK + 0, ctr, sink,
+              d_tables + 256 * kTableBlock, at, kTableBlock, nullptr, 0);
+        }
+      });
+    });
     launches++;
   }
-  if (counts[3]) {
+  if (counts[3] && (mask & 8u)) {
     // Capacity: the class's largest list rounded up to a power of two.
     uint32_t cap = kBlockCap;
     while (cap < std::min<uint32_t>(max_fdeg, kLargeCap)) cap <<= 1;
-    const uint32_t nb = 2 * cap;
+    const uint32_t hf = fit_hash_factor(tu.hash_factor[2], cap);
+    const uint32_t nb = hf * cap;
     const size_t smem = block_stage_bytes(cap, nb);
-    STC_CUDA(cudaFuncSetAttribute(k_block<512, Sink, kTime>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const uint32_t grid = std::min<uint32_t>(counts[3], kSMs * 2);
-    k_block<512, Sink, kTime><<<grid, 512, smem, st>>>(csr, lists + starts[3], counts[3], cap, nb,
-                                                        ctr + C_WORK + 1, ctr, sink,
-                                                        d_tables + 256 * kTableLarge, at,
-                                                        kTableLarge, nullptr, 0);
+    const uint32_t u = kTime ? kStreamUnroll : tu.unroll[2];
+    with_unroll(u, [&](auto U) {
+      constexpr int kU = decltype(U)::value;
+      if constexpr (!kTime || kU == kStreamUnroll) {
+        STC_CUDA(cudaFuncSetAttribute(k_block<512, Sink, kTime, kU>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const uint32_t grid = std::min<uint32_t>(counts[3], kSMs * 2);
+        k_block<512, Sink, kTime, kU><<<grid, 512, smem, st>>>(
+            csr, lists + starts[3], counts[3], cap, nb, hf, ctr + C_WORK + 1, ctr, sink,
+            d_tables + 256 * kTableLarge, at, kTableLarge, nullptr, 0);
+      }
+    });
     launches++;
   }
-  if (counts[4]) {
+  if (counts[4] && (mask & 16u)) {
     const uint32_t grid = std::min<uint32_t>(counts[4], kSMs * 2);
     k_giant<512, Sink, kTime><<<grid, 512, 0, st>>>(csr, lists + starts[4], counts[4],
                                                      ctr + C_WORK + 2, ctr, sink,
@@ -999,8 +1048,9 @@ __global__ void __launch_bounds__(256, 4) k_persistent(Csr g, const uint32_t* __
     __syncthreads();
     const uint32_t item = s_item;
     if (item >= nb) break;
-    block_vertex<256, Sink, false>(g, lists[plan[2] + item], kBlockCap, 4 * kBlockCap, mb, tb,
-                                   scan_tmp, ctr, sink, ArcTimes{nullptr, nullptr}, kTableBlock, tc);
+    block_vertex<256, Sink, false, kStreamUnroll>(g, lists[plan[2] + item], kBlockCap,
+                                                  4 * kBlockCap, 4, mb, tb, scan_tmp, ctr, sink,
+                                                  ArcTimes{nullptr, nullptr}, kTableBlock, tc);
   }
   // Phase 2: warp-granular items.  Every warp of the CTA has left phase 1
   // (the exit above is uniform), so the slices no longer alias mb in use.
@@ -1012,8 +1062,8 @@ __global__ void __launch_bounds__(256, 4) k_persistent(Csr g, const uint32_t* __
     item = __shfl_sync(kFull, item, 0);
     if (item >= total) break;
     if (item < nw) {
-      warp_vertex<Sink, false>(g, lists[plan[1] + item], lane, mw, tw, ctr, sink,
-                               ArcTimes{nullptr, nullptr}, tc);
+      warp_vertex<Sink, false, kStreamUnroll>(g, lists[plan[1] + item], lane, mw, tw, 4, ctr, sink,
+                                              ArcTimes{nullptr, nullptr}, tc);
     } else {
       const uint32_t idx = (item - nw) * 32 + lane;
       if (idx < nt) tiny_vertex<kTinyMax>(g, lists[plan[0] + idx], sink, tc);
@@ -1034,8 +1084,9 @@ void enqueue_persistent(cudaStream_t st, const Csr& csr, const ClassBounds& cb, 
   k_classify_fill<<<kSMs * 4, 256, 0, st>>>(csr.off, csr.n, cb, lists, plan, ctr + C_WORK, nullptr);
   k_persistent<Sink><<<kSMs * 4, 256, kPersistentSmem, st>>>(csr, lists, plan, ctr, sink,
                                                              d_tables);
-  k_block<512, Sink, false><<<kSMs, 512, StageMem::bytes(kLargeCap, 2 * kLargeCap), st>>>(
-      csr, lists, 0, kLargeCap, 2 * kLargeCap, ctr + C_WORK + 6, ctr, sink,
+  k_block<512, Sink, false, kStreamUnroll><<<kSMs, 512, StageMem::bytes(kLargeCap, 2 * kLargeCap),
+                                            st>>>(
+      csr, lists, 0, kLargeCap, 2 * kLargeCap, 2, ctr + C_WORK + 6, ctr, sink,
       d_tables + 256 * kTableLarge, none, kTableLarge, plan, 3);
   k_giant<512, Sink, false><<<kSMs * 2, 512, 0, st>>>(csr, lists, 0, ctr + C_WORK + 7, ctr, sink,
                                                       d_tables + 256 * kTableGiant, none, plan, 4);
@@ -1057,7 +1108,7 @@ void count_persistent(stc_ctx* c, const Csr& csr, const ClassBounds& cb, uint32_
   cudaStream_t st = c->stream;
   STC_CUDA(cudaFuncSetAttribute(k_persistent<Sink>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)kPersistentSmem));
-  STC_CUDA(cudaFuncSetAttribute(k_block<512, Sink, false>,
+  STC_CUDA(cudaFuncSetAttribute(k_block<512, Sink, false, kStreamUnroll>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)StageMem::bytes(kLargeCap, 2 * kLargeCap)));
   c->launches += 6;
@@ -1252,18 +1303,18 @@ void count_triangles(stc_ctx* c, const DeviceGraph& g, const CountConfig& cfg) {
 
   if (timed) {
     launch_classes<TotalSink, true>(st, csr, lists, counts, starts, max_fdeg, ctr, d_table,
-                                    TotalSink{}, at, c->launches);
+                                    TotalSink{}, at, c->tuning, cfg.class_mask, c->launches);
   } else if (cfg.vertex_counts) {
     const VertexSink sink{(unsigned long long*)cfg.vertex_counts, g.verts};
     launch_classes<VertexSink, false>(st, csr, lists, counts, starts, max_fdeg, ctr, d_table, sink,
-                                      at, c->launches);
+                                      at, c->tuning, cfg.class_mask, c->launches);
   } else if (cfg.graph_counts) {
     const GraphSink sink{(unsigned long long*)cfg.graph_counts, g.gbase, g.G};
     launch_classes<GraphSink, false>(st, csr, lists, counts, starts, max_fdeg, ctr, d_table, sink,
-                                     at, c->launches);
+                                     at, c->tuning, cfg.class_mask, c->launches);
   } else {
     launch_classes<TotalSink, false>(st, csr, lists, counts, starts, max_fdeg, ctr, d_table,
-                                     TotalSink{}, at, c->launches);
+                                     TotalSink{}, at, c->tuning, cfg.class_mask, c->launches);
   }
   STC_CUDA(cudaGetLastError());
 }
@@ -1403,7 +1454,8 @@ extern "C" stc_status stc_count_oriented_csr_noalloc(const uint64_t* d_offsets,
   int launches = 0;
   try {
     launch_classes<TotalSink, false>(st, csr, lists, counts, starts, max_fdeg, ctr, scr->table,
-                                     TotalSink{}, ArcTimes{nullptr, nullptr}, launches);
+                                     TotalSink{}, ArcTimes{nullptr, nullptr}, Tuning{}, 0x1Fu,
+                                     launches);
   } catch (const Error& e) {
     (void)cudaGetLastError();
     return e.status;

@@ -88,6 +88,16 @@ constexpr int kMlpOut = 3;
 constexpr int kMlpParams = kMlpHidden * kMlpIn + kMlpHidden + kMlpOut * kMlpHidden + kMlpOut;
 static_assert(kMlpParams == STC_DISPATCH_MODEL_PARAMS, "parameter count of the ABI");
 
+// Tuned launch parameters of the staged classes (warp, block, large):
+// block-class CTA threads, hash buckets per staged element, and int4 chunks
+// in flight per lane in the stream pass.  The defaults are the untuned
+// engine.
+struct Tuning {
+  uint32_t block_threads = 256;
+  uint32_t hash_factor[3] = {4, 4, 2};
+  uint32_t unroll[3] = {2, 2, 2};
+};
+
 }  // namespace stc
 
 struct stc_ctx {
@@ -107,6 +117,7 @@ struct stc_ctx {
   // sizes it was captured with (replayed while they stay the same).
   cudaGraphExec_t graph_exec = nullptr;
   uint64_t graph_key[16] = {};
+  stc::Tuning tuning;
 };
 
 namespace stc {
@@ -196,6 +207,9 @@ struct CountConfig {
   uint32_t shards = 1;
   // Persistent engine captured in a CUDA graph (STC_F_PERSISTENT).
   bool persistent = false;
+  // Vertex classes to count (bit c: class c = tiny, warp, block, large,
+  // giant); the autotuner times one class at a time.
+  uint32_t class_mask = 0x1F;
 };
 void count_triangles(stc_ctx* c, const DeviceGraph& g, const CountConfig& cfg);
 

@@ -89,3 +89,19 @@ def test_union_shifts_ids_per_graph():
     s, d, g = dispatcher.union(el, [0, 2, 4, 5], [3, 3, 4])
     np.testing.assert_array_equal(s, [0, 1, 3, 5, 6])
     np.testing.assert_array_equal(d, [1, 2, 4, 3, 9])
+
+
+def test_tuning_file_round_trip(tmp_path):
+    from signed_triangle_counting_b200 import autotune
+    entries = {"3": {"tuning": {"block_threads": 512, "hash_factor": [8, 4, 2],
+                                "unroll": [1, 2, 4]}, "tuned_on": "x"}}
+    path = tmp_path / "t.json"
+    autotune.save(path, entries)
+    assert autotune.load(path) == entries
+    assert autotune.tuning_for(3, path) == entries["3"]["tuning"]
+    assert autotune.tuning_for(9, path) is None
+    bad = dict(entries)
+    bad["3"] = {"tuning": {"block_threads": 100, "hash_factor": [8, 4, 2], "unroll": [1, 2, 4]}}
+    autotune.save(path, bad)
+    with pytest.raises(ValueError):
+        autotune.load(path)
