@@ -158,6 +158,21 @@ stc_status stc_load_edge_list(const char* path, stc_edge_list* out);
 stc_status stc_parse_edge_text(const char* data, uint64_t size, stc_edge_list* out);
 void stc_free_edge_list(stc_edge_list* el);
 
+/* MatrixMarket input, for the graphs the reference's GPU drivers read
+ * (GM/tc_split/signed_tc.cu:21-33): a `%%MatrixMarket matrix coordinate`
+ * file, field real, double, integer or pattern, symmetry general or
+ * symmetric, 1-based entries `i j [w]`.  Vertex i - 1 and j - 1 get an
+ * undirected edge, diagonal entries are dropped, and `n` is the matrix
+ * dimension.  Signs: w < 0 is negative by default (the rule of the CPU
+ * programs' text input); with STC_MTX_ZERO_NEGATIVE, w <= 0 is negative,
+ * the GPU drivers' rule (GM/signed_tc.hxx:317); weights are read as float
+ * as there, and pattern entries are positive.  A malformed header, an
+ * index out of range or an entry count that differs from the size line's
+ * returns STC_ERR_INVALID_ARGUMENT.  Free with stc_free_edge_list. */
+#define STC_MTX_ZERO_NEGATIVE 0x1u
+stc_status stc_load_mtx(const char* path, uint32_t flags, stc_edge_list* out);
+stc_status stc_parse_mtx(const char* data, uint64_t size, uint32_t flags, stc_edge_list* out);
+
 /* ---------------------------------------------------------- whole path ---- */
 /* The reference programs' path (MC/tc_serial.cpp:172-210; the Gunrock
  * plug-in GM/signed_tc.hxx:527-542): dedup, (degree, id) orientation, forward

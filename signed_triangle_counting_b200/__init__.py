@@ -21,7 +21,7 @@ from ._capi import lib
 
 __all__ = [
     "GlobalTriCounts", "EdgeList", "ForwardCSR", "Stats", "StcError", "Context",
-    "load_graph", "parse_edge_text", "dispatch_features", "synth",
+    "load_graph", "parse_edge_text", "load_mtx", "parse_mtx", "dispatch_features", "synth",
 ]
 
 
@@ -151,6 +151,32 @@ def load_graph(path: str) -> EdgeList:
 def parse_edge_text(data: bytes) -> EdgeList:
     el = _capi.stc_edge_list()
     _check(lib().stc_parse_edge_text(data, len(data), C.byref(el)))
+    try:
+        return _edge_list_from_c(el)
+    finally:
+        lib().stc_free_edge_list(C.byref(el))
+
+
+def load_mtx(path: str, *, zero_negative: bool = False) -> EdgeList:
+    """A MatrixMarket coordinate file as an edge list (stc_load_mtx): weight
+    < 0 is negative, or <= 0 with ``zero_negative`` (the reference GPU
+    drivers' rule, GM/signed_tc.hxx:317)."""
+    el = _capi.stc_edge_list()
+    st = lib().stc_load_mtx(str(path).encode(), _capi.MTX_ZERO_NEGATIVE if zero_negative else 0,
+                            C.byref(el))
+    if st == _capi.STC_ERR_IO:
+        raise OSError(f"cannot read {path}")
+    _check(st)
+    try:
+        return _edge_list_from_c(el)
+    finally:
+        lib().stc_free_edge_list(C.byref(el))
+
+
+def parse_mtx(data: bytes, *, zero_negative: bool = False) -> EdgeList:
+    el = _capi.stc_edge_list()
+    _check(lib().stc_parse_mtx(data, len(data), _capi.MTX_ZERO_NEGATIVE if zero_negative else 0,
+                               C.byref(el)))
     try:
         return _edge_list_from_c(el)
     finally:

@@ -83,6 +83,7 @@ DISPATCH = {"fixed": 0, "learned": 1}
 F_DEVICE_INPUT = 0x1
 F_TIMING = 0x2
 F_PERSISTENT = 0x8
+MTX_ZERO_NEGATIVE = 0x1
 
 # (name, restype, argtypes) for every exported function of include/*.h.
 SIGNATURES = [
@@ -96,6 +97,8 @@ SIGNATURES = [
     ("stc_load_edge_list", C.c_int, [C.c_char_p, C.POINTER(stc_edge_list)]),
     ("stc_parse_edge_text", C.c_int, [C.c_char_p, C.c_uint64, C.POINTER(stc_edge_list)]),
     ("stc_free_edge_list", None, [C.POINTER(stc_edge_list)]),
+    ("stc_load_mtx", C.c_int, [C.c_char_p, C.c_uint32, C.POINTER(stc_edge_list)]),
+    ("stc_parse_mtx", C.c_int, [C.c_char_p, C.c_uint64, C.c_uint32, C.POINTER(stc_edge_list)]),
     ("stc_count", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64,
                             C.POINTER(stc_opts), C.POINTER(stc_counts)]),
     ("stc_count_shard", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64,

@@ -34,7 +34,7 @@ CXX_FLAGS = ["-O3", "-march=x86-64-v3", "-std=c++17", "-fPIC", "-Wall", "-Wno-un
              f"-I{INCLUDE}", f"-I{CSRC}"]
 
 CUDA_SOURCES = ["capi.cu", "build.cu", "count.cu", "dispatch.cu"]
-HOST_SOURCES = ["text_ingest.cpp", "synth_host.cpp"]
+HOST_SOURCES = ["text_ingest.cpp", "mtx_ingest.cpp", "synth_host.cpp"]
 
 
 def _headers() -> list[Path]:

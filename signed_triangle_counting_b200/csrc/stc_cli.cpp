@@ -3,7 +3,13 @@
 // MC/tc_hash_sign_enu.cpp:76-177).
 //
 //   stc [--strategy auto|merge|hash|search] [--dispatch fixed|learned]
-//       [--device N] [--json] <graph_file>
+//       [--model PATH] [--zero-negative] [--device N] [--json] <graph_file>
+//
+// <graph_file> is `u v sign` text (MC/graph_io.h:72-212) or, when it starts
+// with a `%%MatrixMarket` banner, a coordinate .mtx file as the reference's
+// GPU drivers read (--zero-negative: weight <= 0 is negative, their rule).
+// --dispatch learned loads the model from --model or, by default,
+// dispatch_model.json beside this executable.
 //
 // Prints the union of the reference outputs: tc_serial's stage lines,
 // `n=.. raw_edges=..`, `forward_edges=..` and per-type block, then the
@@ -32,9 +38,52 @@ void stage(const char* label, double seconds) { std::printf("[%s] took %.4f seco
 int usage(const char* prog) {
   std::fprintf(stderr,
                "usage: %s [--strategy auto|merge|hash|search] [--dispatch fixed|learned] "
-               "[--device N] [--json] <graph_file>\n",
+               "[--model PATH] [--zero-negative] [--device N] [--json] <graph_file>\n",
                prog);
   return 1;
+}
+
+bool is_mtx(const char* path) {
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return false;
+  char head[15] = {0};
+  const size_t got = std::fread(head, 1, 14, f);
+  std::fclose(f);
+  return got == 14 && std::strncmp(head, "%%MatrixMarket", 14) == 0;
+}
+
+// The "params" array of a dispatch model file (STC_DISPATCH_MODEL_PARAMS
+// floats); false if the file cannot be read or holds a different count.
+bool read_model(const std::string& path, float* params) {
+  FILE* f = std::fopen(path.c_str(), "rb");
+  if (!f) return false;
+  std::string text;
+  char buf[4096];
+  size_t k;
+  while ((k = std::fread(buf, 1, sizeof(buf), f)) > 0) text.append(buf, k);
+  std::fclose(f);
+  size_t at = text.find("\"params\"");
+  if (at == std::string::npos) return false;
+  at = text.find('[', at);
+  if (at == std::string::npos) return false;
+  const char* p = text.c_str() + at + 1;
+  int n = 0;
+  while (n < STC_DISPATCH_MODEL_PARAMS) {
+    char* stop = nullptr;
+    const float v = std::strtof(p, &stop);
+    if (stop == p) break;
+    params[n++] = v;
+    p = stop;
+    while (*p == ',' || *p == ' ' || *p == '\n' || *p == '\r' || *p == '\t') p++;
+  }
+  return n == STC_DISPATCH_MODEL_PARAMS && *p == ']';
+}
+
+std::string beside_executable(const char* argv0, const char* name) {
+  std::string dir(argv0);
+  const size_t slash = dir.rfind('/');
+  dir = slash == std::string::npos ? std::string(".") : dir.substr(0, slash);
+  return dir + "/" + name;
 }
 
 }  // namespace
@@ -45,6 +94,8 @@ int main(int argc, char** argv) {
   opts.flags = STC_F_TIMING;
   int device = 0;
   bool json = false;
+  bool zero_negative = false;
+  std::string model_path;
   for (int i = 1; i < argc; i++) {
     std::string a = argv[i];
     if (a == "--strategy" && i + 1 < argc) {
@@ -59,6 +110,10 @@ int main(int argc, char** argv) {
       if (v == "fixed") opts.dispatch = STC_DISPATCH_FIXED;
       else if (v == "learned") opts.dispatch = STC_DISPATCH_LEARNED;
       else return usage(argv[0]);
+    } else if (a == "--model" && i + 1 < argc) {
+      model_path = argv[++i];
+    } else if (a == "--zero-negative") {
+      zero_negative = true;
     } else if (a == "--device" && i + 1 < argc) {
       device = std::atoi(argv[++i]);
     } else if (a == "--json") {
@@ -76,7 +131,8 @@ int main(int argc, char** argv) {
   Clock total;
   stc_edge_list el;
   Clock io;
-  stc_status s = stc_load_edge_list(path, &el);
+  stc_status s = is_mtx(path) ? stc_load_mtx(path, zero_negative ? STC_MTX_ZERO_NEGATIVE : 0u, &el)
+                              : stc_load_edge_list(path, &el);
   if (s == STC_ERR_IO) {
     std::perror(path);
     return 1;
@@ -94,6 +150,17 @@ int main(int argc, char** argv) {
     std::fprintf(stderr, "stc: cannot open CUDA device %d: %s\n", device, stc_status_string(s));
     stc_free_edge_list(&el);
     return 1;
+  }
+  if (opts.dispatch == STC_DISPATCH_LEARNED) {
+    float params[STC_DISPATCH_MODEL_PARAMS];
+    const std::string mp = model_path.empty() ? beside_executable(argv[0], "dispatch_model.json")
+                                              : model_path;
+    if (!read_model(mp, params) || stc_ctx_set_dispatch_model(ctx, params) != STC_OK) {
+      std::fprintf(stderr, "stc: cannot load dispatch model %s\n", mp.c_str());
+      stc_free_edge_list(&el);
+      stc_ctx_destroy(ctx);
+      return 1;
+    }
   }
   stc_counts c{};
   Clock run;
