@@ -117,13 +117,14 @@ def load_peaks() -> dict:
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
-def load_traffic(workload: int):
-    """Per-launch DRAM bytes of the counting kernel from the committed ncu summary."""
+def load_traffic(workload: int, rmat_scale: int = 24):
+    """DRAM bytes (read + write) of one count stage, from the committed ncu
+    summary (profiles/count_rmat24_traffic.md), or None where none was taken."""
     p = ROOT / "profiles" / "ncu_traffic.json"
-    if not p.exists():
+    if not p.exists() or (workload == 3 and rmat_scale != 24):
         return None
-    d = json.loads(p.read_text())
-    return d.get(str(workload))
+    e = json.loads(p.read_text()).get(str(workload))
+    return e["bytes_per_count"] if e else None
 
 
 def golden_counts(workload: int):
@@ -425,7 +426,7 @@ def run_gpu(args) -> None:
         peaks = load_peaks()
         cms = statistics.mean(count_ms)
         achieved = alg_bytes / (cms / 1e3) / 1e9
-        traffic = load_traffic(args.workload)
+        traffic = load_traffic(args.workload, args.rmat_scale)
         cpu = None
         if world == 1 and not args.skip_cpu:
             r = cpu_reference_sample()
