@@ -198,6 +198,27 @@ stc_status stc_count_shard(stc_ctx* ctx, const uint32_t* src, const uint32_t* ds
                            const int8_t* sign, uint64_t m, const stc_opts* opts, uint32_t shard,
                            uint32_t shards, stc_counts* out, uint64_t* range_out);
 
+/* The whole path from `u v sign` text, parsed on the GPU: load_graph's
+ * grammar (MC/graph_io.h:72-212, as stc_parse_edge_text) followed by
+ * stc_count.  `data` is host memory, or device memory with
+ * STC_F_DEVICE_INPUT; it is copied into a device buffer and split into lines,
+ * parsed and compacted by kernels.  `info` (optional) receives the data line
+ * count and n as stc_parse_edge_text reports them.  stats.ms_h2d covers the
+ * copy and the parse. */
+typedef struct stc_text_info {
+  uint64_t lines; /* data lines (the reference's raw_edges) */
+  uint32_t n;     /* max kept id + 1 (1 when no edge is kept, 0 for empty text) */
+  uint32_t reserved;
+} stc_text_info;
+stc_status stc_count_text(stc_ctx* ctx, const char* data, uint64_t size, const stc_opts* opts,
+                          stc_counts* out, stc_text_info* info);
+
+/* The GPU parser's edge list, copied to host arrays (free with
+ * stc_free_edge_list): identical to stc_parse_edge_text's for the same
+ * bytes. */
+stc_status stc_parse_edge_text_gpu(stc_ctx* ctx, const char* data, uint64_t size,
+                                   const stc_opts* opts, stc_edge_list* out);
+
 /* build_forward_csr + sort_adj_lists (MC/graph_io.h:231-402,
  * MC/tc_serial.cpp:33-93) on the GPU; the result is returned in host memory
  * in the reference's layout.  Free with stc_free_forward_csr. */

@@ -12,6 +12,7 @@ from __future__ import annotations
 
 import ctypes as C
 from dataclasses import dataclass
+from pathlib import Path
 from typing import Iterable, Optional, Sequence
 
 import numpy as np
@@ -280,6 +281,32 @@ class Context:
         _check(lib().stc_count_shard(self._h, _ptr(src), _ptr(dst), _ptr(sign), m, C.byref(o),
                                      shard, shards, C.byref(out), rng), self._h)
         return GlobalTriCounts(out.t0, out.t1, out.t2, out.t3), (int(rng[0]), int(rng[1]))
+
+    def count_text(self, data, *, strategy="auto", dispatch="fixed", timing=True):
+        """The whole path from `u v sign` text parsed on the GPU: bytes, a
+        path, or a torch CUDA uint8 tensor.  Returns (counts, data lines, n)."""
+        dev = hasattr(data, "is_cuda") and data.is_cuda
+        if isinstance(data, (str, Path)):
+            data = Path(data).read_bytes()
+        info = _capi.stc_text_info()
+        out = _capi.stc_counts()
+        o = self._opts(strategy, dispatch, dev, timing)
+        ptr = C.c_void_p(data.data_ptr()) if dev else C.c_char_p(bytes(data))
+        size = int(data.numel()) if dev else len(data)
+        _check(lib().stc_count_text(self._h, ptr, size, C.byref(o), C.byref(out), C.byref(info)),
+               self._h)
+        return GlobalTriCounts(out.t0, out.t1, out.t2, out.t3), info.lines, info.n
+
+    def parse_edge_text_gpu(self, data: bytes) -> EdgeList:
+        """The GPU text parser's edge list (same result as parse_edge_text)."""
+        el = _capi.stc_edge_list()
+        o = self._opts(timing=False)
+        _check(lib().stc_parse_edge_text_gpu(self._h, C.c_char_p(data), len(data), C.byref(o),
+                                             C.byref(el)), self._h)
+        try:
+            return _edge_list_from_c(el)
+        finally:
+            lib().stc_free_edge_list(C.byref(el))
 
     def count_edge_list(self, el: EdgeList, **kw) -> GlobalTriCounts:
         return self.count(el.src, el.dst, el.sign, **kw)

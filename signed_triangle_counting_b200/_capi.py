@@ -50,6 +50,10 @@ class stc_stats(C.Structure):
                 ("kernel_launches", C.c_uint32), ("reserved", C.c_uint32)]
 
 
+class stc_text_info(C.Structure):
+    _fields_ = [("lines", C.c_uint64), ("n", C.c_uint32), ("reserved", C.c_uint32)]
+
+
 class stc_tuning(C.Structure):
     _fields_ = [("block_threads", C.c_uint32), ("hash_factor", C.c_uint32 * 3),
                 ("unroll", C.c_uint32 * 3)]
@@ -104,6 +108,10 @@ SIGNATURES = [
     ("stc_count_shard", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64,
                                   C.POINTER(stc_opts), C.c_uint32, C.c_uint32,
                                   C.POINTER(stc_counts), u64p]),
+    ("stc_count_text", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(stc_opts),
+                                 C.POINTER(stc_counts), C.POINTER(stc_text_info)]),
+    ("stc_parse_edge_text_gpu", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(stc_opts),
+                                          C.POINTER(stc_edge_list)]),
     ("stc_build_forward_csr", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_uint64, C.POINTER(stc_opts),
                                         C.POINTER(stc_forward_csr)]),

@@ -33,7 +33,7 @@ NVCC_FLAGS = ARCH + [
 CXX_FLAGS = ["-O3", "-march=x86-64-v3", "-std=c++17", "-fPIC", "-Wall", "-Wno-unused-function",
              f"-I{INCLUDE}", f"-I{CSRC}"]
 
-CUDA_SOURCES = ["capi.cu", "build.cu", "count.cu", "dispatch.cu"]
+CUDA_SOURCES = ["capi.cu", "build.cu", "count.cu", "dispatch.cu", "text_gpu.cu"]
 HOST_SOURCES = ["text_ingest.cpp", "mtx_ingest.cpp", "synth_host.cpp"]
 
 

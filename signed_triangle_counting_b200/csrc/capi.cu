@@ -292,6 +292,82 @@ stc_status stc_count_shard(stc_ctx* c, const uint32_t* src, const uint32_t* dst,
   });
 }
 
+namespace {
+
+// Copies text (host, or device with STC_F_DEVICE_INPUT) into B_TEXT, padded
+// with zero bytes to a multiple of 16, and parses it on the device.
+uint64_t stage_and_parse_text(stc_ctx* c, const char* data, uint64_t size, const stc_opts* o,
+                              DeviceInput* in, uint64_t* lines, uint32_t* n) {
+  if (size && !data) fail(STC_ERR_INVALID_ARGUMENT, "null text");
+  const uint64_t padded = (size + 15) & ~15ull;
+  char* d_text = buffer<char>(c, B_TEXT, padded ? padded : 16);
+  if (size) {
+    const bool dev = o && (o->flags & STC_F_DEVICE_INPUT);
+    STC_CUDA(cudaMemcpyAsync(d_text, data, size, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                             c->stream));
+    if (padded > size) STC_CUDA(cudaMemsetAsync(d_text + size, 0, padded - size, c->stream));
+  }
+  uint32_t* s = nullptr;
+  uint32_t* d = nullptr;
+  int8_t* g = nullptr;
+  const uint64_t m = parse_text_device(c, d_text, size, &s, &d, &g, lines, n);
+  *in = DeviceInput{s, d, g};
+  return m;
+}
+
+}  // namespace
+
+stc_status stc_count_text(stc_ctx* c, const char* data, uint64_t size, const stc_opts* o,
+                          stc_counts* out, stc_text_info* info) {
+  if (!c || !out) return STC_ERR_INVALID_ARGUMENT;
+  return guarded(c, [&] {
+    CountConfig cfg = count_config(o);
+    begin_call(c, o);
+    DeviceInput in;
+    uint64_t lines = 0;
+    uint32_t n = 0;
+    const uint64_t m = stage_and_parse_text(c, data, size, o, &in, &lines, &n);
+    DeviceGraph g;
+    build_graph(c, in.src, in.dst, in.sign, m, g);
+    count_triangles(c, g, cfg);
+    mark(c, 5);
+    end_call(c, g, out);
+    if (info) *info = stc_text_info{lines, size ? n : 0u, 0u};
+  });
+}
+
+stc_status stc_parse_edge_text_gpu(stc_ctx* c, const char* data, uint64_t size,
+                                   const stc_opts* o, stc_edge_list* out) {
+  if (!c || !out) return STC_ERR_INVALID_ARGUMENT;
+  memset(out, 0, sizeof(*out));
+  return guarded(c, [&] {
+    begin_call(c, o);
+    DeviceInput in;
+    uint64_t lines = 0;
+    uint32_t n = 0;
+    const uint64_t m = stage_and_parse_text(c, data, size, o, &in, &lines, &n);
+    const uint64_t cap = m ? m : 1;
+    out->src = (uint32_t*)malloc(cap * sizeof(uint32_t));
+    out->dst = (uint32_t*)malloc(cap * sizeof(uint32_t));
+    out->sign = (int8_t*)malloc(cap);
+    if (!out->src || !out->dst || !out->sign) {
+      stc_free_edge_list(out);
+      fail(STC_ERR_OUT_OF_MEMORY, "host allocation of the edge list failed");
+    }
+    if (m) {
+      STC_CUDA(cudaMemcpyAsync(out->src, in.src, m * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                               c->stream));
+      STC_CUDA(cudaMemcpyAsync(out->dst, in.dst, m * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                               c->stream));
+      STC_CUDA(cudaMemcpyAsync(out->sign, in.sign, m, cudaMemcpyDeviceToHost, c->stream));
+    }
+    STC_CUDA(cudaStreamSynchronize(c->stream));
+    out->n = size ? n : 0;
+    out->lines = lines;
+    out->m = m;
+  });
+}
+
 stc_status stc_build_forward_csr(stc_ctx* c, const uint32_t* src, const uint32_t* dst,
                                  const int8_t* sign, uint64_t m, const stc_opts* o,
                                  stc_forward_csr* out) {

@@ -41,6 +41,7 @@ enum BufId {
   B_DISPATCH_TRAIN,               // dispatcher training samples and parameters
   B_TIMES,                        // timing recorder: cycles and arcs per cell
   B_SHARD_COST,                   // cost prefix of a sharded count (n + 1 words)
+  B_TEXT,                         // text input of the GPU parser (padded to 16 bytes)
   B_COUNT_
 };
 
@@ -187,6 +188,11 @@ void graph_from_forward_csr(stc_ctx* c, uint32_t n, uint64_t m, const uint64_t* 
 void build_graph_batch(stc_ctx* c, const uint32_t* d_src, const uint32_t* d_dst,
                        const int8_t* d_sign, uint64_t m, const uint64_t* h_eoff, uint32_t G,
                        DeviceGraph& g);
+// GPU text ingest: parses `size` bytes at d_text (device, padded to a
+// multiple of 16 bytes) into the device input arrays; returns the kept edge
+// count, the data line count and n.
+uint64_t parse_text_device(stc_ctx* c, const char* d_text, uint64_t size, uint32_t** src,
+                           uint32_t** dst, int8_t** sign, uint64_t* lines_out, uint32_t* n_out);
 // Forward CSR in the reference's id-space layout, copied to host arrays.
 void export_forward_csr(stc_ctx* c, const DeviceGraph& g, stc_forward_csr* out);
 

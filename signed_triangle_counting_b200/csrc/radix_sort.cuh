@@ -256,16 +256,37 @@ __global__ void __launch_bounds__(kScanThreads) k_range_apply(F f, E emit, uint6
   }
 }
 
-// Runs the three-launch scan; `sums` needs kMaxSortGrid + 1 words.  Returns
-// the grand total through `*d_total` (device) when non-null.
-template <class F, class E>
-inline void range_scan(F f, E emit, uint64_t n, uint64_t* sums, cudaStream_t st,
-                       int* launches = nullptr) {
+// The first two launches of a range scan: per-CTA totals, then their
+// exclusive scan in place; the grand total lands in sums[grid], and the
+// returned grid is what range_apply needs.  `sums` needs kMaxSortGrid + 1
+// words.
+template <class F>
+inline uint32_t range_reduce_scan(F f, uint64_t n, uint64_t* sums, cudaStream_t st,
+                                  int* launches = nullptr) {
   RangePartition p = range_partition(n, kScanTile, kMaxSortGrid);
   k_range_reduce<<<p.grid, kScanThreads, 0, st>>>(f, n, p.per_cta, sums);
   k_scan_small<<<1, 1024, 0, st>>>(sums, p.grid);
+  if (launches) *launches += 2;
+  return p.grid;
+}
+
+// The third launch: every element's exclusive prefix to `emit`, from the
+// offsets range_reduce_scan left in `sums` (which the caller may read, e.g.
+// the total, in between).
+template <class F, class E>
+inline void range_apply(F f, E emit, uint64_t n, const uint64_t* sums, cudaStream_t st,
+                        int* launches = nullptr) {
+  RangePartition p = range_partition(n, kScanTile, kMaxSortGrid);
   k_range_apply<<<p.grid, kScanThreads, 0, st>>>(f, emit, n, p.per_cta, sums);
-  if (launches) *launches += 3;
+  if (launches) *launches += 1;
+}
+
+// The whole three-launch scan.
+template <class F, class E>
+inline void range_scan(F f, E emit, uint64_t n, uint64_t* sums, cudaStream_t st,
+                       int* launches = nullptr) {
+  range_reduce_scan(f, n, sums, st, launches);
+  range_apply(f, emit, n, sums, st, launches);
 }
 
 }  // namespace stc

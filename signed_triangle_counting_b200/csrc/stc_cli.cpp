@@ -3,11 +3,13 @@
 // MC/tc_hash_sign_enu.cpp:76-177).
 //
 //   stc [--strategy auto|merge|hash|search] [--dispatch fixed|learned]
-//       [--model PATH] [--zero-negative] [--device N] [--json] <graph_file>
+//       [--model PATH] [--zero-negative] [--host-ingest] [--device N] [--json]
+//       <graph_file>
 //
-// <graph_file> is `u v sign` text (MC/graph_io.h:72-212) or, when it starts
-// with a `%%MatrixMarket` banner, a coordinate .mtx file as the reference's
-// GPU drivers read (--zero-negative: weight <= 0 is negative, their rule).
+// <graph_file> is `u v sign` text (MC/graph_io.h:72-212), parsed on the GPU
+// (--host-ingest: by the host threads instead), or, when it starts with a
+// `%%MatrixMarket` banner, a coordinate .mtx file as the reference's GPU
+// drivers read (--zero-negative: weight <= 0 is negative, their rule).
 // --dispatch learned loads the model from --model or, by default,
 // dispatch_model.json beside this executable.
 //
@@ -15,6 +17,11 @@
 // `n=.. raw_edges=..`, `forward_edges=..` and per-type block, then the
 // Balanced / Unbalanced / Total lines of the merge and hash programs, then the
 // total time.  Exit status 1 on a usage or I/O error, as in the reference.
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -38,7 +45,8 @@ void stage(const char* label, double seconds) { std::printf("[%s] took %.4f seco
 int usage(const char* prog) {
   std::fprintf(stderr,
                "usage: %s [--strategy auto|merge|hash|search] [--dispatch fixed|learned] "
-               "[--model PATH] [--zero-negative] [--device N] [--json] <graph_file>\n",
+               "[--model PATH] [--zero-negative] [--host-ingest] [--device N] [--json] "
+               "<graph_file>\n",
                prog);
   return 1;
 }
@@ -79,6 +87,35 @@ bool read_model(const std::string& path, float* params) {
   return n == STC_DISPATCH_MODEL_PARAMS && *p == ']';
 }
 
+// A read-only mapping of a whole file.
+struct MappedFile {
+  const char* data = nullptr;
+  uint64_t size = 0;
+  bool open(const char* path) {
+    const int fd = ::open(path, O_RDONLY);
+    if (fd < 0) return false;
+    struct stat st;
+    if (fstat(fd, &st) < 0) {
+      ::close(fd);
+      return false;
+    }
+    size = (uint64_t)st.st_size;
+    if (size) {
+      void* p = mmap(nullptr, size, PROT_READ, MAP_PRIVATE, fd, 0);
+      if (p == MAP_FAILED) {
+        ::close(fd);
+        return false;
+      }
+      data = (const char*)p;
+    }
+    ::close(fd);
+    return true;
+  }
+  ~MappedFile() {
+    if (data) munmap((void*)data, size);
+  }
+};
+
 std::string beside_executable(const char* argv0, const char* name) {
   std::string dir(argv0);
   const size_t slash = dir.rfind('/');
@@ -95,6 +132,7 @@ int main(int argc, char** argv) {
   int device = 0;
   bool json = false;
   bool zero_negative = false;
+  bool host_ingest = false;
   std::string model_path;
   for (int i = 1; i < argc; i++) {
     std::string a = argv[i];
@@ -114,6 +152,8 @@ int main(int argc, char** argv) {
       model_path = argv[++i];
     } else if (a == "--zero-negative") {
       zero_negative = true;
+    } else if (a == "--host-ingest") {
+      host_ingest = true;
     } else if (a == "--device" && i + 1 < argc) {
       device = std::atoi(argv[++i]);
     } else if (a == "--json") {
@@ -129,10 +169,18 @@ int main(int argc, char** argv) {
   if (!path) return usage(argv[0]);
 
   Clock total;
-  stc_edge_list el;
+  const bool mtx = is_mtx(path);
+  const bool gpu_text = !mtx && !host_ingest;
+  stc_edge_list el{};
+  MappedFile text;
   Clock io;
-  stc_status s = is_mtx(path) ? stc_load_mtx(path, zero_negative ? STC_MTX_ZERO_NEGATIVE : 0u, &el)
-                              : stc_load_edge_list(path, &el);
+  stc_status s = STC_OK;
+  if (gpu_text) {
+    s = text.open(path) ? STC_OK : STC_ERR_IO;
+  } else {
+    s = mtx ? stc_load_mtx(path, zero_negative ? STC_MTX_ZERO_NEGATIVE : 0u, &el)
+            : stc_load_edge_list(path, &el);
+  }
   if (s == STC_ERR_IO) {
     std::perror(path);
     return 1;
@@ -141,8 +189,7 @@ int main(int argc, char** argv) {
     std::fprintf(stderr, "%s: %s\n", path, stc_status_string(s));
     return 1;
   }
-  stage("Graph Load (I/O + parse)", io.sec());
-  std::printf("  n=%u  raw_edges=%llu\n", el.n, (unsigned long long)el.lines);
+  const double io_s = io.sec();
 
   stc_ctx* ctx = nullptr;
   s = stc_ctx_create(device, &ctx);
@@ -163,8 +210,15 @@ int main(int argc, char** argv) {
     }
   }
   stc_counts c{};
+  stc_text_info info{};
   Clock run;
-  s = stc_count(ctx, el.src, el.dst, el.sign, el.m, &opts, &c);
+  if (gpu_text) {
+    s = stc_count_text(ctx, text.data, text.size, &opts, &c, &info);
+  } else {
+    info.lines = el.lines;
+    info.n = el.n;
+    s = stc_count(ctx, el.src, el.dst, el.sign, el.m, &opts, &c);
+  }
   const double run_s = run.sec();
   stc_free_edge_list(&el);
   if (s != STC_OK) {
@@ -176,7 +230,10 @@ int main(int argc, char** argv) {
   stc_ctx_last_stats(ctx, &st);
   stc_ctx_destroy(ctx);
 
-  stage("Build Forward CSR", (st.ms_h2d + st.ms_dedup + st.ms_orient) / 1e3);
+  // With GPU ingest the parse runs on the device inside the H2D stage.
+  stage("Graph Load (I/O + parse)", io_s + (gpu_text ? st.ms_h2d / 1e3 : 0.0));
+  std::printf("  n=%u  raw_edges=%llu\n", info.n, (unsigned long long)info.lines);
+  stage("Build Forward CSR", ((gpu_text ? 0.0 : st.ms_h2d) + st.ms_dedup + st.ms_orient) / 1e3);
   stage("Algorithm-Specific Preprocessing (Adjacency List Sort)", st.ms_csr / 1e3);
   std::printf("  forward_edges=%llu\n", (unsigned long long)st.m_forward);
   stage("Triangle Counting Execution", st.ms_count / 1e3);
