@@ -486,7 +486,7 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["mine", "reference"], default="mine")
     ap.add_argument("--workload", type=int, default=3, choices=[1, 2, 3, 4, 5])
-    ap.add_argument("--strategy", default="auto", choices=["auto", "merge", "hash", "search"])
+    ap.add_argument("--strategy", default="auto", choices=["auto", "merge", "hash", "search", "split"])
     ap.add_argument("--dispatch", default="fixed", choices=["fixed", "learned"])
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--no-tuning", action="store_true",

@@ -92,7 +92,13 @@ typedef enum stc_strategy {
   STC_STRATEGY_AUTO = 0,   /* dispatcher picks per edge bucket (default) */
   STC_STRATEGY_MERGE = 1,  /* force the warp-cooperative sorted merge */
   STC_STRATEGY_HASH = 2,   /* force the shared-memory hash probe */
-  STC_STRATEGY_SEARCH = 3  /* force binary search / galloping */
+  STC_STRATEGY_SEARCH = 3, /* force binary search / galloping */
+  STC_STRATEGY_SPLIT = 4   /* force the sign-split stream: B is read from a copy of the
+                              forward CSR whose lists hold their positive heads, then
+                              their negative heads, so a head's sign follows from its
+                              position and no sign byte is loaded; each element is
+                              probed in the staged hash of N+(u)
+                              (MC/tc_merge_sign_split.cpp:20-146, GM/signed_tc.hxx:302-396) */
 } stc_strategy;
 
 typedef enum stc_dispatch {
@@ -292,7 +298,7 @@ stc_status stc_count_batch_packed(stc_ctx* ctx, const uint32_t* src, const uint3
  * all strategies give the same counts, so a table changes only speed. */
 #define STC_DISPATCH_CELLS 1024
 #define STC_DISPATCH_FEATURES 6
-#define STC_DISPATCH_MODEL_PARAMS 163
+#define STC_DISPATCH_MODEL_PARAMS 180
 
 /* Timing recorder: the whole path as stc_count (opts->strategy is usually
  * forced to one strategy), with every arc of the staged and giant classes
@@ -316,27 +322,32 @@ stc_status stc_dispatch_features(float* out);
 
 /* Trains the dispatcher's perceptron on the device.  The perceptron has
  * STC_DISPATCH_FEATURES inputs, 16 hidden ReLU units and one output per
- * strategy (MERGE, HASH, SEARCH): the predicted log2 of the SM cycles one arc
- * of the cell costs under that strategy.  Training is full-batch Adam over
- * `samples` rows of `features`, `targets` (samples x 3 measured log2 cycles
- * per arc, NaN where a strategy is unavailable) and non-negative `weights`,
- * minimising the weighted squared error plus weight_decay / 2 times the
- * squared weights.  Deterministic for a given seed.  `params` receives the
- * STC_DISPATCH_MODEL_PARAMS trained parameters (W1[16][6], b1[16], W2[3][16],
- * b2[3]) and `loss` (optional) the final weighted squared error.
- * samples <= 4096. */
+ * strategy (MERGE, HASH, SEARCH, SPLIT): the predicted log2 of the SM cycles
+ * one arc of the cell costs under that strategy.  Training is full-batch Adam
+ * over `samples` rows of `features`, `targets` (samples x 4 measured log2
+ * cycles per arc, NaN where a strategy is unavailable) and non-negative
+ * `weights`, minimising the weighted squared error plus weight_decay / 2
+ * times the squared weights.  Deterministic for a given seed.  `params`
+ * receives the STC_DISPATCH_MODEL_PARAMS trained parameters (W1[16][6],
+ * b1[16], W2[4][16], b2[4]) and `loss` (optional) the final weighted squared
+ * error.  samples <= 4096. */
 stc_status stc_dispatcher_train(stc_ctx* ctx, const float* features, const float* targets,
                                 const float* weights, uint32_t samples, uint32_t epochs,
                                 float learning_rate, float weight_decay, uint64_t seed,
                                 float* params, float* loss);
 
 /* Loads a trained model into the context: an inference kernel evaluates it
- * on every cell and writes the learned tables on the device, each cell
- * taking the strategy of least predicted cost (the giant class, which stages
- * no hash, never gets HASH).  Calls with dispatch STC_DISPATCH_LEARNED then
- * use these tables.  NULL unloads the model; without a model, LEARNED falls
- * back to the fixed tables. */
-stc_status stc_ctx_set_dispatch_model(stc_ctx* ctx, const float* params);
+ * on every cell and writes the learned tables on the device.  A cell takes
+ * the strategy of least predicted cost where that is predicted at least 5%
+ * cheaper than the fixed table's choice, and keeps the fixed choice
+ * elsewhere (the giant class, which stages no hash, never gets HASH or
+ * SPLIT).  `support` (optional, STC_DISPATCH_CELLS bytes) limits the
+ * overrides to the cells marked non-zero, normally the cells the model's
+ * training data covered, so that the model is not trusted where it would
+ * extrapolate; NULL allows them everywhere.  Calls with dispatch
+ * STC_DISPATCH_LEARNED then use these tables.  params = NULL unloads the
+ * model; without a model, LEARNED falls back to the fixed tables. */
+stc_status stc_ctx_set_dispatch_model(stc_ctx* ctx, const float* params, const uint8_t* support);
 
 /* Copies to `out` (STC_DISPATCH_CELLS bytes) the tables a call with
  * strategy AUTO and this dispatch would use on this context. */

@@ -427,15 +427,17 @@ class Context:
     def train_dispatcher(self, features, targets, weights, *, epochs=3000, lr=0.02,
                          weight_decay=1e-3, seed=1):
         """Trains the dispatcher's perceptron on the device: features
-        (samples, DISPATCH_FEATURES), targets (samples, 3) measured log2
-        cycles per arc of MERGE / HASH / SEARCH (NaN = unavailable), weights
+        (samples, DISPATCH_FEATURES), targets (samples, DISPATCH_OUTPUTS)
+        measured log2 cycles per arc of MERGE / HASH / SEARCH / SPLIT (NaN =
+        unavailable), weights
         (samples,).  Returns (parameters, final weighted squared error)."""
         X = np.ascontiguousarray(features, np.float32)
         T = np.ascontiguousarray(targets, np.float32)
         w = np.ascontiguousarray(weights, np.float32)
-        if (X.ndim != 2 or X.shape[1] != _capi.DISPATCH_FEATURES or T.shape != (len(X), 3)
-                or w.shape != (len(X),)):
-            raise ValueError("features (S, DISPATCH_FEATURES), targets (S, 3), weights (S,)")
+        if (X.ndim != 2 or X.shape[1] != _capi.DISPATCH_FEATURES
+                or T.shape != (len(X), _capi.DISPATCH_OUTPUTS) or w.shape != (len(X),)):
+            raise ValueError("features (S, DISPATCH_FEATURES), targets (S, DISPATCH_OUTPUTS), "
+                             "weights (S,)")
         params = np.zeros(_capi.DISPATCH_MODEL_PARAMS, np.float32)
         loss = C.c_float()
         _check(lib().stc_dispatcher_train(self._h, X.ctypes.data_as(_capi.f32p),
@@ -444,23 +446,37 @@ class Context:
                                           params.ctypes.data_as(_capi.f32p), C.byref(loss)), self._h)
         return params, float(loss.value)
 
-    def set_dispatch_model(self, params) -> None:
+    def set_dispatch_model(self, params, support=None) -> None:
         """Loads a model (``DISPATCH_MODEL_PARAMS`` floats) for dispatch="learned";
-        None unloads it (learned then falls back to the fixed tables)."""
+        ``support`` (DISPATCH_CELLS booleans, or cell indices) limits its
+        overrides of the fixed tables to those cells.  None unloads it
+        (learned then falls back to the fixed tables)."""
         if params is None:
-            _check(lib().stc_ctx_set_dispatch_model(self._h, None), self._h)
+            _check(lib().stc_ctx_set_dispatch_model(self._h, None, None), self._h)
             return
         p = np.ascontiguousarray(params, np.float32)
         if p.shape != (_capi.DISPATCH_MODEL_PARAMS,):
             raise ValueError(f"a model has {_capi.DISPATCH_MODEL_PARAMS} parameters")
-        _check(lib().stc_ctx_set_dispatch_model(self._h, p.ctypes.data_as(_capi.f32p)), self._h)
+        mask = None
+        if support is not None:
+            sup = np.asarray(support)
+            if sup.dtype == bool or sup.shape == (_capi.DISPATCH_CELLS,) and sup.max(initial=0) <= 1:
+                mask = np.ascontiguousarray(sup, np.uint8)
+            else:
+                mask = np.zeros(_capi.DISPATCH_CELLS, np.uint8)
+                mask[sup.astype(np.int64)] = 1
+            if mask.shape != (_capi.DISPATCH_CELLS,):
+                raise ValueError("support: DISPATCH_CELLS booleans or cell indices")
+        _check(lib().stc_ctx_set_dispatch_model(self._h, p.ctypes.data_as(_capi.f32p),
+                                                mask.ctypes.data_as(_capi.u8p)
+                                                if mask is not None else None), self._h)
 
     def load_dispatch_model(self, path=None) -> dict:
         """Loads a model file written by ``dispatcher.save`` (default: the
         model shipped with the package) and returns its metadata."""
         from . import dispatcher
         model = dispatcher.load(path)
-        self.set_dispatch_model(model["params"])
+        self.set_dispatch_model(model["params"], model.get("support"))
         return model
 
     def dispatch_tables(self, dispatch="fixed") -> np.ndarray:

@@ -79,10 +79,11 @@ STC_ERR_DEVICE_TIMEOUT = 6
 STC_ERR_NO_DEVICE = 7
 STC_ERR_INTERNAL = 8
 
-STRATEGY = {"auto": 0, "merge": 1, "hash": 2, "search": 3}
+STRATEGY = {"auto": 0, "merge": 1, "hash": 2, "search": 3, "split": 4}
 DISPATCH_CELLS = 1024
 DISPATCH_FEATURES = 6
-DISPATCH_MODEL_PARAMS = 163
+DISPATCH_MODEL_PARAMS = 180
+DISPATCH_OUTPUTS = 4  # merge, hash, search, split
 DISPATCH = {"fixed": 0, "learned": 1}
 F_DEVICE_INPUT = 0x1
 F_TIMING = 0x2
@@ -133,7 +134,7 @@ SIGNATURES = [
     ("stc_dispatch_features", C.c_int, [f32p]),
     ("stc_dispatcher_train", C.c_int, [C.c_void_p, f32p, f32p, f32p, C.c_uint32, C.c_uint32,
                                        C.c_float, C.c_float, C.c_uint64, f32p, f32p]),
-    ("stc_ctx_set_dispatch_model", C.c_int, [C.c_void_p, f32p]),
+    ("stc_ctx_set_dispatch_model", C.c_int, [C.c_void_p, f32p, u8p]),
     ("stc_dispatch_tables", C.c_int, [C.c_void_p, C.c_uint32, u8p]),
     ("stc_ctx_set_tuning", C.c_int, [C.c_void_p, C.POINTER(stc_tuning)]),
     ("stc_ctx_get_tuning", C.c_int, [C.c_void_p, C.POINTER(stc_tuning)]),

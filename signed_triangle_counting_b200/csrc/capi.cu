@@ -135,7 +135,7 @@ constexpr uint64_t kBatchGroupEdges = 1536ull << 20;
 CountConfig count_config(const stc_opts* o) {
   CountConfig cfg;
   if (o) {
-    if (o->strategy > STC_STRATEGY_SEARCH) fail(STC_ERR_INVALID_ARGUMENT, "unknown strategy");
+    if (o->strategy > STC_STRATEGY_SPLIT) fail(STC_ERR_INVALID_ARGUMENT, "unknown strategy");
     if (o->dispatch > STC_DISPATCH_LEARNED) fail(STC_ERR_INVALID_ARGUMENT, "unknown dispatch");
     cfg.strategy = o->strategy;
     cfg.dispatch = o->dispatch;
@@ -615,11 +615,11 @@ stc_status stc_dispatcher_train(stc_ctx* c, const float* features, const float* 
   });
 }
 
-stc_status stc_ctx_set_dispatch_model(stc_ctx* c, const float* params) {
+stc_status stc_ctx_set_dispatch_model(stc_ctx* c, const float* params, const uint8_t* support) {
   if (!c) return STC_ERR_INVALID_ARGUMENT;
   return guarded(c, [&] {
     c->stream = c->own_stream;
-    load_dispatch_model(c, params);
+    load_dispatch_model(c, params, support);
   });
 }
 

@@ -64,6 +64,10 @@ struct Csr {
   const int8_t* __restrict__ sgn;
   const uint32_t* __restrict__ verts;  // rank -> id (per-source counts only)
   uint32_t n;
+  // Sign-split heads (same offsets, padded likewise) and positives per
+  // vertex; null unless a count uses STC_STRATEGY_SPLIT.
+  const uint32_t* __restrict__ nbr_split = nullptr;
+  const uint32_t* __restrict__ psplit = nullptr;
 };
 
 // Per-thread type counters indexed by the number of negative edges.
@@ -170,18 +174,20 @@ constexpr uint32_t kIdMask = 0x7FFFFFFFu;  // hash keys: id | negative << 31
 
 // Shared-memory image of one staged list of capacity `cap` with `nb` hash
 // buckets: the hash (two 32-bit keys per 8-byte bucket), the sorted ids,
-// each arc's B extent [lo, hi) as element indices of the CSR, the chunk
-// prefix sums, then the byte arrays (list signs, arc strategies).
+// each arc's B extent [lo, hi) as element indices of the CSR, the first
+// negative head of a SPLIT arc's B in the split copy, the chunk prefix
+// sums, then the byte arrays (list signs, arc strategies).
 struct StageMem {
   uint32_t* hk;
   uint32_t* a;
   uint32_t* lo;
   uint32_t* hi;
+  uint32_t* sp;
   uint32_t* pre;
   int8_t* s;
   uint8_t* st;
   __host__ __device__ static constexpr size_t bytes(uint32_t cap, uint32_t nb) {
-    return 8ull * nb + 18ull * cap + 4;
+    return 8ull * nb + 22ull * cap + 4;
   }
   __device__ static StageMem carve(unsigned char* p, uint32_t cap, uint32_t nb) {
     StageMem m;
@@ -193,6 +199,8 @@ struct StageMem {
     m.lo = w;
     w += cap;
     m.hi = w;
+    w += cap;
+    m.sp = w;
     w += cap;
     m.pre = w;
     w += cap + 1;
@@ -248,7 +256,9 @@ __device__ __forceinline__ void stage(const Csr& g, uint64_t ub, uint32_t d, uin
            atomicCAS(&m.hk[2 * b + 1], kEmpty, key) != kEmpty)
       b = (b + 1) & (geo.nb - 1);
     const uint32_t blen = m.hi[i] - m.lo[i];
-    m.st[i] = (i + 1 < d && blen) ? table[size_bucket(d - i - 1)][size_bucket(blen)] : kNoArc;
+    const uint8_t st = (i + 1 < d && blen) ? table[size_bucket(d - i - 1)][size_bucket(blen)] : kNoArc;
+    m.st[i] = st;
+    if (st == STC_STRATEGY_SPLIT) m.sp[i] = m.lo[i] + g.psplit[x];
   }
   sync();
 }
@@ -267,7 +277,7 @@ __device__ __noinline__ uint32_t probe_rest(const uint32_t* hk, uint32_t nb, uin
 
 __device__ __forceinline__ uint32_t arc_chunks(const StageMem& m, uint32_t i) {
   const uint8_t st = m.st[i];
-  if (st != STC_STRATEGY_HASH && st != STC_STRATEGY_MERGE) return 0;
+  if (st != STC_STRATEGY_HASH && st != STC_STRATEGY_MERGE && st != STC_STRATEGY_SPLIT) return 0;
   return ((m.hi[i] + 3) >> 2) - (m.lo[i] >> 2);
 }
 
@@ -315,6 +325,23 @@ __device__ __forceinline__ uint32_t chunk_mask(uint32_t ci, uint32_t lo, uint32_
   return ((1u << last) - 1) & ~((1u << first) - 1);
 }
 
+// Chunk ci of an arc's B: from the sorted heads with their sign bytes, or,
+// for a SPLIT arc, from the sign-split copy, where an element is negative
+// exactly when its index is at least `sp` (the sign word is synthesised in
+// the layout of the sign bytes: bit 8 e + 7 for element e).
+__device__ __forceinline__ void load_chunk(const Csr& g, uint32_t ci, uint32_t st, uint32_t sp,
+                                           uint4& q, uint32_t& sw) {
+  if (st == STC_STRATEGY_SPLIT) {
+    q = reinterpret_cast<const uint4*>(g.nbr_split)[ci];
+    const uint32_t g0 = 4 * ci;
+    sw = ((uint32_t)(g0 >= sp) << 7) | ((uint32_t)(g0 + 1 >= sp) << 15) |
+         ((uint32_t)(g0 + 2 >= sp) << 23) | ((uint32_t)(g0 + 3 >= sp) << 31);
+  } else {
+    q = reinterpret_cast<const uint4*>(g.nbr)[ci];
+    sw = reinterpret_cast<const uint32_t*>(g.sgn)[ci];
+  }
+}
+
 // One int4 chunk of B for arc k of a staged list: four ids q, their four sign
 // bytes sw, and the mask vm (non-zero) of the ids inside the arc.  HASH looks
 // every id up in the staged hash (one 8-byte bucket read gives membership and
@@ -323,7 +350,7 @@ __device__ __forceinline__ uint32_t chunk_mask(uint32_t ci, uint32_t lo, uint32_
 __device__ __forceinline__ void process_chunk(const StageMem& m, uint32_t d, const Geo& geo,
                                               const uint4& q, uint32_t sw, uint32_t vm, uint32_t k,
                                               uint32_t nuv, uint32_t st, PackedCounts& pc) {
-  if (st == STC_STRATEGY_HASH) {
+  if (st == STC_STRATEGY_HASH || st == STC_STRATEGY_SPLIT) {
 #pragma unroll
     for (uint32_t e = 0; e < 4; e++) {
       const uint32_t x = pick4(q, e);
@@ -369,8 +396,6 @@ __device__ __forceinline__ void stream_pass(const Csr& g, const StageMem& m, uin
   const uint32_t per = (total + warps - 1) / warps;
   const uint32_t c_begin = min(total, warp * per), c_end = min(total, c_begin + per);
   if (c_begin >= c_end) return;
-  const uint4* __restrict__ nbr4 = reinterpret_cast<const uint4*>(g.nbr);
-  const uint32_t* __restrict__ sgn4 = reinterpret_cast<const uint32_t*>(g.sgn);
   // Arc cursor: the last arc with pre[k] <= first chunk of this lane.
   uint32_t k;
   {
@@ -383,7 +408,7 @@ __device__ __forceinline__ void stream_pass(const Csr& g, const StageMem& m, uin
     k = lo_k;
   }
   uint32_t pk = m.pre[k], pk1 = m.pre[k + 1], alo = m.lo[k], ahi = m.hi[k];
-  uint32_t ast = m.st[k], anuv = m.s[k] < 0;
+  uint32_t ast = m.st[k], anuv = m.s[k] < 0, asp = m.sp[k];
   uint32_t rounds = 0;
   for (uint32_t base = c_begin; base < c_end; base += 32 * U) {
     uint4 q[U];
@@ -403,10 +428,10 @@ __device__ __forceinline__ void stream_pass(const Csr& g, const StageMem& m, uin
           ahi = m.hi[k];
           ast = m.st[k];
           anuv = m.s[k] < 0;
+          asp = m.sp[k];
         }
         const uint32_t ci = (alo >> 2) + (c - pk);
-        q[u] = nbr4[ci];
-        sw[u] = sgn4[ci];
+        load_chunk(g, ci, ast, asp, q[u], sw[u]);
         vm[u] = chunk_mask(ci, alo, ahi);
         sk[u] = k;
         snuv[u] = anuv;
@@ -471,13 +496,13 @@ __device__ __forceinline__ void record_arc(const ArcTimes& at, uint32_t tclass, 
 // chunks of B.
 __device__ __forceinline__ void arc_stream(const Csr& g, const StageMem& m, uint32_t d, uint32_t k,
                                            uint32_t lane, const Geo& geo, PackedCounts& pc) {
-  const uint4* __restrict__ nbr4 = reinterpret_cast<const uint4*>(g.nbr);
-  const uint32_t* __restrict__ sgn4 = reinterpret_cast<const uint32_t*>(g.sgn);
   const uint32_t lo = m.lo[k], hi = m.hi[k], st = m.st[k], nuv = m.s[k] < 0;
+  const uint32_t sp = st == STC_STRATEGY_SPLIT ? m.sp[k] : 0u;
   const uint32_t c1 = (hi + 3) >> 2;
   for (uint32_t ci = (lo >> 2) + lane; ci < c1; ci += 32) {
-    const uint4 q = nbr4[ci];
-    const uint32_t sw = sgn4[ci];
+    uint4 q;
+    uint32_t sw;
+    load_chunk(g, ci, st, sp, q, sw);
     process_chunk(m, d, geo, q, sw, chunk_mask(ci, lo, hi), k, nuv, st, pc);
   }
 }
@@ -1150,6 +1175,64 @@ void count_persistent(stc_ctx* c, const Csr& csr, const ClassBounds& cb, uint32_
   STC_CUDA(cudaGraphLaunch(c->graph_exec, st));
 }
 
+// ------------------------------------------------------------- split ----
+// The sign-split copy of the arc heads (the layout of
+// MC/tc_merge_sign_split.cpp:20-146 and GM/signed_tc.hxx:302-396, kept beside
+// the sorted heads instead of replacing them): each list's positive heads,
+// then its negative heads, both ascending; psplit[u] = positive heads of u.
+// Each lane takes one vertex; a list of up to 32 heads is split by its lane
+// alone (count the positives, then place every head), and the warp splits
+// the longer lists of its 32 vertices together, 32 heads per step, placing
+// them with ballots and the popcounts of the lanes below.
+constexpr uint32_t kSplitShort = 32;
+
+__global__ void k_split_csr(const uint64_t* __restrict__ off, const uint32_t* __restrict__ nbr,
+                            const int8_t* __restrict__ sgn, uint32_t n,
+                            uint32_t* __restrict__ out, uint32_t* __restrict__ psplit) {
+  const uint32_t lane = lane_id();
+  const uint32_t lt = lanemask_lt();
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
+    const uint32_t u = base + lane;
+    const bool valid = u < n;
+    const uint64_t b = valid ? off[u] : 0, e = valid ? off[u + 1] : 0;
+    if (valid && e - b <= kSplitShort) {
+      uint32_t pos = 0;
+      for (uint64_t i = b; i < e; i++) pos += sgn[i] >= 0;
+      uint32_t wp = 0, wn = 0;
+      for (uint64_t i = b; i < e; i++) {
+        const uint32_t x = nbr[i];
+        if (sgn[i] >= 0) out[b + wp++] = x;
+        else out[b + pos + wn++] = x;
+      }
+      psplit[u] = pos;
+    }
+    uint32_t longs = __ballot_sync(kFull, valid && e - b > kSplitShort);
+    while (longs) {
+      const int src = __ffs(longs) - 1;
+      longs &= longs - 1;
+      const uint64_t lb = __shfl_sync(kFull, b, src), le = __shfl_sync(kFull, e, src);
+      uint32_t pos = 0;
+      for (uint64_t at = lb; at < le; at += 32) {
+        const uint64_t i = at + lane;
+        pos += __popc(__ballot_sync(kFull, i < le && sgn[i] >= 0));
+      }
+      uint32_t wp = 0, wn = 0;
+      for (uint64_t at = lb; at < le; at += 32) {
+        const uint64_t i = at + lane;
+        const bool in = i < le;
+        const bool p = in && sgn[i] >= 0;
+        const uint32_t bp = __ballot_sync(kFull, p), bn = __ballot_sync(kFull, in && !p);
+        if (p) out[lb + wp + __popc(bp & lt)] = nbr[i];
+        else if (in) out[lb + pos + wn + __popc(bn & lt)] = nbr[i];
+        wp += __popc(bp);
+        wn += __popc(bn);
+      }
+      if (lane == 0) psplit[base + src] = pos;
+    }
+  }
+}
+
 // ------------------------------------------------------------ shards ----
 // A shard of a count is a contiguous range of source vertices in rank space
 // chosen so that the shards carry about the same merge-model cost: vertex u
@@ -1245,10 +1328,25 @@ const uint8_t* dispatch_tables(stc_ctx* c, const CountConfig& cfg) {
   return buffer<uint8_t>(c, B_DISPATCH_FIXED, kTableBytes);
 }
 
-void count_triangles(stc_ctx* c, const DeviceGraph& g, const CountConfig& cfg) {
-  if (g.n == 0 || g.m_fwd == 0) return;
+// Builds the sign-split copy of g's heads on the context's stream.
+void build_split(stc_ctx* c, DeviceGraph& g) {
+  g.nbr_split = buffer<uint32_t>(c, B_SPLIT_NBR, g.m_fwd + 4);
+  g.psplit = buffer<uint32_t>(c, B_SPLIT_POS, g.n);
+  STC_CUDA(cudaMemsetAsync(g.nbr_split + g.m_fwd, 0, 4 * sizeof(uint32_t), c->stream));
+  k_split_csr<<<kSMs * 8, 256, 0, c->stream>>>(g.off, g.nbr, g.sgn, g.n, g.nbr_split, g.psplit);
+  c->launches++;
+  STC_CUDA(cudaGetLastError());
+}
+
+void count_triangles(stc_ctx* c, const DeviceGraph& gin, const CountConfig& cfg) {
+  if (gin.n == 0 || gin.m_fwd == 0) return;
   cudaStream_t st = c->stream;
-  Csr csr{g.off, g.nbr, g.sgn, g.verts, g.n};
+  DeviceGraph g = gin;
+  const bool split = cfg.strategy == STC_STRATEGY_SPLIT ||
+                     (cfg.strategy == STC_STRATEGY_AUTO && cfg.dispatch == STC_DISPATCH_LEARNED &&
+                      c->model_loaded && c->learned_uses_split);
+  if (split) build_split(c, g);
+  Csr csr{g.off, g.nbr, g.sgn, g.verts, g.n, g.nbr_split, g.psplit};
   unsigned long long* ctr = (unsigned long long*)counters(c);
   const uint8_t* d_table = dispatch_tables(c, cfg);
   const bool timed = cfg.arc_cycles != nullptr;
@@ -1450,7 +1548,7 @@ extern "C" stc_status stc_count_oriented_csr_noalloc(const uint64_t* d_offsets,
                                             nullptr);
   STC_NA(cudaMemsetAsync(ctr + C_WORK, 0, 8 * sizeof(uint64_t), st));
 
-  const Csr csr{d_offsets, d_heads, d_signs, nullptr, n};
+  const Csr csr{d_offsets, d_heads, d_signs, nullptr, n, nullptr, nullptr};
   int launches = 0;
   try {
     launch_classes<TotalSink, false>(st, csr, lists, counts, starts, max_fdeg, ctr, scr->table,

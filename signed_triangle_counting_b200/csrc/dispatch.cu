@@ -32,7 +32,8 @@ constexpr int kTrainWarps = kTrainThreads / 32;
 constexpr uint32_t kMaxTrainSamples = 4096;
 constexpr uint64_t kStreamMlpInit = 11;  // generator stream of the initial weights
 
-// Parameter offsets (layout W1[hidden][in], b1[hidden], W2[out][hidden], b2[out]).
+// Parameter offsets (layout W1[hidden][in], b1[hidden], W2[out][hidden], b2[out];
+// outputs MERGE, HASH, SEARCH, SPLIT).
 constexpr int kOffB1 = kMlpHidden * kMlpIn;
 constexpr int kOffW2 = kOffB1 + kMlpHidden;
 constexpr int kOffB2 = kOffW2 + kMlpOut * kMlpHidden;
@@ -75,9 +76,18 @@ __device__ __forceinline__ void mlp_forward(const float* p, const float* f, floa
   }
 }
 
-// One thread per cell: the strategy of least predicted cost (HASH excluded
-// for the giant class, which stages no hash).
-__global__ void k_mlp_tables(const float* __restrict__ params, uint8_t* __restrict__ tables) {
+// A learned cell overrides the fixed table only where the model predicts the
+// override at least this much cheaper (log2 of 1.05): the fixed thresholds
+// stay the fallback wherever the model is unsure or extrapolating.
+constexpr float kOverrideMargin = 0.0704f;
+
+// One thread per cell: the strategy of least predicted cost, if the cell is
+// in the model's support and that strategy beats the fixed table's choice by
+// the margin, else the fixed choice.  The giant
+// class stages no hash, so it never takes HASH or SPLIT (its fixed HASH
+// cells run MERGE, and are compared as such).
+__global__ void k_mlp_tables(const float* __restrict__ params, const uint8_t* __restrict__ fixed,
+                             const uint8_t* __restrict__ support, uint8_t* __restrict__ tables) {
   __shared__ float p[kMlpParams];
   for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) p[i] = params[i];
   __syncthreads();
@@ -87,12 +97,16 @@ __global__ void k_mlp_tables(const float* __restrict__ params, uint8_t* __restri
   cell_features(cell, f);
   mlp_forward(p, f, h, z);
   const bool giant = (cell >> 8) == kTableGiant;
+  auto staged_only = [](int o) { return o == STC_STRATEGY_HASH - 1 || o == STC_STRATEGY_SPLIT - 1; };
   int best = 0;
   for (int o = 1; o < kMlpOut; o++) {
-    if (giant && o == STC_STRATEGY_HASH - 1) continue;
+    if (giant && staged_only(o)) continue;
     if (z[o] < z[best]) best = o;
   }
-  tables[cell] = (uint8_t)(best + 1);
+  int fx = fixed[cell] - 1;
+  if (giant && staged_only(fx)) fx = STC_STRATEGY_MERGE - 1;
+  const bool trusted = support == nullptr || support[cell] != 0;
+  tables[cell] = trusted && z[best] + kOverrideMargin < z[fx] ? (uint8_t)(best + 1) : fixed[cell];
 }
 
 // Adds v, summed over the warp, to the warp's gradient row (lane 0 owns it;
@@ -242,21 +256,35 @@ void dispatch_features(float* out) {
   for (uint32_t cell = 0; cell < kTableBytes; cell++) cell_features(cell, out + (size_t)cell * kMlpIn);
 }
 
-void load_dispatch_model(stc_ctx* c, const float* params) {
+void load_dispatch_model(stc_ctx* c, const float* params, const uint8_t* support) {
   if (!params) {
     c->model_loaded = false;
     return;
   }
   for (int i = 0; i < kMlpParams; i++)
     if (!std::isfinite(params[i])) fail(STC_ERR_INVALID_ARGUMENT, "model parameter is not finite");
-  float* d_params = buffer<float>(c, B_DISPATCH_TRAIN, kMlpParams);
+  CountConfig fixed_cfg;
+  fixed_cfg.dispatch = STC_DISPATCH_FIXED;
+  const uint8_t* d_fixed = dispatch_tables(c, fixed_cfg);
+  // Parameters, then the support mask, in one staging buffer.
+  float* d_params = buffer<float>(c, B_DISPATCH_TRAIN, kMlpParams + kTableBytes / sizeof(float));
+  uint8_t* d_support = reinterpret_cast<uint8_t*>(d_params + kMlpParams);
   uint8_t* d_tables = buffer<uint8_t>(c, B_DISPATCH, kTableBytes);
   STC_CUDA(cudaMemcpyAsync(d_params, params, kMlpParams * sizeof(float), cudaMemcpyHostToDevice,
                            c->stream));
-  k_mlp_tables<<<(unsigned)(kTableBytes / 256), 256, 0, c->stream>>>(d_params, d_tables);
+  if (support)
+    STC_CUDA(cudaMemcpyAsync(d_support, support, kTableBytes, cudaMemcpyHostToDevice, c->stream));
+  k_mlp_tables<<<(unsigned)(kTableBytes / 256), 256, 0, c->stream>>>(
+      d_params, d_fixed, support ? d_support : nullptr, d_tables);
   STC_CUDA(cudaGetLastError());
+  uint8_t h[kTableBytes];
+  STC_CUDA(cudaMemcpyAsync(h, d_tables, kTableBytes, cudaMemcpyDeviceToHost, c->stream));
   STC_CUDA(cudaStreamSynchronize(c->stream));
   c->model_loaded = true;
+  // Counts with these tables build the sign-split heads only if some cell
+  // picks SPLIT.
+  c->learned_uses_split = false;
+  for (size_t i = 0; i < kTableBytes; i++) c->learned_uses_split |= h[i] == STC_STRATEGY_SPLIT;
 }
 
 void train_dispatcher(stc_ctx* c, const float* features, const float* targets,

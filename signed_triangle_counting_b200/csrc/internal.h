@@ -42,6 +42,8 @@ enum BufId {
   B_TIMES,                        // timing recorder: cycles and arcs per cell
   B_SHARD_COST,                   // cost prefix of a sharded count (n + 1 words)
   B_TEXT,                         // text input of the GPU parser (padded to 16 bytes)
+  B_SPLIT_NBR,                    // sign-split copy of the arc heads (m + 4)
+  B_SPLIT_POS,                    // positive arcs per vertex (n)
   B_COUNT_
 };
 
@@ -81,11 +83,11 @@ static_assert(kTableBytes == STC_DISPATCH_CELLS, "one table byte per dispatch ce
 
 // The dispatcher's multilayer perceptron: STC_DISPATCH_FEATURES inputs, one
 // hidden ReLU layer, one predicted log2 cost per strategy (MERGE, HASH,
-// SEARCH).
+// SEARCH, SPLIT).
 // Parameter layout: W1[hidden][in], b1[hidden], W2[out][hidden], b2[out].
 constexpr int kMlpIn = STC_DISPATCH_FEATURES;
 constexpr int kMlpHidden = 16;
-constexpr int kMlpOut = 3;
+constexpr int kMlpOut = 4;
 constexpr int kMlpParams = kMlpHidden * kMlpIn + kMlpHidden + kMlpOut * kMlpHidden + kMlpOut;
 static_assert(kMlpParams == STC_DISPATCH_MODEL_PARAMS, "parameter count of the ABI");
 
@@ -114,6 +116,7 @@ struct stc_ctx {
   int launches = 0;
   bool fixed_ready = false;   // B_DISPATCH_FIXED holds the fixed tables
   bool model_loaded = false;  // B_DISPATCH holds the tables of a loaded model
+  bool learned_uses_split = false;  // the learned tables pick STC_STRATEGY_SPLIT somewhere
   // The persistent count captured in a CUDA graph, and the pointers and
   // sizes it was captured with (replayed while they stay the same).
   cudaGraphExec_t graph_exec = nullptr;
@@ -171,6 +174,11 @@ struct DeviceGraph {
   // g owns [gbase[g], gbase[g + 1]).  G == 0 for a single graph.
   uint32_t G = 0;
   uint64_t* gbase = nullptr;
+  // Sign-split copy of the arc heads (each list's positive heads, then its
+  // negative heads, both ascending) and the positive count per vertex; built
+  // when a count uses STC_STRATEGY_SPLIT.
+  uint32_t* nbr_split = nullptr;
+  uint32_t* psplit = nullptr;
 };
 
 // Stage timing helper: records an event when the context is timing.
@@ -225,7 +233,7 @@ void count_triangles(stc_ctx* c, const DeviceGraph& g, const CountConfig& cfg);
 void fixed_dispatch_tables(uint8_t* out);
 void dispatch_features(float* out);
 const uint8_t* dispatch_tables(stc_ctx* c, const CountConfig& cfg);
-void load_dispatch_model(stc_ctx* c, const float* params);
+void load_dispatch_model(stc_ctx* c, const float* params, const uint8_t* support);
 void train_dispatcher(stc_ctx* c, const float* features, const float* targets,
                       const float* weights, uint32_t samples, uint32_t epochs, float lr, float wd,
                       uint64_t seed, float* params, float* loss);

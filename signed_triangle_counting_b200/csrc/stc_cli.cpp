@@ -2,7 +2,7 @@
 // (MC/tc_serial.cpp:172-210, MC/tc_merge_sign_enu.cpp:46-154,
 // MC/tc_hash_sign_enu.cpp:76-177).
 //
-//   stc [--strategy auto|merge|hash|search] [--dispatch fixed|learned]
+//   stc [--strategy auto|merge|hash|search|split] [--dispatch fixed|learned]
 //       [--model PATH] [--zero-negative] [--host-ingest] [--device N] [--json]
 //       <graph_file>
 //
@@ -44,7 +44,7 @@ void stage(const char* label, double seconds) { std::printf("[%s] took %.4f seco
 
 int usage(const char* prog) {
   std::fprintf(stderr,
-               "usage: %s [--strategy auto|merge|hash|search] [--dispatch fixed|learned] "
+               "usage: %s [--strategy auto|merge|hash|search|split] [--dispatch fixed|learned] "
                "[--model PATH] [--zero-negative] [--host-ingest] [--device N] [--json] "
                "<graph_file>\n",
                prog);
@@ -61,8 +61,9 @@ bool is_mtx(const char* path) {
 }
 
 // The "params" array of a dispatch model file (STC_DISPATCH_MODEL_PARAMS
-// floats); false if the file cannot be read or holds a different count.
-bool read_model(const std::string& path, float* params) {
+// floats) and its "support" cell list as a mask (all cells when absent);
+// false if the file cannot be read or holds a different count.
+bool read_model(const std::string& path, float* params, uint8_t* support) {
   FILE* f = std::fopen(path.c_str(), "rb");
   if (!f) return false;
   std::string text;
@@ -84,7 +85,25 @@ bool read_model(const std::string& path, float* params) {
     p = stop;
     while (*p == ',' || *p == ' ' || *p == '\n' || *p == '\r' || *p == '\t') p++;
   }
-  return n == STC_DISPATCH_MODEL_PARAMS && *p == ']';
+  if (n != STC_DISPATCH_MODEL_PARAMS || *p != ']') return false;
+  size_t sat = text.find("\"support\"");
+  if (sat == std::string::npos) {
+    std::memset(support, 1, STC_DISPATCH_CELLS);
+    return true;
+  }
+  sat = text.find('[', sat);
+  if (sat == std::string::npos) return false;
+  std::memset(support, 0, STC_DISPATCH_CELLS);
+  const char* q = text.c_str() + sat + 1;
+  while (true) {
+    while (*q == ' ' || *q == ',' || *q == '\n' || *q == '\r' || *q == '\t') q++;
+    if (*q == ']') return true;
+    char* stop = nullptr;
+    const long cell = std::strtol(q, &stop, 10);
+    if (stop == q || cell < 0 || cell >= STC_DISPATCH_CELLS) return false;
+    support[cell] = 1;
+    q = stop;
+  }
 }
 
 // A read-only mapping of a whole file.
@@ -142,6 +161,7 @@ int main(int argc, char** argv) {
       else if (v == "merge") opts.strategy = STC_STRATEGY_MERGE;
       else if (v == "hash") opts.strategy = STC_STRATEGY_HASH;
       else if (v == "search") opts.strategy = STC_STRATEGY_SEARCH;
+      else if (v == "split") opts.strategy = STC_STRATEGY_SPLIT;
       else return usage(argv[0]);
     } else if (a == "--dispatch" && i + 1 < argc) {
       std::string v = argv[++i];
@@ -200,9 +220,11 @@ int main(int argc, char** argv) {
   }
   if (opts.dispatch == STC_DISPATCH_LEARNED) {
     float params[STC_DISPATCH_MODEL_PARAMS];
+    uint8_t support[STC_DISPATCH_CELLS];
     const std::string mp = model_path.empty() ? beside_executable(argv[0], "dispatch_model.json")
                                               : model_path;
-    if (!read_model(mp, params) || stc_ctx_set_dispatch_model(ctx, params) != STC_OK) {
+    if (!read_model(mp, params, support) ||
+        stc_ctx_set_dispatch_model(ctx, params, support) != STC_OK) {
       std::fprintf(stderr, "stc: cannot load dispatch model %s\n", mp.c_str());
       stc_free_edge_list(&el);
       stc_ctx_destroy(ctx);

@@ -30,16 +30,17 @@ import numpy as np
 
 from . import _capi, dispatch_features, synth
 
-STRATEGIES = ("merge", "hash", "search")  # label k is strategy code k + 1
+STRATEGIES = ("merge", "hash", "search", "split")  # output k is strategy code k + 1
+STAGED_ONLY = (1, 3)  # outputs (HASH, SPLIT) that need the staged hash
 GIANT = 3                                  # class index whose lists stage no hash
 DEFAULT_MODEL = Path(__file__).resolve().parent / "dispatch_model.json"
-FORMAT_VERSION = 2
+FORMAT_VERSION = 3
 
 
 def record(ctx, src, dst, sign) -> dict:
-    """Per-cell cycles of every strategy on one graph (three timed runs).
+    """Per-cell cycles of every strategy on one graph (four timed runs).
 
-    Returns {"cycles": (3, CELLS) float64, "arcs": (CELLS,) float64,
+    Returns {"cycles": (4, CELLS) float64, "arcs": (CELLS,) float64,
     "counts": GlobalTriCounts}; raises if the strategies disagree on the
     counts or on which arcs they timed."""
     cycles, arcs, counts = [], None, None
@@ -59,11 +60,13 @@ def merge(records) -> dict:
 
 
 def cell_costs(rec) -> np.ndarray:
-    """Mean cycles per arc, (3, CELLS); HASH is unavailable in the giant class
-    (its arcs run MERGE), so it costs infinity there; empty cells cost 0."""
+    """Mean cycles per arc, (4, CELLS); HASH and SPLIT are unavailable in the
+    giant class (its arcs run MERGE), so they cost infinity there; empty
+    cells cost 0."""
     arcs = rec["arcs"]
     cost = np.divide(rec["cycles"], np.maximum(arcs, 1.0)[None, :])
-    cost[1, GIANT * 256:(GIANT + 1) * 256] = np.inf
+    for k in STAGED_ONLY:
+        cost[k, GIANT * 256:(GIANT + 1) * 256] = np.inf
     return cost
 
 
@@ -86,36 +89,62 @@ def samples(rec, min_arcs: int = 32, weight_power: float = 0.5):
     return X, targets.astype(np.float32), w.astype(np.float32), cells
 
 
-def regret(rec, tables) -> dict:
+def regret(rec, tables, strategies=STRATEGIES[:3]) -> dict:
     """Cycles a dispatch table would spend on a recording, relative to the
-    per-cell best strategy.  ``tables``: strategy codes, (4, 16, 16) or flat."""
+    per-cell best of ``strategies`` (by default the three the shipped model
+    chooses from).  ``tables``: strategy codes, (4, 16, 16) or flat."""
     t = np.asarray(tables).reshape(-1).astype(np.int64)
     arcs = rec["arcs"]
     cost = cell_costs(rec)
+    best_cost = cost.copy()
+    for k, name in enumerate(STRATEGIES):
+        if name not in strategies:
+            best_cost[k] = np.inf
     k = t - 1
-    # The giant class runs MERGE where a table says HASH.
+    # The giant class runs MERGE where a table says HASH or SPLIT.
     giant = np.arange(len(t)) // 256 == GIANT
-    k = np.where(giant & (k == 1), 0, k)
+    k = np.where(giant & np.isin(k, STAGED_ONLY), 0, k)
     used = arcs > 0
     chosen = cost[k, np.arange(len(t))]
     spent = float((arcs * np.where(used, chosen, 0.0)).sum())
-    best = float((arcs * np.where(used, cost.min(axis=0), 0.0)).sum())
+    best = float((arcs * np.where(used, best_cost.min(axis=0), 0.0)).sum())
     return {"cycles": spent, "best_cycles": best, "ratio": spent / best if best else 1.0}
 
 
+# Output bias that keeps a strategy out of every table (its predicted log2
+# cost can never be the least).
+EXCLUDED_BIAS = 1e30
+
+
 def train(ctx, rec, *, epochs: int = 3000, lr: float = 0.02, weight_decay: float = 1e-3,
-          seed: int = 1, min_arcs: int = 32, weight_power: float = 0.5):
+          seed: int = 1, min_arcs: int = 32, weight_power: float = 0.5, use_split: bool = False):
     """Trains on a recording and loads the model into ``ctx``; returns
     (params, info).  ``weighted_accuracy``: the weight of the training cells
-    whose table entry is their measured fastest strategy."""
+    whose table entry is their measured fastest strategy.
+
+    SPLIT is left out unless ``use_split``: the per-arc recorder measures it
+    5-17% cheaper than HASH, but counted in the packed stream (forced on
+    RMAT-24: 407.4 vs 406.1 ms) it gains nothing, and any table that uses it
+    also pays for building the sign-split heads.  Left out, its targets are
+    dropped and its output bias is set to EXCLUDED_BIAS."""
     X, T, w, cells = samples(rec, min_arcs, weight_power)
+    if not use_split:
+        T = T.copy()
+        T[:, 3] = np.nan
     params, loss = ctx.train_dispatcher(X, T, w, epochs=epochs, lr=lr, weight_decay=weight_decay,
                                         seed=seed)
-    ctx.set_dispatch_model(params)
+    if not use_split:
+        params = params.copy()
+        params[-1] = EXCLUDED_BIAS
+    # The model overrides the fixed tables only on the cells its training
+    # data covered.
+    ctx.set_dispatch_model(params, cells)
     pred = ctx.dispatch_tables("learned").reshape(-1)[cells].astype(np.int64) - 1
-    best = np.argmin(np.where(np.isnan(T), np.inf, T), axis=1)
+    best = np.argmin(np.where(np.isnan(T), np.inf, T), axis=1)  # among the trained strategies
     acc = float((w * (pred == best)).sum())
-    info = {"samples": int(len(cells)), "loss": loss, "weighted_accuracy": acc,
+    info = {"samples": int(len(cells)), "support": [int(c) for c in cells], "loss": loss,
+            "weighted_accuracy": acc,
+            "strategies": list(STRATEGIES if use_split else STRATEGIES[:3]),
             "objective": "log2 cycles per arc, weighted squared error", "epochs": epochs,
             "lr": lr, "weight_decay": weight_decay, "seed": seed, "min_arcs": min_arcs,
             "weight_power": weight_power}
@@ -124,8 +153,8 @@ def train(ctx, rec, *, epochs: int = 3000, lr: float = 0.02, weight_decay: float
 
 def save(path, params, meta: dict) -> None:
     doc = {"format": FORMAT_VERSION, "kind": "stc-dispatch-mlp",
-           "layout": "W1[16][6], b1[16], W2[3][16], b2[3]; outputs: log2 cycles per arc "
-                     "of merge, hash, search",
+           "layout": "W1[16][6], b1[16], W2[4][16], b2[4]; outputs: log2 cycles per arc "
+                     "of merge, hash, search, split",
            "params": [float(x) for x in np.asarray(params, np.float32)]}
     doc.update(meta)
     Path(path).write_text(json.dumps(doc, indent=1) + "\n")
@@ -175,6 +204,8 @@ def _main() -> None:
     ap.add_argument("--workload", type=int, default=3)
     ap.add_argument("--epochs", type=int, default=3000)
     ap.add_argument("--batch-graphs", type=int, default=4096)
+    ap.add_argument("--with-split", action="store_true",
+                    help="let the model choose the SPLIT strategy")
     ap.add_argument("--save-recording", default=None,
                     help="write the per-cell recordings to this .npz file")
     a = ap.parse_args()
@@ -194,10 +225,12 @@ def _main() -> None:
             np.savez(a.save_recording, names=np.array(names),
                      cycles=np.stack([r["cycles"] for r in recs]),
                      arcs=np.stack([r["arcs"] for r in recs]))
-        params, info = train(ctx, rec, epochs=a.epochs)
+        params, info = train(ctx, rec, epochs=a.epochs, use_split=a.with_split)
         meta = {"gpu": gpu, "trained_on": names, **info,
-                "train_regret_fixed": regret(rec, ctx.dispatch_tables("fixed"))["ratio"],
-                "train_regret_learned": regret(rec, ctx.dispatch_tables("learned"))["ratio"]}
+                "train_regret_fixed": regret(rec, ctx.dispatch_tables("fixed"),
+                                             info["strategies"])["ratio"],
+                "train_regret_learned": regret(rec, ctx.dispatch_tables("learned"),
+                                               info["strategies"])["ratio"]}
         save(a.out, params, meta)
         print(json.dumps(meta), flush=True)
     else:
@@ -208,8 +241,9 @@ def _main() -> None:
             np.savez(a.save_recording, names=np.array([f"workload{a.workload}"]),
                      cycles=rec["cycles"][None], arcs=rec["arcs"][None])
         out = {"gpu": gpu, "workload": a.workload, "model_trained_on": model.get("trained_on"),
-               "fixed": regret(rec, ctx.dispatch_tables("fixed")),
-               "learned": regret(rec, ctx.dispatch_tables("learned")),
+               "fixed": regret(rec, ctx.dispatch_tables("fixed"), model.get("strategies", STRATEGIES[:3])),
+               "learned": regret(rec, ctx.dispatch_tables("learned"), model.get("strategies", STRATEGIES[:3])),
+               "learned_vs_all_four": regret(rec, ctx.dispatch_tables("learned"), STRATEGIES),
                "counts": rec["counts"].as_tuple()}
         print(json.dumps(out), flush=True)
 

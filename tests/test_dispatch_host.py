@@ -25,8 +25,9 @@ def fake_recording(seed=0):
     rng = np.random.default_rng(seed)
     arcs = rng.integers(0, 200, _capi.DISPATCH_CELLS).astype(np.float64)
     arcs[rng.random(_capi.DISPATCH_CELLS) < 0.3] = 0
-    per_arc = rng.uniform(100, 1000, (3, _capi.DISPATCH_CELLS))
-    per_arc[1, 768:] = per_arc[0, 768:]  # giant: HASH runs as MERGE
+    per_arc = rng.uniform(100, 1000, (4, _capi.DISPATCH_CELLS))
+    per_arc[1, 768:] = per_arc[0, 768:]  # giant: HASH and SPLIT run as MERGE
+    per_arc[3, 768:] = per_arc[0, 768:]
     return {"cycles": per_arc * arcs, "arcs": arcs}
 
 
@@ -34,11 +35,11 @@ def test_samples_targets_and_weights():
     rec = fake_recording()
     X, T, w, cells = dispatcher.samples(rec, min_arcs=32)
     assert (rec["arcs"][cells] >= 32).all()
-    assert len(X) == len(T) == len(w) == len(cells) and T.shape[1] == 3
+    assert len(X) == len(T) == len(w) == len(cells) and T.shape[1] == 4
     cost = rec["cycles"][:, cells] / rec["arcs"][cells]
     giant = cells >= 768
     np.testing.assert_allclose(T[~giant], np.log2(cost[:, ~giant]).T, rtol=1e-6)
-    assert np.isnan(T[giant, 1]).all() and not np.isnan(T[giant][:, [0, 2]]).any()
+    assert np.isnan(T[giant][:, [1, 3]]).all() and not np.isnan(T[giant][:, [0, 2]]).any()
     np.testing.assert_allclose(w, np.sqrt(rec["arcs"][cells]) / np.sqrt(rec["arcs"][cells]).sum(),
                                rtol=1e-5)
     np.testing.assert_array_equal(X, stc.dispatch_features()[cells])
@@ -48,17 +49,21 @@ def test_regret_of_best_and_worst_tables():
     rec = fake_recording(1)
     cost = rec["cycles"] / np.maximum(rec["arcs"], 1)
     cost[1, 768:] = np.inf
+    cost[3, 768:] = np.inf
     best = np.argmin(cost, axis=0) + 1
-    assert dispatcher.regret(rec, best)["ratio"] == pytest.approx(1.0)
+    assert dispatcher.regret(rec, best, dispatcher.STRATEGIES)["ratio"] == pytest.approx(1.0)
+    # Judged against three strategies, a table that uses SPLIT may beat 1.0.
+    assert dispatcher.regret(rec, best)["ratio"] <= 1.0 + 1e-12
     worst = np.argmax(np.where(np.isfinite(cost), cost, -np.inf), axis=0) + 1
-    assert dispatcher.regret(rec, worst)["ratio"] > 1.2
-    # A table that says HASH in the giant class is charged the MERGE cost.
-    t = best.copy()
-    t[768:] = 2
-    r = dispatcher.regret(rec, t)
+    assert dispatcher.regret(rec, worst, dispatcher.STRATEGIES)["ratio"] > 1.2
+    # A table that says HASH or SPLIT in the giant class is charged the
+    # MERGE cost.
     t2 = best.copy()
     t2[768:] = 1
-    assert r["cycles"] == pytest.approx(dispatcher.regret(rec, t2)["cycles"])
+    for code in (2, 4):
+        t = best.copy()
+        t[768:] = code
+        assert dispatcher.regret(rec, t)["cycles"] == pytest.approx(dispatcher.regret(rec, t2)["cycles"])
 
 
 def test_model_file_round_trip(tmp_path):
@@ -79,7 +84,7 @@ def test_shipped_model_file_is_valid():
     m = dispatcher.load()
     assert m["params"].shape == (_capi.DISPATCH_MODEL_PARAMS,)
     assert np.isfinite(m["params"]).all()
-    assert m["trained_on"] and m["samples"] > 0
+    assert m["trained_on"] and m["samples"] > 0 and len(m["support"]) == m["samples"]
     assert m["train_regret_learned"] < m["train_regret_fixed"]
 
 
