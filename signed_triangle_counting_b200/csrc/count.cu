@@ -39,6 +39,7 @@
 #include <algorithm>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 
 #include "internal.h"
 #include "radix_sort.cuh"
@@ -388,7 +389,9 @@ __device__ __forceinline__ void process_chunk(const StageMem& m, uint32_t d, con
 // 4-byte load), a 4-bit mask of the ids inside the arc, then for HASH one
 // 8-byte bucket read per id answers membership and the A' sign together;
 // MERGE chunks are merged against the sorted A' instead.
-template <int U>
+// kSplit: compiled with the SPLIT path (a split index per arc, a per-chunk
+// choice of source); kernels without it stay as lean as before SPLIT.
+template <int U, bool kSplit>
 __device__ __forceinline__ void stream_pass(const Csr& g, const StageMem& m, uint32_t d,
                                             uint32_t warp, uint32_t warps, uint32_t lane,
                                             const Geo& geo, PackedCounts& pc, TypeCounts& tc) {
@@ -408,7 +411,7 @@ __device__ __forceinline__ void stream_pass(const Csr& g, const StageMem& m, uin
     k = lo_k;
   }
   uint32_t pk = m.pre[k], pk1 = m.pre[k + 1], alo = m.lo[k], ahi = m.hi[k];
-  uint32_t ast = m.st[k], anuv = m.s[k] < 0, asp = m.sp[k];
+  uint32_t ast = m.st[k], anuv = m.s[k] < 0, asp = kSplit ? m.sp[k] : 0u;
   uint32_t rounds = 0;
   for (uint32_t base = c_begin; base < c_end; base += 32 * U) {
     uint4 q[U];
@@ -428,10 +431,10 @@ __device__ __forceinline__ void stream_pass(const Csr& g, const StageMem& m, uin
           ahi = m.hi[k];
           ast = m.st[k];
           anuv = m.s[k] < 0;
-          asp = m.sp[k];
+          if (kSplit) asp = m.sp[k];
         }
         const uint32_t ci = (alo >> 2) + (c - pk);
-        load_chunk(g, ci, ast, asp, q[u], sw[u]);
+        load_chunk(g, ci, kSplit ? ast : (uint32_t)STC_STRATEGY_HASH, asp, q[u], sw[u]);
         vm[u] = chunk_mask(ci, alo, ahi);
         sk[u] = k;
         snuv[u] = anuv;
@@ -744,7 +747,7 @@ constexpr size_t kWarpStageBytes = (StageMem::bytes(kWarpCap, kWarpBuckets) + 15
 
 // One warp-class list, staged in the warp's shared-memory slice `m` with
 // up to hf hash buckets per element; U int4 chunks in flight per lane.
-template <class Sink, bool kTime, int U>
+template <class Sink, bool kTime, int U, bool kSplit>
 __device__ __forceinline__ void warp_vertex(const Csr& g, uint32_t u, uint32_t lane,
                                             const StageMem& m, const uint8_t (*table)[16],
                                             uint32_t hf, unsigned long long* __restrict__ ctr,
@@ -765,7 +768,7 @@ __device__ __forceinline__ void warp_vertex(const Csr& g, uint32_t u, uint32_t l
     timed_pass(g, m, d, 0, 1, lane, geo, pc, out, at, kTableWarp);
   } else {
     warp_chunk_scan(m, d, lane);
-    stream_pass<U>(g, m, d, 0, 1, lane, geo, pc, out);
+    stream_pass<U, kSplit>(g, m, d, 0, 1, lane, geo, pc, out);
     search_pass(g, m, d, 0, 1, lane, pc, out);
   }
   pc.drain(out);
@@ -773,7 +776,7 @@ __device__ __forceinline__ void warp_vertex(const Csr& g, uint32_t u, uint32_t l
   __syncwarp();
 }
 
-template <class Sink, bool kTime, int U>
+template <class Sink, bool kTime, int U, bool kSplit>
 __global__ void __launch_bounds__(256) k_warp(Csr g, const uint32_t* __restrict__ list, uint32_t cnt,
                                               unsigned long long* __restrict__ ctr, Sink sink,
                                               const uint8_t* __restrict__ gtable, ArcTimes at,
@@ -789,7 +792,7 @@ __global__ void __launch_bounds__(256) k_warp(Csr g, const uint32_t* __restrict_
   TypeCounts tc;
   const uint32_t warps = gridDim.x * kWarps;
   for (uint32_t idx = blockIdx.x * kWarps + w; idx < cnt; idx += warps)
-    warp_vertex<Sink, kTime, U>(g, list[idx], lane, m, table, hf, ctr, sink, at, tc);
+    warp_vertex<Sink, kTime, U, kSplit>(g, list[idx], lane, m, table, hf, ctr, sink, at, tc);
   if (!kVC) flush_counts<256>(tc, ctr);
 }
 
@@ -801,7 +804,7 @@ constexpr size_t kMaxStageSmem = 220 * 1024;  // dynamic shared memory a staged 
 
 // One block-class list (the whole CTA), staged in `m` of capacity `cap`
 // with `nb` hash buckets.
-template <int THREADS, class Sink, bool kTime, int U>
+template <int THREADS, class Sink, bool kTime, int U, bool kSplit>
 __device__ __forceinline__ void block_vertex(const Csr& g, uint32_t u, uint32_t cap, uint32_t nb,
                                              uint32_t hf, const StageMem& m,
                                              const uint8_t (*table)[16],
@@ -826,14 +829,14 @@ __device__ __forceinline__ void block_vertex(const Csr& g, uint32_t u, uint32_t 
     timed_pass(g, m, d, w, kWarps, lane, geo, pc, out, at, tclass);
   } else {
     block_chunk_scan<THREADS>(m, d, scan_tmp);
-    stream_pass<U>(g, m, d, w, kWarps, lane, geo, pc, out);
+    stream_pass<U, kSplit>(g, m, d, w, kWarps, lane, geo, pc, out);
     search_pass(g, m, d, w, kWarps, lane, pc, out);
   }
   pc.drain(out);
   if (kVC) block_vertex_flush<THREADS>(vc, u, sink);
 }
 
-template <int THREADS, class Sink, bool kTime, int U>
+template <int THREADS, class Sink, bool kTime, int U, bool kSplit>
 __global__ void __launch_bounds__(THREADS) k_block(Csr g, const uint32_t* __restrict__ list,
                                                    uint32_t cnt, uint32_t cap, uint32_t nb, uint32_t hf,
                                                    unsigned long long* __restrict__ queue,
@@ -859,8 +862,8 @@ __global__ void __launch_bounds__(THREADS) k_block(Csr g, const uint32_t* __rest
     __syncthreads();
     const uint32_t item = s_item;
     if (item >= cnt) break;
-    block_vertex<THREADS, Sink, kTime, U>(g, list[item], cap, nb, hf, m, table, scan_tmp, ctr,
-                                          sink, at, tclass, tc);
+    block_vertex<THREADS, Sink, kTime, U, kSplit>(g, list[item], cap, nb, hf, m, table, scan_tmp,
+                                                  ctr, sink, at, tclass, tc);
   }
   if (!kVC) flush_counts<THREADS>(tc, ctr);
 }
@@ -932,6 +935,10 @@ template <class F> void with_unroll(uint32_t u, F&& f) {
   else if (u == 4) f(Int<4>{});
   else f(Int<2>{});
 }
+template <class F> void with_split(bool split, F&& f) {
+  if (split) f(std::true_type{});
+  else f(std::false_type{});
+}
 template <class F> void with_block_threads(uint32_t t, F&& f) {
   if (t == 128) f(Int<128>{});
   else if (t == 512) f(Int<512>{});
@@ -963,11 +970,13 @@ void launch_classes(cudaStream_t st, const Csr& csr, const uint32_t* lists, cons
   if (counts[1] && (mask & 2u)) {
     const uint32_t grid = std::min<uint32_t>((counts[1] + 7) / 8, kSMs * 8);
     const uint32_t u = kTime ? kStreamUnroll : tu.unroll[0];
-    with_unroll(u, [&](auto U) {
-      if constexpr (!kTime || decltype(U)::value == kStreamUnroll)
-        k_warp<Sink, kTime, decltype(U)::value><<<grid, 256, 0, st>>>(
-            csr, lists + starts[1], counts[1], ctr, sink, d_tables + 256 * kTableWarp, at,
-            tu.hash_factor[0]);
+    with_split(!kTime && csr.nbr_split != nullptr, [&](auto S) {
+      with_unroll(u, [&](auto U) {
+        if constexpr (!kTime || (decltype(U)::value == kStreamUnroll && !decltype(S)::value))
+          k_warp<Sink, kTime, decltype(U)::value, decltype(S)::value><<<grid, 256, 0, st>>>(
+              csr, lists + starts[1], counts[1], ctr, sink, d_tables + 256 * kTableWarp, at,
+              tu.hash_factor[0]);
+      });
     });
     launches++;
   }
@@ -978,17 +987,20 @@ void launch_classes(cudaStream_t st, const Csr& csr, const uint32_t* lists, cons
     const size_t smem = block_stage_bytes(cap, nb);
     const uint32_t threads = kTime ? 256 : tu.block_threads;
     const uint32_t u = kTime ? kStreamUnroll : tu.unroll[1];
-    with_block_threads(threads, [&](auto T) {
-      with_unroll(u, [&](auto U) {
-        constexpr int kT = decltype(T)::value, kU = decltype(U)::value;
-        if constexpr (!kTime || (kT == 256 && kU == kStreamUnroll)) {
-          STC_CUDA(cudaFuncSetAttribute(k_block<kT, Sink, kTime, kU>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-          const uint32_t grid = std::min<uint32_t>(counts[2], kSMs * 8);
-          k_block<kT, Sink, kTime, kU><<<grid, kT, smem, st>>>(
-              csr, lists + starts[2], counts[2], cap, nb, hf, ctr + C_WORK + 0, ctr, sink,
-              d_tables + 256 * kTableBlock, at, kTableBlock, nullptr, 0);
-        }
+    with_split(!kTime && csr.nbr_split != nullptr, [&](auto S) {
+      with_block_threads(threads, [&](auto T) {
+        with_unroll(u, [&](auto U) {
+          constexpr int kT = decltype(T)::value, kU = decltype(U)::value;
+          constexpr bool kS = decltype(S)::value;
+          if constexpr (!kTime || (kT == 256 && kU == kStreamUnroll && !kS)) {
+            STC_CUDA(cudaFuncSetAttribute(k_block<kT, Sink, kTime, kU, kS>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            const uint32_t grid = std::min<uint32_t>(counts[2], kSMs * 8);
+            k_block<kT, Sink, kTime, kU, kS><<<grid, kT, smem, st>>>(
+                csr, lists + starts[2], counts[2], cap, nb, hf, ctr + C_WORK + 0, ctr, sink,
+                d_tables + 256 * kTableBlock, at, kTableBlock, nullptr, 0);
+          }
+        });
       });
     });
     launches++;
@@ -1001,16 +1013,19 @@ void launch_classes(cudaStream_t st, const Csr& csr, const uint32_t* lists, cons
     const uint32_t nb = hf * cap;
     const size_t smem = block_stage_bytes(cap, nb);
     const uint32_t u = kTime ? kStreamUnroll : tu.unroll[2];
-    with_unroll(u, [&](auto U) {
-      constexpr int kU = decltype(U)::value;
-      if constexpr (!kTime || kU == kStreamUnroll) {
-        STC_CUDA(cudaFuncSetAttribute(k_block<512, Sink, kTime, kU>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        const uint32_t grid = std::min<uint32_t>(counts[3], kSMs * 2);
-        k_block<512, Sink, kTime, kU><<<grid, 512, smem, st>>>(
-            csr, lists + starts[3], counts[3], cap, nb, hf, ctr + C_WORK + 1, ctr, sink,
-            d_tables + 256 * kTableLarge, at, kTableLarge, nullptr, 0);
-      }
+    with_split(!kTime && csr.nbr_split != nullptr, [&](auto S) {
+      with_unroll(u, [&](auto U) {
+        constexpr int kU = decltype(U)::value;
+        constexpr bool kS = decltype(S)::value;
+        if constexpr (!kTime || (kU == kStreamUnroll && !kS)) {
+          STC_CUDA(cudaFuncSetAttribute(k_block<512, Sink, kTime, kU, kS>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+          const uint32_t grid = std::min<uint32_t>(counts[3], kSMs * 2);
+          k_block<512, Sink, kTime, kU, kS><<<grid, 512, smem, st>>>(
+              csr, lists + starts[3], counts[3], cap, nb, hf, ctr + C_WORK + 1, ctr, sink,
+              d_tables + 256 * kTableLarge, at, kTableLarge, nullptr, 0);
+        }
+      });
     });
     launches++;
   }
@@ -1073,7 +1088,7 @@ __global__ void __launch_bounds__(256, 4) k_persistent(Csr g, const uint32_t* __
     __syncthreads();
     const uint32_t item = s_item;
     if (item >= nb) break;
-    block_vertex<256, Sink, false, kStreamUnroll>(g, lists[plan[2] + item], kBlockCap,
+    block_vertex<256, Sink, false, kStreamUnroll, false>(g, lists[plan[2] + item], kBlockCap,
                                                   4 * kBlockCap, 4, mb, tb, scan_tmp, ctr, sink,
                                                   ArcTimes{nullptr, nullptr}, kTableBlock, tc);
   }
@@ -1087,7 +1102,8 @@ __global__ void __launch_bounds__(256, 4) k_persistent(Csr g, const uint32_t* __
     item = __shfl_sync(kFull, item, 0);
     if (item >= total) break;
     if (item < nw) {
-      warp_vertex<Sink, false, kStreamUnroll>(g, lists[plan[1] + item], lane, mw, tw, 4, ctr, sink,
+      warp_vertex<Sink, false, kStreamUnroll, false>(g, lists[plan[1] + item], lane, mw, tw, 4, ctr,
+                                                     sink,
                                               ArcTimes{nullptr, nullptr}, tc);
     } else {
       const uint32_t idx = (item - nw) * 32 + lane;
@@ -1109,8 +1125,8 @@ void enqueue_persistent(cudaStream_t st, const Csr& csr, const ClassBounds& cb, 
   k_classify_fill<<<kSMs * 4, 256, 0, st>>>(csr.off, csr.n, cb, lists, plan, ctr + C_WORK, nullptr);
   k_persistent<Sink><<<kSMs * 4, 256, kPersistentSmem, st>>>(csr, lists, plan, ctr, sink,
                                                              d_tables);
-  k_block<512, Sink, false, kStreamUnroll><<<kSMs, 512, StageMem::bytes(kLargeCap, 2 * kLargeCap),
-                                            st>>>(
+  k_block<512, Sink, false, kStreamUnroll, false>
+      <<<kSMs, 512, StageMem::bytes(kLargeCap, 2 * kLargeCap), st>>>(
       csr, lists, 0, kLargeCap, 2 * kLargeCap, 2, ctr + C_WORK + 6, ctr, sink,
       d_tables + 256 * kTableLarge, none, kTableLarge, plan, 3);
   k_giant<512, Sink, false><<<kSMs * 2, 512, 0, st>>>(csr, lists, 0, ctr + C_WORK + 7, ctr, sink,
@@ -1133,7 +1149,7 @@ void count_persistent(stc_ctx* c, const Csr& csr, const ClassBounds& cb, uint32_
   cudaStream_t st = c->stream;
   STC_CUDA(cudaFuncSetAttribute(k_persistent<Sink>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)kPersistentSmem));
-  STC_CUDA(cudaFuncSetAttribute(k_block<512, Sink, false, kStreamUnroll>,
+  STC_CUDA(cudaFuncSetAttribute(k_block<512, Sink, false, kStreamUnroll, false>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)StageMem::bytes(kLargeCap, 2 * kLargeCap)));
   c->launches += 6;
@@ -1364,7 +1380,9 @@ void count_triangles(stc_ctx* c, const DeviceGraph& gin, const CountConfig& cfg)
       !timed && (cfg.strategy == STC_STRATEGY_AUTO || cfg.strategy == STC_STRATEGY_SEARCH);
   const ClassBounds cb{tiny ? kTinyMax : 1u, kWarpCap, kBlockCap, kLargeCap};
 
-  if (cfg.persistent && !timed && cfg.shards <= 1) {
+  // The persistent engine has no SPLIT path: counts that use SPLIT take the
+  // per-class kernels.
+  if (cfg.persistent && !timed && cfg.shards <= 1 && !split) {
     uint32_t* lists = buffer<uint32_t>(c, B_WORK, (size_t)g.n + kPlanWords + 8);
     uint32_t* plan = lists + g.n + 4;
     if (cfg.vertex_counts) {
