@@ -301,3 +301,21 @@ def test_batch_workload_full(ctx, golden):
     assert [int(x) for x in np.diff(offs)] == b["m_input"]
     got = ctx.count_batch_packed(src, dst, sign, offs)
     assert [list(c.as_tuple()) for c in got] == b["t"]
+
+
+def test_complete_graph_closed_form(ctx):
+    # A dense core too large for the oracle: K_8400 (35 M edges, forward
+    # lists up to 8399 arcs, all in the giant class).  Signs are products of
+    # vertex labels (a positive, b negative vertices), so every triangle is
+    # balanced and the counts have closed forms: T3 = C(a,3) + C(b,3),
+    # T1 = C(a,2) b + a C(b,2), T0 = T2 = 0.
+    from math import comb
+    k = 8400
+    rng = np.random.default_rng(5)
+    label = np.where(rng.random(k) < 0.6, 1, -1).astype(np.int8)
+    a, b = np.triu_indices(k, 1)
+    sign = (label[a] * label[b]).astype(np.int8)
+    perm = rng.permutation(k).astype(np.uint32)
+    na, nb = int((label > 0).sum()), int((label < 0).sum())
+    want = (0, comb(na, 2) * nb + na * comb(nb, 2), 0, comb(na, 3) + comb(nb, 3))
+    assert ctx.count(perm[a], perm[b], sign).as_tuple() == want
