@@ -171,7 +171,12 @@ __device__ __forceinline__ void arc_merge_global(const uint32_t* a, const int8_t
 // Strategy codes in the per-arc table: STC_STRATEGY_MERGE / _HASH / _SEARCH,
 // or kNoArc for the last arc of a list (empty A') and arcs with empty B.
 constexpr uint8_t kNoArc = 0xFF;
-constexpr uint32_t kIdMask = 0x7FFFFFFFu;  // hash keys: id | negative << 31
+// Hash keys are id << 1 | (the A' edge is negative).  Ids stay below
+// 2^31 - 2, so a key is at most 0xFFFFFFFB: it never equals kEmpty, and no
+// key matches kNoId, the id that pads the entries of a chunk outside its arc.
+// A query x matches key w exactly when w - 2x is 0 or 1, and that difference
+// is the A' sign.
+constexpr uint32_t kNoId = 0x7FFFFFFEu;
 
 // Shared-memory image of one staged list of capacity `cap` with `nb` hash
 // buckets: the hash (two 32-bit keys per 8-byte bucket), the sorted ids,
@@ -251,7 +256,7 @@ __device__ __forceinline__ void stage(const Csr& g, uint64_t ub, uint32_t d, uin
   sync();
   for (uint32_t i = t; i < d; i += TS) {
     const uint32_t x = m.a[i];
-    const uint32_t key = x | ((uint32_t)(m.s[i] < 0) << 31);
+    const uint32_t key = (x << 1) | (uint32_t)(m.s[i] < 0);
     uint32_t b = hash_slot(x, geo.shift);
     while (atomicCAS(&m.hk[2 * b], kEmpty, key) != kEmpty &&
            atomicCAS(&m.hk[2 * b + 1], kEmpty, key) != kEmpty)
@@ -264,13 +269,17 @@ __device__ __forceinline__ void stage(const Csr& g, uint64_t ub, uint32_t d, uin
   sync();
 }
 
-// Exact lookup continuing from bucket b (after a full bucket without a
-// match): 0 if x is not in the hash, else 1 | (the key's sign flag << 1).
-__device__ __noinline__ uint32_t probe_rest(const uint32_t* hk, uint32_t nb, uint32_t b, uint32_t x) {
+// Exact lookup of x from its home bucket on: 0 if x is not in the hash,
+// else 1 | (the key's sign flag << 1).
+__device__ __noinline__ uint32_t probe_rest(const uint32_t* hk, uint32_t nb, uint32_t shift,
+                                            uint32_t x) {
+  const uint32_t q = x << 1;
+  uint32_t b = hash_slot(x, shift);
   while (true) {
     const uint2 w = *reinterpret_cast<const uint2*>(hk + 2 * b);
-    if ((w.x & kIdMask) == x) return 1u | ((w.x >> 31) << 1);
-    if ((w.y & kIdMask) == x) return 1u | ((w.y >> 31) << 1);
+    const uint32_t d0 = w.x - q, d1 = w.y - q;
+    if (d0 < 2) return 1u | (d0 << 1);
+    if (d1 < 2) return 1u | (d1 << 1);
     if (w.y == kEmpty) return 0;
     b = (b + 1) & (nb - 1);
   }
@@ -346,27 +355,41 @@ __device__ __forceinline__ void load_chunk(const Csr& g, uint32_t ci, uint32_t s
 // One int4 chunk of B for arc k of a staged list: four ids q, their four sign
 // bytes sw, and the mask vm (non-zero) of the ids inside the arc.  HASH looks
 // every id up in the staged hash (one 8-byte bucket read gives membership and
-// the A' sign); MERGE locates the chunk in the sorted A' = a[k+1 ..) by one
-// binary search and merges its ascending ids forward.
+// the A' sign): ids outside the arc are replaced by kNoId, which matches no
+// key, and the rare id whose home bucket is full without a match is looked up
+// again past it, once per chunk.  MERGE locates the chunk in the sorted
+// A' = a[k+1 ..) by one binary search and merges its ascending ids forward.
 __device__ __forceinline__ void process_chunk(const StageMem& m, uint32_t d, const Geo& geo,
                                               const uint4& q, uint32_t sw, uint32_t vm, uint32_t k,
                                               uint32_t nuv, uint32_t st, PackedCounts& pc) {
   if (st == STC_STRATEGY_HASH || st == STC_STRATEGY_SPLIT) {
+    uint4 x4 = q;
+    if (vm != 0xFu) {
+      x4.x = (vm & 1u) ? x4.x : kNoId;
+      x4.y = (vm & 2u) ? x4.y : kNoId;
+      x4.z = (vm & 4u) ? x4.z : kNoId;
+      x4.w = (vm & 8u) ? x4.w : kNoId;
+    }
+    bool again = false;
 #pragma unroll
     for (uint32_t e = 0; e < 4; e++) {
-      const uint32_t x = pick4(q, e);
-      const uint32_t b = hash_slot(x, geo.shift);
-      const uint2 w = *reinterpret_cast<const uint2*>(m.hk + 2 * b);
-      const bool m0 = (w.x & kIdMask) == x, m1 = (w.y & kIdMask) == x;
-      uint32_t hit = (m0 | m1) & (vm >> e) & 1u;
-      uint32_t na = (m0 ? w.x : w.y) >> 31;
-      if (!(m0 | m1) && w.y != kEmpty && ((vm >> e) & 1u)) {
-        const uint32_t r = probe_rest(m.hk, geo.nb, (b + 1) & (geo.nb - 1), x);
-        hit = r & 1u;
-        na = r >> 1;
+      const uint32_t x = pick4(x4, e);
+      const uint2 w = *reinterpret_cast<const uint2*>(m.hk + 2 * hash_slot(x, geo.shift));
+      const uint32_t d0 = w.x - 2 * x, d1 = w.y - 2 * x;
+      if (d0 < 2 || d1 < 2)
+        pc.add(nuv + (d0 < 2 ? d0 : d1) + ((sw >> (8 * e + 7)) & 1u));
+      else
+        again |= w.y != kEmpty;
+    }
+    if (again) {
+#pragma unroll 1
+      for (uint32_t e = 0; e < 4; e++) {
+        const uint32_t x = pick4(x4, e);
+        const uint2 w = *reinterpret_cast<const uint2*>(m.hk + 2 * hash_slot(x, geo.shift));
+        if (w.x - 2 * x < 2 || w.y - 2 * x < 2 || w.y == kEmpty) continue;  // settled above
+        const uint32_t r = probe_rest(m.hk, geo.nb, geo.shift, x);
+        if (r) pc.add(nuv + (r >> 1) + ((sw >> (8 * e + 7)) & 1u));
       }
-      const uint32_t nb = (sw >> (8 * e + 7)) & 1u;
-      if (hit) pc.add(nuv + na + nb);
     }
   } else {  // MERGE
     const uint32_t a0 = k + 1, alen = d - a0;
@@ -777,7 +800,7 @@ __device__ __forceinline__ void warp_vertex(const Csr& g, uint32_t u, uint32_t l
 }
 
 template <class Sink, bool kTime, int U, bool kSplit>
-__global__ void __launch_bounds__(256) k_warp(Csr g, const uint32_t* __restrict__ list, uint32_t cnt,
+__global__ void __launch_bounds__(256, U >= 4 ? 3 : 4) k_warp(Csr g, const uint32_t* __restrict__ list, uint32_t cnt,
                                               unsigned long long* __restrict__ ctr, Sink sink,
                                               const uint8_t* __restrict__ gtable, ArcTimes at,
                                               uint32_t hf) {
