@@ -96,6 +96,21 @@ struct PackedCounts {
   }
 };
 
+// Four 8-bit counters packed in one 32-bit word, for the streamed chunks:
+// one 32-bit shift and add per triangle; widened into TypeCounts before any
+// field can reach 2^8.
+struct PackedCounts8 {
+  uint32_t w = 0;
+  __device__ __forceinline__ void add(uint32_t neg) { w += 1u << (8 * neg); }
+  __device__ __forceinline__ void drain(TypeCounts& tc) {
+    tc.c[0] += w & 0xFFu;
+    tc.c[1] += (w >> 8) & 0xFFu;
+    tc.c[2] += (w >> 16) & 0xFFu;
+    tc.c[3] += w >> 24;
+    w = 0;
+  }
+};
+
 __device__ __forceinline__ uint32_t size_bucket(uint32_t x) { return min(15u, 32u - __clz(x)); }
 
 // First index i in [0, len) with a[i] >= x (len if none); `a` may point to
@@ -359,10 +374,12 @@ __device__ __forceinline__ void load_chunk(const Csr& g, uint32_t ci, uint32_t s
 // key, and the rare id whose home bucket is full without a match is looked up
 // again past it, once per chunk.  MERGE locates the chunk in the sorted
 // A' = a[k+1 ..) by one binary search and merges its ascending ids forward.
+// At most four adds per chunk reach any one field of `pc`.
+template <class PC>
 __device__ __forceinline__ void process_chunk(const StageMem& m, uint32_t d, const Geo& geo,
                                               const uint4& q, uint32_t sw, uint32_t vm, uint32_t k,
-                                              uint32_t nuv, uint32_t st, PackedCounts& pc) {
-  if (st == STC_STRATEGY_HASH || st == STC_STRATEGY_SPLIT) {
+                                              uint32_t nuv, uint32_t st, PC& pc) {
+  if (st != STC_STRATEGY_MERGE) {  // HASH or SPLIT
     uint4 x4 = q;
     if (vm != 0xFu) {
       x4.x = (vm & 1u) ? x4.x : kNoId;
@@ -417,7 +434,7 @@ __device__ __forceinline__ void process_chunk(const StageMem& m, uint32_t d, con
 template <int U, bool kSplit>
 __device__ __forceinline__ void stream_pass(const Csr& g, const StageMem& m, uint32_t d,
                                             uint32_t warp, uint32_t warps, uint32_t lane,
-                                            const Geo& geo, PackedCounts& pc, TypeCounts& tc) {
+                                            const Geo& geo, TypeCounts& tc) {
   const uint32_t total = m.pre[d];
   const uint32_t per = (total + warps - 1) / warps;
   const uint32_t c_begin = min(total, warp * per), c_end = min(total, c_begin + per);
@@ -433,8 +450,24 @@ __device__ __forceinline__ void stream_pass(const Csr& g, const StageMem& m, uin
     }
     k = lo_k;
   }
-  uint32_t pk = m.pre[k], pk1 = m.pre[k + 1], alo = m.lo[k], ahi = m.hi[k];
-  uint32_t ast = m.st[k], anuv = m.s[k] < 0, asp = kSplit ? m.sp[k] : 0u;
+  // Per arc: chunk index = cb + flattened index; the masks of its first and
+  // last chunk (every chunk between is whole).
+  uint32_t pk, pk1, cb, mf, ml, ast, anuv, asp = 0;
+  auto enter = [&](uint32_t kk) {
+    pk = m.pre[kk];
+    pk1 = m.pre[kk + 1];
+    const uint32_t alo = m.lo[kk], ahi = m.hi[kk];
+    cb = (alo >> 2) - pk;
+    mf = (0xFu << (alo & 3u)) & 0xFu;
+    ml = 0xFu >> (3u - ((ahi - 1u) & 3u));
+    ast = m.st[kk];
+    anuv = m.s[kk] < 0;
+    if (kSplit) asp = m.sp[kk];
+  };
+  enter(k);
+  // 8-bit fields: at most 4 U adds per field per round.
+  constexpr uint32_t kDrainRounds = 255 / (4 * U);
+  PackedCounts8 p8;
   uint32_t rounds = 0;
   for (uint32_t base = c_begin; base < c_end; base += 32 * U) {
     uint4 q[U];
@@ -448,17 +481,11 @@ __device__ __forceinline__ void stream_pass(const Csr& g, const StageMem& m, uin
           do {
             k++;
           } while (m.pre[k + 1] <= c);
-          pk = m.pre[k];
-          pk1 = m.pre[k + 1];
-          alo = m.lo[k];
-          ahi = m.hi[k];
-          ast = m.st[k];
-          anuv = m.s[k] < 0;
-          if (kSplit) asp = m.sp[k];
+          enter(k);
         }
-        const uint32_t ci = (alo >> 2) + (c - pk);
+        const uint32_t ci = cb + c;
         load_chunk(g, ci, kSplit ? ast : (uint32_t)STC_STRATEGY_HASH, asp, q[u], sw[u]);
-        vm[u] = chunk_mask(ci, alo, ahi);
+        vm[u] = (c == pk ? mf : 0xFu) & (c + 1 == pk1 ? ml : 0xFu);
         sk[u] = k;
         snuv[u] = anuv;
         sst[u] = ast;
@@ -466,12 +493,13 @@ __device__ __forceinline__ void stream_pass(const Csr& g, const StageMem& m, uin
     }
 #pragma unroll
     for (int u = 0; u < U; u++)
-      if (vm[u]) process_chunk(m, d, geo, q[u], sw[u], vm[u], sk[u], snuv[u], sst[u], pc);
-    if (++rounds == 8000) {  // at most 4 * U adds per field per round
-      pc.drain(tc);
+      if (vm[u]) process_chunk(m, d, geo, q[u], sw[u], vm[u], sk[u], snuv[u], sst[u], p8);
+    if (++rounds == kDrainRounds) {
+      p8.drain(tc);
       rounds = 0;
     }
   }
+  p8.drain(tc);
 }
 
 // SEARCH arcs of a staged list, one arc per warp.
@@ -791,7 +819,7 @@ __device__ __forceinline__ void warp_vertex(const Csr& g, uint32_t u, uint32_t l
     timed_pass(g, m, d, 0, 1, lane, geo, pc, out, at, kTableWarp);
   } else {
     warp_chunk_scan(m, d, lane);
-    stream_pass<U, kSplit>(g, m, d, 0, 1, lane, geo, pc, out);
+    stream_pass<U, kSplit>(g, m, d, 0, 1, lane, geo, out);
     search_pass(g, m, d, 0, 1, lane, pc, out);
   }
   pc.drain(out);
@@ -852,7 +880,7 @@ __device__ __forceinline__ void block_vertex(const Csr& g, uint32_t u, uint32_t 
     timed_pass(g, m, d, w, kWarps, lane, geo, pc, out, at, tclass);
   } else {
     block_chunk_scan<THREADS>(m, d, scan_tmp);
-    stream_pass<U, kSplit>(g, m, d, w, kWarps, lane, geo, pc, out);
+    stream_pass<U, kSplit>(g, m, d, w, kWarps, lane, geo, out);
     search_pass(g, m, d, w, kWarps, lane, pc, out);
   }
   pc.drain(out);
