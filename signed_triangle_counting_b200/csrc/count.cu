@@ -87,6 +87,9 @@ struct TypeCounts {
 struct PackedCounts {
   unsigned long long w = 0;
   __device__ __forceinline__ void add(uint32_t neg) { w += 1ull << (16 * neg); }
+  __device__ __forceinline__ void add_if(bool hit, uint32_t neg) {
+    w += (unsigned long long)hit << (16 * neg);
+  }
   __device__ __forceinline__ void drain(TypeCounts& tc) {
     tc.c[0] += w & 0xFFFF;
     tc.c[1] += (w >> 16) & 0xFFFF;
@@ -102,6 +105,8 @@ struct PackedCounts {
 struct PackedCounts8 {
   uint32_t w = 0;
   __device__ __forceinline__ void add(uint32_t neg) { w += 1u << (8 * neg); }
+  // Branch-free: adds nothing unless `hit`; neg <= 3 either way.
+  __device__ __forceinline__ void add_if(bool hit, uint32_t neg) { w += (uint32_t)hit << (8 * neg); }
   __device__ __forceinline__ void drain(TypeCounts& tc) {
     tc.c[0] += w & 0xFFu;
     tc.c[1] += (w >> 8) & 0xFFu;
@@ -374,7 +379,10 @@ __device__ __forceinline__ void load_chunk(const Csr& g, uint32_t ci, uint32_t s
 // key, and the rare id whose home bucket is full without a match is looked up
 // again past it, once per chunk.  MERGE locates the chunk in the sorted
 // A' = a[k+1 ..) by one binary search and merges its ascending ids forward.
-// At most four adds per chunk reach any one field of `pc`.
+// At most four adds per chunk reach any one field of `pc`.  The HASH
+// lookups are branch-free: with a few percent of ids hitting, some lane of a
+// warp hits at almost every step, so a branch per hit would diverge at
+// almost every step.
 template <class PC>
 __device__ __forceinline__ void process_chunk(const StageMem& m, uint32_t d, const Geo& geo,
                                               const uint4& q, uint32_t sw, uint32_t vm, uint32_t k,
@@ -393,10 +401,9 @@ __device__ __forceinline__ void process_chunk(const StageMem& m, uint32_t d, con
       const uint32_t x = pick4(x4, e);
       const uint2 w = *reinterpret_cast<const uint2*>(m.hk + 2 * hash_slot(x, geo.shift));
       const uint32_t d0 = w.x - 2 * x, d1 = w.y - 2 * x;
-      if (d0 < 2 || d1 < 2)
-        pc.add(nuv + (d0 < 2 ? d0 : d1) + ((sw >> (8 * e + 7)) & 1u));
-      else
-        again |= w.y != kEmpty;
+      const bool hit = d0 < 2 || d1 < 2;
+      again |= !hit && w.y != kEmpty;
+      pc.add_if(hit, nuv + (d0 < 2 ? d0 : d1 & 1u) + ((sw >> (8 * e + 7)) & 1u));
     }
     if (again) {
 #pragma unroll 1
