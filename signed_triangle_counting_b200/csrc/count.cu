@@ -429,9 +429,14 @@ __device__ __forceinline__ void process_chunk(const StageMem& m, uint32_t d, con
 }
 
 // The streamed arcs of a staged list as one sequence of aligned int4
-// chunks.  Warp w takes a contiguous share of the sequence and its lanes
-// take consecutive chunks (coalesced); each lane keeps the extent of its
-// current arc in registers and moves its cursor only at an arc boundary.
+// chunks.  Warp w takes a contiguous 1/warps share of the sequence and its
+// lanes take consecutive chunks (coalesced); each lane keeps the extent of
+// its current arc in registers and moves its cursor only at an arc
+// boundary.  With `next` (a shared counter, zero on entry), the shares
+// cover the first 7/8 of the sequence and the warps then claim the rest
+// 64 U chunks at a time, so that a warp held up by B lists from DRAM or
+// by SEARCH arcs takes less of it and the CTA reaches its next barrier
+// together.
 // Per chunk: the four ids (one 16-byte load) and their four sign bytes (one
 // 4-byte load), a 4-bit mask of the ids inside the arc, then for HASH one
 // 8-byte bucket read per id answers membership and the A' sign together;
@@ -441,25 +446,14 @@ __device__ __forceinline__ void process_chunk(const StageMem& m, uint32_t d, con
 template <int U, bool kSplit>
 __device__ __forceinline__ void stream_pass(const Csr& g, const StageMem& m, uint32_t d,
                                             uint32_t warp, uint32_t warps, uint32_t lane,
-                                            const Geo& geo, TypeCounts& tc) {
+                                            const Geo& geo, TypeCounts& tc, uint32_t* next) {
   const uint32_t total = m.pre[d];
-  const uint32_t per = (total + warps - 1) / warps;
-  const uint32_t c_begin = min(total, warp * per), c_end = min(total, c_begin + per);
-  if (c_begin >= c_end) return;
-  // Arc cursor: the last arc with pre[k] <= first chunk of this lane.
-  uint32_t k;
-  {
-    uint32_t lo_k = 0, hi_k = d;  // pre[d] = total > chunk
-    const uint32_t c0 = c_begin + lane;
-    while (hi_k - lo_k > 1) {
-      const uint32_t mid = (lo_k + hi_k) >> 1;
-      if (m.pre[mid] <= c0) lo_k = mid; else hi_k = mid;
-    }
-    k = lo_k;
-  }
-  // Per arc: chunk index = cb + flattened index; the masks of its first and
-  // last chunk (every chunk between is whole).
-  uint32_t pk, pk1, cb, mf, ml, ast, anuv, asp = 0;
+  const uint32_t fixed = next ? total - total / 8 : total;
+  const uint32_t per = (fixed + warps - 1) / warps;
+  uint32_t seg_begin = min(fixed, warp * per), seg_end = min(fixed, seg_begin + per);
+  // Arc cursor k and, per arc: chunk index = cb + flattened index; the masks
+  // of its first and last chunk (every chunk between is whole).
+  uint32_t k = 0, pk, pk1, cb, mf, ml, ast, anuv, asp = 0;
   auto enter = [&](uint32_t kk) {
     pk = m.pre[kk];
     pk1 = m.pre[kk + 1];
@@ -471,40 +465,63 @@ __device__ __forceinline__ void stream_pass(const Csr& g, const StageMem& m, uin
     anuv = m.s[kk] < 0;
     if (kSplit) asp = m.sp[kk];
   };
-  enter(k);
   // 8-bit fields: at most 4 U adds per field per round.
   constexpr uint32_t kDrainRounds = 255 / (4 * U);
+  constexpr uint32_t kClaim = 64 * U;  // chunks a warp claims at a time
   PackedCounts8 p8;
   uint32_t rounds = 0;
-  for (uint32_t base = c_begin; base < c_end; base += 32 * U) {
-    uint4 q[U];
-    uint32_t sw[U], vm[U], sk[U], snuv[U], sst[U];
-#pragma unroll
-    for (int u = 0; u < U; u++) {
-      const uint32_t c = base + 32 * u + lane;
-      vm[u] = 0;
-      if (c < c_end) {
-        if (c >= pk1) {
-          do {
-            k++;
-          } while (m.pre[k + 1] <= c);
-          enter(k);
+  while (true) {
+    if (seg_begin < seg_end) {
+      // Forward to the last arc with pre[k] <= the lane's first chunk (the
+      // chunks of a lane only grow, and pre[d] = total exceeds every chunk).
+      {
+        uint32_t lo_k = k, hi_k = d;
+        const uint32_t c0 = seg_begin + lane;
+        while (hi_k - lo_k > 1) {
+          const uint32_t mid = (lo_k + hi_k) >> 1;
+          if (m.pre[mid] <= c0) lo_k = mid; else hi_k = mid;
         }
-        const uint32_t ci = cb + c;
-        load_chunk(g, ci, kSplit ? ast : (uint32_t)STC_STRATEGY_HASH, asp, q[u], sw[u]);
-        vm[u] = (c == pk ? mf : 0xFu) & (c + 1 == pk1 ? ml : 0xFu);
-        sk[u] = k;
-        snuv[u] = anuv;
-        sst[u] = ast;
+        k = lo_k;
+        enter(k);
+      }
+      for (uint32_t base = seg_begin; base < seg_end; base += 32 * U) {
+        uint4 q[U];
+        uint32_t sw[U], vm[U], sk[U], snuv[U], sst[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+          const uint32_t c = base + 32 * u + lane;
+          vm[u] = 0;
+          if (c < seg_end) {
+            if (c >= pk1) {
+              do {
+                k++;
+              } while (m.pre[k + 1] <= c);
+              enter(k);
+            }
+            const uint32_t ci = cb + c;
+            load_chunk(g, ci, kSplit ? ast : (uint32_t)STC_STRATEGY_HASH, asp, q[u], sw[u]);
+            vm[u] = (c == pk ? mf : 0xFu) & (c + 1 == pk1 ? ml : 0xFu);
+            sk[u] = k;
+            snuv[u] = anuv;
+            sst[u] = ast;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++)
+          if (vm[u]) process_chunk(m, d, geo, q[u], sw[u], vm[u], sk[u], snuv[u], sst[u], p8);
+        if (++rounds == kDrainRounds) {
+          p8.drain(tc);
+          rounds = 0;
+        }
       }
     }
-#pragma unroll
-    for (int u = 0; u < U; u++)
-      if (vm[u]) process_chunk(m, d, geo, q[u], sw[u], vm[u], sk[u], snuv[u], sst[u], p8);
-    if (++rounds == kDrainRounds) {
-      p8.drain(tc);
-      rounds = 0;
-    }
+    if (!next) break;
+    uint32_t s0 = 0;
+    if (lane == 0) s0 = atomicAdd(next, kClaim);
+    s0 = fixed + __shfl_sync(kFull, s0, 0);
+    if (s0 >= total) break;
+    seg_begin = s0;
+    seg_end = min(total, s0 + kClaim);
   }
   p8.drain(tc);
 }
@@ -826,7 +843,7 @@ __device__ __forceinline__ void warp_vertex(const Csr& g, uint32_t u, uint32_t l
     timed_pass(g, m, d, 0, 1, lane, geo, pc, out, at, kTableWarp);
   } else {
     warp_chunk_scan(m, d, lane);
-    stream_pass<U, kSplit>(g, m, d, 0, 1, lane, geo, out);
+    stream_pass<U, kSplit>(g, m, d, 0, 1, lane, geo, out, nullptr);
     search_pass(g, m, d, 0, 1, lane, pc, out);
   }
   pc.drain(out);
@@ -861,7 +878,8 @@ inline size_t block_stage_bytes(uint32_t cap, uint32_t nb) { return StageMem::by
 constexpr size_t kMaxStageSmem = 220 * 1024;  // dynamic shared memory a staged CTA may use
 
 // One block-class list (the whole CTA), staged in `m` of capacity `cap`
-// with `nb` hash buckets.
+// with `nb` hash buckets.  scan_tmp has THREADS / 32 + 2 words: the chunk
+// scan's and the stream's claim counter.
 template <int THREADS, class Sink, bool kTime, int U, bool kSplit>
 __device__ __forceinline__ void block_vertex(const Csr& g, uint32_t u, uint32_t cap, uint32_t nb,
                                              uint32_t hf, const StageMem& m,
@@ -879,6 +897,10 @@ __device__ __forceinline__ void block_vertex(const Csr& g, uint32_t u, uint32_t 
     return;
   }
   const Geo geo = Geo::of(d, nb, hf);
+  // The stream's claim counter: the CTA passed a barrier since the last list
+  // used it, and stage() passes another before this one does.
+  uint32_t* next = scan_tmp + kWarps + 1;
+  if (threadIdx.x == 0) *next = 0;
   stage<THREADS>(g, ub, d, threadIdx.x, m, geo, table, BlockSync{});
   TypeCounts vc;
   TypeCounts& out = kVC ? vc : tc;
@@ -887,8 +909,8 @@ __device__ __forceinline__ void block_vertex(const Csr& g, uint32_t u, uint32_t 
     timed_pass(g, m, d, w, kWarps, lane, geo, pc, out, at, tclass);
   } else {
     block_chunk_scan<THREADS>(m, d, scan_tmp);
-    stream_pass<U, kSplit>(g, m, d, w, kWarps, lane, geo, out);
     search_pass(g, m, d, w, kWarps, lane, pc, out);
+    stream_pass<U, kSplit>(g, m, d, w, kWarps, lane, geo, out, next);
   }
   pc.drain(out);
   if (kVC) block_vertex_flush<THREADS>(vc, u, sink);
@@ -905,7 +927,7 @@ __global__ void __launch_bounds__(THREADS) k_block(Csr g, const uint32_t* __rest
   constexpr bool kVC = Sink::kPerVertex;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ uint8_t table[16][16];
-  __shared__ uint32_t scan_tmp[THREADS / 32 + 1];
+  __shared__ uint32_t scan_tmp[THREADS / 32 + 2];
   __shared__ uint32_t s_item;
   for (int i = threadIdx.x; i < 256; i += THREADS) (&table[0][0])[i] = gtable[i];
   if (plan) {  // list and count planned on the device
@@ -1131,7 +1153,7 @@ __global__ void __launch_bounds__(256, 4) k_persistent(Csr g, const uint32_t* __
                                                        const uint8_t* __restrict__ gtables) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ uint8_t tw[16][16], tb[16][16];
-  __shared__ uint32_t scan_tmp[256 / 32 + 1];
+  __shared__ uint32_t scan_tmp[256 / 32 + 2];
   __shared__ uint32_t s_item;
   (&tw[0][0])[threadIdx.x] = gtables[256 * kTableWarp + threadIdx.x];
   (&tb[0][0])[threadIdx.x] = gtables[256 * kTableBlock + threadIdx.x];
