@@ -123,17 +123,37 @@ def _check(status: int, ctx=None) -> None:
         raise StcError(status, msg)
 
 
-def _edge_list_from_c(el: _capi.stc_edge_list) -> EdgeList:
+class _EdgeBuffers:
+    """Owns the three malloc'd arrays of one stc_edge_list and frees them
+    (stc_free_edge_list) once no numpy view of them is left."""
+
+    def __init__(self, el: _capi.stc_edge_list):
+        self._el = el
+
+    def __del__(self):
+        try:
+            lib().stc_free_edge_list(C.byref(self._el))
+        except Exception:
+            pass
+
+
+def _view(ptr, ctype, m: int, owner: _EdgeBuffers, dtype) -> np.ndarray:
+    arr = (ctype * m).from_address(C.cast(ptr, C.c_void_p).value)
+    arr._owner = owner  # the ctypes array, numpy's base, keeps the owner alive
+    return np.frombuffer(arr, dtype=dtype)
+
+
+def _edge_list_take(el: _capi.stc_edge_list) -> EdgeList:
+    """An EdgeList over the library's arrays without copying them; the arrays
+    are freed with the last view."""
     m = el.m
-    if m:
-        src = np.ctypeslib.as_array(el.src, (m,)).copy()
-        dst = np.ctypeslib.as_array(el.dst, (m,)).copy()
-        sign = np.ctypeslib.as_array(el.sign, (m,)).copy()
-    else:
-        src = np.zeros(0, np.uint32)
-        dst = np.zeros(0, np.uint32)
-        sign = np.zeros(0, np.int8)
-    return EdgeList(n=el.n, m=m, src=src, dst=dst, sign=sign, lines=el.lines)
+    owner = _EdgeBuffers(el)
+    if not m:
+        return EdgeList(n=el.n, m=0, src=np.zeros(0, np.uint32), dst=np.zeros(0, np.uint32),
+                        sign=np.zeros(0, np.int8), lines=el.lines)
+    return EdgeList(n=el.n, m=m, src=_view(el.src, C.c_uint32, m, owner, np.uint32),
+                    dst=_view(el.dst, C.c_uint32, m, owner, np.uint32),
+                    sign=_view(el.sign, C.c_int8, m, owner, np.int8), lines=el.lines)
 
 
 def load_graph(path: str) -> EdgeList:
@@ -143,19 +163,13 @@ def load_graph(path: str) -> EdgeList:
     if st == _capi.STC_ERR_IO:
         raise OSError(f"cannot read {path}")
     _check(st)
-    try:
-        return _edge_list_from_c(el)
-    finally:
-        lib().stc_free_edge_list(C.byref(el))
+    return _edge_list_take(el)
 
 
 def parse_edge_text(data: bytes) -> EdgeList:
     el = _capi.stc_edge_list()
     _check(lib().stc_parse_edge_text(data, len(data), C.byref(el)))
-    try:
-        return _edge_list_from_c(el)
-    finally:
-        lib().stc_free_edge_list(C.byref(el))
+    return _edge_list_take(el)
 
 
 def load_mtx(path: str, *, zero_negative: bool = False) -> EdgeList:
@@ -168,20 +182,14 @@ def load_mtx(path: str, *, zero_negative: bool = False) -> EdgeList:
     if st == _capi.STC_ERR_IO:
         raise OSError(f"cannot read {path}")
     _check(st)
-    try:
-        return _edge_list_from_c(el)
-    finally:
-        lib().stc_free_edge_list(C.byref(el))
+    return _edge_list_take(el)
 
 
 def parse_mtx(data: bytes, *, zero_negative: bool = False) -> EdgeList:
     el = _capi.stc_edge_list()
     _check(lib().stc_parse_mtx(data, len(data), _capi.MTX_ZERO_NEGATIVE if zero_negative else 0,
                                C.byref(el)))
-    try:
-        return _edge_list_from_c(el)
-    finally:
-        lib().stc_free_edge_list(C.byref(el))
+    return _edge_list_take(el)
 
 
 def _host_arrays(src, dst, sign):
@@ -303,10 +311,7 @@ class Context:
         o = self._opts(timing=False)
         _check(lib().stc_parse_edge_text_gpu(self._h, C.c_char_p(data), len(data), C.byref(o),
                                              C.byref(el)), self._h)
-        try:
-            return _edge_list_from_c(el)
-        finally:
-            lib().stc_free_edge_list(C.byref(el))
+        return _edge_list_take(el)
 
     def count_edge_list(self, el: EdgeList, **kw) -> GlobalTriCounts:
         return self.count(el.src, el.dst, el.sign, **kw)

@@ -23,8 +23,40 @@
 
 namespace {
 
+constexpr uint32_t kPow10[9] = {1u, 10u, 100u, 1000u, 10000u, 100000u, 1000000u, 10000000u,
+                                 100000000u};
+
+// Decimal digits at p as a uint32 with wrap-around (x = 10 x + d per digit,
+// mod 2^32), 8 bytes at a time while 8 bytes remain.  In t = bytes - '0',
+// digit bytes hold 0..9; the first byte that is not a digit has its high bit
+// set in t | (t + 0x76) (a borrow or carry only moves towards later bytes,
+// so the bytes before it are exact).  The k leading digits are shifted to
+// the top and combined pairwise by three multiply-shift steps (the
+// eight-digit method of simdjson's number parser), then x = x 10^k + value,
+// which equals k steps of the per-digit rule mod 2^32.
 inline const char* parse_uint(const char* p, const char* end, uint32_t& out) {
   uint32_t x = 0;
+  while (end - p >= 8) {
+    uint64_t w;
+    memcpy(&w, p, 8);
+    const uint64_t t = w - 0x3030303030303030ull;
+    const uint64_t nd = (t | (t + 0x7676767676767676ull)) & 0x8080808080808080ull;
+    const unsigned k = nd ? (unsigned)__builtin_ctzll(nd) >> 3 : 8u;
+    if (k == 0) {
+      out = x;
+      return p;
+    }
+    uint64_t v = k == 8 ? t : t << (8 * (8 - k));
+    v = ((v & 0x0F0F0F0F0F0F0F0Full) * 2561u) >> 8;
+    v = ((v & 0x00FF00FF00FF00FFull) * 6553601u) >> 16;
+    v = ((v & 0x0000FFFF0000FFFFull) * 42949672960001ull) >> 32;
+    x = x * kPow10[k] + (uint32_t)v;
+    p += k;
+    if (k < 8) {
+      out = x;
+      return p;
+    }
+  }
   while (p < end && *p >= '0' && *p <= '9') x = x * 10u + (uint32_t)(*p++ - '0');
   out = x;
   return p;
