@@ -35,7 +35,7 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "edges/s (undirected edges after dedup, whole counting path)"
 UNIT = "edges/s"
-CPU_SAMPLE_SCALE = 20  # RMAT scale of the bounded CPU sample
+CPU_SAMPLE_DIV = 64  # the CPU baseline counts the sources with id < n / CPU_SAMPLE_DIV
 
 WORKLOADS = {
     1: "ER G(n=10,000, m=100,000), p(+)=0.7",
@@ -118,8 +118,8 @@ def load_peaks() -> dict:
 
 
 def load_traffic(workload: int, rmat_scale: int = 24):
-    """DRAM bytes (read + write) of one count stage, from the committed ncu
-    summary (profiles/count_rmat24_traffic.md), or None where none was taken."""
+    """DRAM bytes (read + write) of one count stage as measured by ncu and
+    committed with the profiles, or None where none was taken."""
     p = ROOT / "profiles" / "ncu_traffic.json"
     if not p.exists() or (workload == 3 and rmat_scale != 24):
         return None
@@ -178,22 +178,56 @@ def make_device_workload(ctx, workload: int, seed_offset: int, torch, scale: int
             torch.from_numpy(el.sign).to(dev))
 
 
-def cpu_reference_sample(threads: int | None = None) -> dict:
-    """The reference's own CPU path (oracle/_ref harness around tc_serial.cpp:
-    build_forward_csr + sort_adj_lists + count_triangles, OpenMP on all host
-    threads) on RMAT scale CPU_SAMPLE_SCALE with the workload's parameters."""
+def cpu_reference_run(scale: int, steps: int, warmup: int, log=None) -> dict | None:
+    """The reference's own CPU path on the power-law workload, with all host
+    threads (OpenMP).  The input is the workload's edge list made by the
+    oracle's restatement of the generator (bit-equal to the package's, and
+    loading nothing from the package).  The reference's build_forward_csr
+    and sort_adj_lists run once, at full size, and are timed there.  Each
+    step then times its count_triangles (MC/tc_serial.cpp:138-170, unchanged)
+    on a bounded sample of the same graph: the sources whose id is below
+    n / CPU_SAMPLE_DIV, a uniform random vertex sample because the generator
+    relabels ids by a seeded bijection.  A step's rate charges the sample its
+    count time plus its share (by edges) of the full-size build and sort:
+    sampled edges / (count s + (build s + sort s) * sampled edges / edges)."""
     import oracle
-    from signed_triangle_counting_b200 import synth
     if not oracle.ref_available():
         return None
-    el = synth.rmat(synth.workload_seed(3), CPU_SAMPLE_SCALE, 1 << CPU_SAMPLE_SCALE,
-                    16 << CPU_SAMPLE_SCALE, p_pos=0.5)
-    t, sec, fwd = oracle.ref_count_arrays(el.src, el.dst, el.sign, with_edges=True)
-    total = sum(sec)
-    return dict(edges=fwd, seconds=total, value=fwd / total, counts=t, stage_seconds=sec,
-                sample=f"RMAT scale {CPU_SAMPLE_SCALE} (2^{CPU_SAMPLE_SCALE} vertices, "
-                       f"{16 << CPU_SAMPLE_SCALE} samples, {fwd} unique edges), same (a,b,c) and "
-                       f"p(+); timed: build_forward_csr + sort_adj_lists + count_triangles")
+    from oracle import RefKeptCSR, synth_rmat
+    seed = 1000 + 3  # the power-law workload's seed
+    t0 = time.perf_counter()
+    src, dst, sign = synth_rmat(seed, scale, 1 << scale, 16 << scale, 0.57, 0.19, 0.19, 0.5)
+    gen_s = time.perf_counter() - t0
+    kept = RefKeptCSR(src, dst, sign)
+    del src, dst, sign
+    try:
+        n_s = max(1, kept.n // CPU_SAMPLE_DIV)
+        arcs_s, work_s = kept.prefix_size(n_s)
+        arcs, work = kept.prefix_size(kept.n)
+        prep_share = (kept.build_s + kept.sort_s) * arcs_s / max(1, arcs)
+        vals, secs, counts = [], [], None
+        for i in range(warmup + steps):
+            counts, sec = kept.count_prefix(n_s)
+            if log:
+                log(f"cpu sample step {i}: {sec:.3f} s")
+            if i >= warmup:
+                secs.append(sec)
+                vals.append(arcs_s / (sec + prep_share))
+        count_s = statistics.median(secs)
+        return dict(
+            value=statistics.median(vals), step_seconds=secs, counts=counts,
+            threads=kept.threads, edges=arcs, n=kept.n, sample_edges=arcs_s,
+            build_s=kept.build_s, sort_s=kept.sort_s, gen_s=gen_s,
+            count_edges_per_s=arcs_s / count_s,
+            count_s_full_projected=count_s * work / max(1, work_s),
+            sample=(f"RMAT scale {scale} (the workload's graph: {arcs} edges after dedup); "
+                    f"timed per step: the reference's count_triangles over the {arcs_s} edges "
+                    f"of the sources with id < n/{CPU_SAMPLE_DIV} ({n_s} of {kept.n} vertices, a "
+                    f"uniform random vertex sample), plus the sample's edge share of its "
+                    f"build_forward_csr ({kept.build_s:.2f} s) and sort_adj_lists "
+                    f"({kept.sort_s:.2f} s), measured once at full size"))
+    finally:
+        kept.close()
 
 
 def run_reference(args) -> None:
@@ -205,72 +239,149 @@ def run_reference(args) -> None:
         print(json.dumps({"impl": "reference", "unavailable":
                           "oracle/_ref (the reference compiled from its sources) is missing"}))
         return
-    cores = os.cpu_count()
-    vals = []
-    r = None
-    for i in range(args.warmup + args.steps):
-        r = cpu_reference_sample()
-        if i >= args.warmup:
-            vals.append(r["value"])
-    value = statistics.median(vals)
+    r = cpu_reference_run(args.rmat_scale, args.steps, args.warmup)
+    value = r["value"]
     out = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["seconds"] * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32/i8",
-        "data": "synthetic",
-        "config": {"workload": WORKLOADS[3], "parallelism": "host OpenMP",
-                   "cpu_sample": r["sample"]},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": statistics.mean(r["step_seconds"]) * 1e3,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "u32/i8 (ids/signs), u64 counters", "data": "synthetic (seeded, generated on the host)",
+        "config": dict(workload_config(3, args.rmat_scale), m_input=16 << args.rmat_scale,
+                       m_unique=r["edges"], n=r["n"]),
+        "run": {"parallelism": f"host OpenMP, {r['threads']} threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": r["threads"], "kind": "reference",
                          "sample": r["sample"]},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "counts": list(r["counts"]),
+        "reference_stages": {k: r[k] for k in ("build_s", "sort_s", "gen_s", "count_edges_per_s",
+                                               "count_s_full_projected", "sample_edges", "edges")},
+        "sample_counts": list(r["counts"]),
     }
     print(json.dumps(out))
 
 
-def compare_forms(ctx, args, src, dst, sign, offs, stream, torch, edges) -> dict:
-    """The metric's comparison on resident inputs, one process, one GPU:
-    the plain fixed form (one graph per call, per-class kernels, fixed
-    dispatch) against the learned + batched form (the whole batch in one
-    call on the persistent engine, learned dispatch; for a single graph,
-    learned dispatch alone).  Each form: one warm-up pass, then `steps`
-    timed passes with CUDA events."""
-    ctx.load_dispatch_model()
-    spans = ([(int(offs[g]), int(offs[g + 1])) for g in range(len(offs) - 1)]
-             if offs is not None else [(0, int(src.numel()))])
+def workload_config(workload: int, rmat_scale: int = 24) -> dict:
+    """The `config` both arms print for a workload."""
+    if workload == 3 and rmat_scale != 24:
+        name = f"RMAT scale {rmat_scale}, edge factor 16, (.57,.19,.19,.05), p(+)=0.5"
+    else:
+        name = WORKLOADS[workload]
+    return {"workload": name}
+
+
+def _time_form(fn, steps: int, stream, torch) -> float:
+    """One untimed pass, then `steps` passes timed with CUDA events on
+    `stream`; mean milliseconds per pass."""
+    fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(steps):
+        fn()
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / steps
+
+
+def forms_run(ctx, args, stream, torch) -> dict:
+    """The metric's second half, in the same run: the plain fixed-threshold
+    form against the learned and batched forms, on the batched and the
+    skewed workloads, each form timed over resident inputs (one untimed
+    pass, then --forms-steps passes, CUDA events), counts checked against
+    the reference's.
+
+    batch: graphs [0, G) of the 4,096-graph batch (G = --forms-graphs; the
+      graph recipes are drawn i.i.d., so a prefix is a random sample):
+        plain_fixed      one call per graph, per-class kernels, fixed dispatch
+        batched_fixed    all G graphs in one call, persistent engine replayed
+                         from a CUDA graph, fixed dispatch
+        learned_batched  as batched_fixed with the learned dispatch tables
+    skew: the whole skewed graph, per-class kernels:
+        plain_fixed      fixed dispatch
+        learned          learned dispatch tables"""
+    from signed_triangle_counting_b200 import autotune, synth
+    dev = torch.device("cuda", ctx.device)
+    model = ctx.load_dispatch_model()
+    out = {"dispatch_model": model.get("trained_on"), "steps": args.forms_steps}
+    sampler = ClockSampler(ctx.device)
+    sampler.start()
     kw = dict(stream=stream.cuda_stream)
 
+    # ---- batched workload
+    G = args.forms_graphs
+    specs = synth.batch_specs(4096)[:G]
+    t0 = time.perf_counter()
+    el, offs = synth.batch_packed(specs)
+    gen_s = time.perf_counter() - t0
+    src = torch.from_numpy(el.src.view("int32")).to(dev)
+    dst = torch.from_numpy(el.dst.view("int32")).to(dev)
+    sign = torch.from_numpy(el.sign).to(dev)
+    del el
+    spans = [(int(offs[g]), int(offs[g + 1])) for g in range(G)]
+    ctx.set_tuning(autotune.tuning_for(4))
+    res = {}
+
     def plain():
-        for b, e in spans:
-            if e > b:
-                ctx.count(src[b:e], dst[b:e], sign[b:e], dispatch="fixed", persistent=False, **kw)
+        res["plain"] = [ctx.count(src[b:e], dst[b:e], sign[b:e], dispatch="fixed",
+                                  persistent=False, **kw) for b, e in spans]
 
-    def learned():
-        if offs is not None:
-            ctx.count_batch_packed(src, dst, sign, offs, dispatch="learned", persistent=True, **kw)
-        else:
-            ctx.count(src, dst, sign, dispatch="learned", persistent=False, **kw)
+    def batched(dispatch):
+        def fn():
+            res[dispatch] = ctx.count_batch_packed(src, dst, sign, offs, dispatch=dispatch,
+                                                   persistent=True, **kw)
+        return fn
 
-    def timed(fn):
-        fn()
-        torch.cuda.synchronize()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        for _ in range(args.steps):
-            fn()
-        b.record(stream)
-        torch.cuda.synchronize()
-        return a.elapsed_time(b) / args.steps
+    ms = {"plain_fixed": _time_form(plain, args.forms_steps, stream, torch),
+          "batched_fixed": _time_form(batched("fixed"), args.forms_steps, stream, torch),
+          "learned_batched": _time_form(batched("learned"), args.forms_steps, stream, torch)}
+    edges = ctx.last_stats().m_unique
+    want = golden_counts(4)
+    got = {k: [list(c.as_tuple()) for c in res[r]]
+           for k, r in (("plain_fixed", "plain"), ("batched_fixed", "fixed"),
+                        ("learned_batched", "learned"))}
+    exact = (all(v == want[:G] for v in got.values()) if want else None)
+    out["batch"] = {
+        "graphs": G, "m_input": int(offs[-1]), "m_unique": int(edges), "gen_s": gen_s,
+        "exact": exact,
+        "forms": {k: {"ms": v, "edges_per_s": edges / (v / 1e3)} for k, v in ms.items()},
+        "ratio_learned_batched_vs_plain_fixed": ms["plain_fixed"] / ms["learned_batched"],
+        "ratio_batched_fixed_vs_plain_fixed": ms["plain_fixed"] / ms["batched_fixed"],
+        "ratio_learned_vs_fixed_batched": ms["batched_fixed"] / ms["learned_batched"],
+    }
+    del src, dst, sign
 
-    ms_plain, ms_learned = timed(plain), timed(learned)
+    # ---- skewed workload
+    t0 = time.perf_counter()
+    el = synth.workload(5)
+    gen_s = time.perf_counter() - t0
+    src = torch.from_numpy(el.src.view("int32")).to(dev)
+    dst = torch.from_numpy(el.dst.view("int32")).to(dev)
+    sign = torch.from_numpy(el.sign).to(dev)
+    del el
+    ctx.set_tuning(autotune.tuning_for(5))
+
+    def single(dispatch):
+        def fn():
+            res[dispatch] = ctx.count(src, dst, sign, dispatch=dispatch, persistent=False, **kw)
+        return fn
+
+    ms = {"plain_fixed": _time_form(single("fixed"), args.forms_steps, stream, torch),
+          "learned": _time_form(single("learned"), args.forms_steps, stream, torch)}
+    st = ctx.last_stats()
+    want = golden_counts(5)
+    exact = (res["fixed"].as_tuple() == want and res["learned"].as_tuple() == want
+             if want else None)
+    out["skew"] = {
+        "m_input": int(src.numel()), "m_unique": int(st.m_unique), "gen_s": gen_s, "exact": exact,
+        "stage_ms": {"dedup": st.ms_dedup, "orient": st.ms_orient, "csr": st.ms_csr,
+                     "count": st.ms_count},
+        "forms": {k: {"ms": v, "edges_per_s": st.m_unique / (v / 1e3)} for k, v in ms.items()},
+        "ratio_learned_vs_plain_fixed": ms["plain_fixed"] / ms["learned"],
+    }
+    del src, dst, sign
     ctx.set_dispatch_model(None)
-    return {"plain_fixed": {"edges_per_s": edges / (ms_plain / 1e3), "ms": ms_plain,
-                            "form": "one graph per call, per-class kernels, fixed dispatch"},
-            "learned_batched": {"edges_per_s": edges / (ms_learned / 1e3), "ms": ms_learned,
-                                "form": ("whole batch in one call, persistent engine (CUDA graph), "
-                                         "learned dispatch") if offs is not None else
-                                        "learned dispatch, per-class kernels"},
-            "ratio": ms_plain / ms_learned}
+    out["clocks"] = sampler.stop()
+    return out
 
 
 def run_gpu(args) -> None:
@@ -307,6 +418,7 @@ def run_gpu(args) -> None:
     else:
         offs_run = offs
     torch.cuda.synchronize()
+    m_total_input = int(wl[0].numel())
     m_input = src.numel()
     persistent = args.engine == "persistent" or (args.engine == "auto" and offs is not None)
     kw = dict(strategy=args.strategy, dispatch=args.dispatch, stream=stream.cuda_stream,
@@ -419,8 +531,8 @@ def run_gpu(args) -> None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
     e2e_value = edges * e2e_steps / (e2e_ms / 1e3)
-    forms = (compare_forms(ctx, args, src, dst, sign, offs_run, stream, torch, edges)
-             if args.compare_forms and world == 1 else None)
+    forms = (forms_run(ctx, args, stream, torch)
+             if world == 1 and args.workload == 3 and not args.no_forms else None)
 
     if rank == 0:
         peaks = load_peaks()
@@ -428,11 +540,12 @@ def run_gpu(args) -> None:
         achieved = alg_bytes / (cms / 1e3) / 1e9
         traffic = load_traffic(args.workload, args.rmat_scale)
         cpu = None
-        if world == 1 and not args.skip_cpu:
-            r = cpu_reference_sample()
+        if world == 1 and args.workload == 3 and not args.skip_cpu:
+            r = cpu_reference_run(args.rmat_scale, steps=2, warmup=0)
             if r:
-                cpu = {"value": r["value"], "unit": UNIT, "cores": os.cpu_count(),
-                       "kind": "reference", "sample": r["sample"]}
+                cpu = {"value": r["value"], "unit": UNIT, "cores": r["threads"],
+                       "kind": "reference", "sample": r["sample"],
+                       "count_edges_per_s": r["count_edges_per_s"]}
         if world == 1:
             par = "1 GPU"
         elif offs is not None:
@@ -446,16 +559,14 @@ def run_gpu(args) -> None:
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "u32/i8 (ids/signs), u64 counters",
             "data": "synthetic (seeded, generated on the device)",
-            "config": {"workload": WORKLOADS[args.workload] if full else
-                       f"RMAT scale {args.rmat_scale}, edge factor 16, (.57,.19,.19,.05), p(+)=0.5",
-                       "m_input": int(m_input) if world == 1 or offs is None else None,
-                       "m_unique": edges, "n": st.n if offs is None else None,
-                       "strategy": args.strategy, "dispatch": args.dispatch,
-                       "dispatch_model": model.get("trained_on") if model else None,
-                       "engine": "persistent (CUDA graph)" if persistent else "class kernels",
-                       "tuning": tuning,
-                       "l2": f"inputs {m_input * 9 / 1e9:.1f} GB per rank > 126 MB L2, no flush",
-                       "parallelism": par},
+            "config": dict(workload_config(args.workload, args.rmat_scale),
+                           m_input=int(m_total_input), m_unique=edges,
+                           n=st.n if offs is None else None),
+            "run": {"parallelism": par, "strategy": args.strategy, "dispatch": args.dispatch,
+                    "dispatch_model": model.get("trained_on") if model else None,
+                    "engine": "persistent (CUDA graph)" if persistent else "class kernels",
+                    "tuning": tuning,
+                    "l2": f"inputs {m_input * 9 / 1e9:.1f} GB per rank > 126 MB L2, no flush"},
             "exact": exact, "counts": counts_out,
             "stage_ms": {"dedup": st.ms_dedup, "orient": st.ms_orient, "csr": st.ms_csr,
                          "count": st.ms_count, "device_total": st.ms_total},
@@ -491,8 +602,11 @@ def main() -> None:
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--no-tuning", action="store_true",
                     help="untuned launch parameters instead of the workload's autotuned ones")
-    ap.add_argument("--compare-forms", action="store_true",
-                    help="also time the plain fixed form against the learned + batched form")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the plain / batched / learned forms on the batch and skew workloads")
+    ap.add_argument("--forms-graphs", type=int, default=1024,
+                    help="graphs of the batch workload the forms are timed on")
+    ap.add_argument("--forms-steps", type=int, default=3)
     ap.add_argument("--engine", default="auto", choices=["auto", "persistent", "classes"],
                     help="counting engine (auto: persistent for the batch, class kernels else)")
     ap.add_argument("--rmat-scale", type=int, default=24,

@@ -267,10 +267,12 @@ stc_status stc_count_batch(stc_ctx* ctx, const stc_graph* graphs, uint32_t G,
  * else STC_ERR_LIMIT.
  * Scratch: one file-scope device array of about 16 MiB, which every GPU that
  * loads the library keeps until the process exits.  All calls share it, so
- * calls that overlap on the GPU race.  The first call on a device looks up
- * the array's device address (cudaGetSymbolAddress) with that device
- * current; make that first call before any stream capture.  `stream` may be
- * NULL (the legacy default stream). */
+ * calls that overlap on the GPU race.  The first call in a CUDA context
+ * looks up the array's device address there (cudaGetSymbolAddress) with
+ * that context current, and a call looks it up again when the current
+ * context is not the one it last saw on that device (after cudaDeviceReset,
+ * or under a caller's own context); make the first call in a context before
+ * any stream capture.  `stream` may be NULL (the legacy default stream). */
 stc_status stc_count_oriented_csr_noalloc(const uint64_t* d_offsets, const uint32_t* d_heads,
                                           const int8_t* d_signs, uint32_t n, uint64_t m,
                                           void* stream, stc_counts* out);

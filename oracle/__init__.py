@@ -46,9 +46,14 @@ _ref = None
 
 
 def build() -> None:
-    """Runs oracle/Makefile (the C restatement, and _ref/ when the reference
-    sources are present)."""
-    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    """Runs oracle/Makefile: the C restatement, and _ref/ when the
+    STC_REFERENCE_DIR environment variable names the reference's
+    "Signed_TC/Multicore Implementations" directory."""
+    cmd = ["make", "-s", "-C", str(HERE)]
+    ref = os.environ.get("STC_REFERENCE_DIR")
+    if ref:
+        cmd.append(f"REF={ref}")
+    subprocess.run(cmd, check=True)
 
 
 def lib() -> C.CDLL:
@@ -69,6 +74,11 @@ def lib() -> C.CDLL:
         L.orc_count_merge.argtypes = [C.POINTER(_CSR), u64p, u64p]
         L.orc_count_hash.argtypes = [C.POINTER(_CSR), u64p, u64p]
         L.orc_count_arrays.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, u64p]
+        L.orc_synth_rmat.argtypes = [C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint64, C.c_double,
+                                     C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
+                                     C.c_void_p]
+        L.orc_write_edge_text.argtypes = [C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_uint64]
         _lib = L
     return _lib
 
@@ -167,6 +177,30 @@ def count_arrays(src, dst, sign) -> tuple:
     return tuple(t)
 
 
+def synth_rmat(seed: int, scale: int, n: int, samples: int, a=0.57, b=0.19, c=0.19,
+               p_pos=0.5) -> tuple:
+    """The package's seeded RMAT generator restated in C (synth_rmat.c):
+    (src, dst, sign) arrays equal to signed_triangle_counting_b200.synth.rmat's
+    for the same arguments, made without loading the package's library."""
+    src = np.empty(samples, np.uint32)
+    dst = np.empty(samples, np.uint32)
+    sign = np.empty(samples, np.int8)
+    rc = lib().orc_synth_rmat(seed, scale, n, samples, a, b, c, p_pos, src.ctypes.data,
+                              dst.ctypes.data, sign.ctypes.data)
+    if rc != 0:
+        raise ValueError(f"orc_synth_rmat rejected its arguments ({rc})")
+    return src, dst, sign
+
+
+def write_edge_text(path, src, dst, sign) -> None:
+    """`u v sign` lines (sign 1 / -1), the reference programs' input format."""
+    src, dst, sign = _arr(src, np.uint32), _arr(dst, np.uint32), _arr(sign, np.int8)
+    rc = lib().orc_write_edge_text(str(path).encode(), src.ctypes.data, dst.ctypes.data,
+                                   sign.ctypes.data, len(src))
+    if rc != 0:
+        raise OSError(f"writing {path} failed ({rc})")
+
+
 # ------------------------------------------------------- reference (_ref) --
 def ref_available() -> bool:
     return REF_HARNESS.exists() and all((REF_DIR / p).exists() for p in REF_PROGRAMS)
@@ -181,6 +215,12 @@ def _ref_lib() -> C.CDLL:
         L.stc_ref_forward_csr.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64,
                                           u32p, u64p, C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_void_p, C.c_void_p]
+        L.stc_ref_prepare.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64,
+                                      C.POINTER(C.c_double), u32p, u64p]
+        L.stc_ref_prefix_size.argtypes = [C.c_uint32, u64p, u64p]
+        L.stc_ref_count_prefix.argtypes = [C.c_uint32, u64p, C.POINTER(C.c_double)]
+        L.stc_ref_release.argtypes = []
+        L.stc_ref_threads.argtypes = []
         _ref = L
     return _ref
 
@@ -217,6 +257,59 @@ def ref_forward_csr(src, dst, sign) -> dict:
     out["edges"], out["signs"] = out["edges"][:M], out["signs"][:M]
     out["fdeg"], out["rank"] = out["fdeg"][:N], out["rank"][:N]
     return out
+
+
+class RefKeptCSR:
+    """The reference's forward CSR of one edge list, built and sorted once by
+    its own build_forward_csr and sort_adj_lists and kept in the harness, so
+    that count_triangles can be timed on samples of its sources.  One at a
+    time per process."""
+
+    def __init__(self, src, dst, sign):
+        src, dst, sign = _arr(src, np.uint32), _arr(dst, np.uint32), _arr(sign, np.int8)
+        sec = (C.c_double * 2)()
+        n, fe = C.c_uint32(), C.c_uint64()
+        L = _ref_lib()
+        assert L.stc_ref_prepare(src.ctypes.data, dst.ctypes.data, sign.ctypes.data, len(src), sec,
+                                 C.byref(n), C.byref(fe)) == 0
+        self.n, self.m = n.value, fe.value
+        self.build_s, self.sort_s = sec[0], sec[1]
+        self.threads = int(L.stc_ref_threads())
+
+    def prefix_size(self, n_sources: int) -> tuple:
+        """(forward edges, merge work) of the sources with id < n_sources."""
+        arcs, work = C.c_uint64(), C.c_uint64()
+        assert _ref_lib().stc_ref_prefix_size(n_sources, C.byref(arcs), C.byref(work)) == 0
+        return arcs.value, work.value
+
+    def count_prefix(self, n_sources: int) -> tuple:
+        """count_triangles over the sources with id < n_sources:
+        ((t0, t1, t2, t3), seconds)."""
+        t = (C.c_uint64 * 4)()
+        sec = C.c_double()
+        assert _ref_lib().stc_ref_count_prefix(n_sources, t, C.byref(sec)) == 0
+        return tuple(t), sec.value
+
+    def vertex_counts(self) -> np.ndarray:
+        """The reference's per-source counts cnt[4n] (tc_serial.cpp:141-158),
+        recovered as differences of prefix counts (one count per vertex: for
+        small graphs only)."""
+        out = np.zeros((self.n, 4), np.uint64)
+        prev = np.zeros(4, np.uint64)
+        for u in range(self.n):
+            cur = np.array(self.count_prefix(u + 1)[0], np.uint64)
+            out[u] = cur - prev
+            prev = cur
+        return out.reshape(-1)
+
+    def close(self) -> None:
+        _ref_lib().stc_ref_release()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 _NUM = r"(\d+)"

@@ -98,4 +98,83 @@ int stc_ref_forward_csr(const uint32_t* u, const uint32_t* v, const int8_t* s, u
   return 0;
 }
 
+// ---------------------------------------------------------------------
+// A reference CSR kept between calls, so that the benchmark's CPU baseline
+// can time count_triangles on a bounded sample of a large graph: the
+// sample is the sources whose id is below a bound.  The generators relabel
+// ids by a seeded bijection, so such a prefix is a uniform random sample of
+// the vertices.
+
+namespace {
+ForwardCSR g_kept{};
+bool g_have_kept = false;
+}  // namespace
+
+// OpenMP threads the reference's parallel loops use.
+int stc_ref_threads(void) { return omp_get_max_threads(); }
+
+void stc_ref_release(void) {
+  if (g_have_kept) free_forward_csr(g_kept);
+  g_kept = ForwardCSR{};
+  g_have_kept = false;
+}
+
+// build_forward_csr + sort_adj_lists of these edges, kept for
+// stc_ref_count_prefix; seconds[0] and seconds[1] receive their times.
+int stc_ref_prepare(const uint32_t* u, const uint32_t* v, const int8_t* s, uint64_t m,
+                    double seconds[2], uint32_t* n_out, uint64_t* forward_edges) {
+  if (m >= (1ull << 32)) return 1;
+  stc_ref_release();
+  EdgeList el = make_edge_list(u, v, s, m);
+  Timer tb;
+  g_kept = build_forward_csr(el);
+  const double t_build = tb.elapsed_sec();
+  free_edge_list(el);
+  Timer ts;
+  sort_adj_lists(g_kept);
+  const double t_sort = ts.elapsed_sec();
+  g_have_kept = true;
+  if (seconds) {
+    seconds[0] = t_build;
+    seconds[1] = t_sort;
+  }
+  if (n_out) *n_out = g_kept.n;
+  if (forward_edges) *forward_edges = g_kept.m;
+  return 0;
+}
+
+// Sources [0, n_sources) of the kept CSR: their forward edges and their
+// merge work, the sum over those edges u -> v of fdeg[u] + fdeg[v] (the
+// entries a merge of both lists scans).
+int stc_ref_prefix_size(uint32_t n_sources, uint64_t* arcs, uint64_t* merge_work) {
+  if (!g_have_kept || n_sources > g_kept.n) return 1;
+  uint64_t w = 0;
+  for (uint32_t x = 0; x < n_sources; x++)
+    for (uint64_t e = g_kept.offsets[x]; e < g_kept.offsets[x + 1]; e++)
+      w += (uint64_t)g_kept.fdeg[x] + g_kept.fdeg[g_kept.edges[e]];
+  if (arcs) *arcs = g_kept.offsets[n_sources];
+  if (merge_work) *merge_work = w;
+  return 0;
+}
+
+// count_triangles (tc_serial.cpp:138-170), unchanged, over the sources with
+// id below n_sources of the kept CSR: it runs on a copy of the CSR header
+// whose n is n_sources, while every array stays whole, so each source's
+// merges read its neighbours' lists as in a full count.  t[0..3] receives
+// the counts of the triangles whose first vertex in the CSR's orientation
+// is one of those sources, `seconds` the time of the call.
+int stc_ref_count_prefix(uint32_t n_sources, uint64_t t[4], double* seconds) {
+  if (!g_have_kept || n_sources > g_kept.n) return 1;
+  ForwardCSR view = g_kept;
+  view.n = n_sources;
+  Timer tc;
+  GlobalTriCounts g = count_triangles(view);
+  if (seconds) *seconds = tc.elapsed_sec();
+  t[0] = g.t0;
+  t[1] = g.t1;
+  t[2] = g.t2;
+  t[3] = g.t3;
+  return 0;
+}
+
 }  // extern "C"

@@ -70,6 +70,16 @@ int orc_count_hash(const orc_forward_csr* csr, uint64_t* balanced, uint64_t* unb
 int orc_count_arrays(const uint32_t* u, const uint32_t* v, const int8_t* s, uint64_t m,
                      uint64_t t[4]);
 
+/* synth_rmat.c: the package's seeded RMAT workload generator restated
+ * (same arguments and output as stc_synth_rmat in include/stc_synth.h), so
+ * that the reference's code can be fed the benchmark input without the
+ * package's library; OpenMP over the samples. */
+int orc_synth_rmat(uint64_t seed, uint32_t scale, uint64_t n, uint64_t samples, double a,
+                   double b, double c, double p_pos, uint32_t* src, uint32_t* dst, int8_t* sign);
+/* Writes `u v sign` lines (sign 1 or -1): the reference programs' input. */
+int orc_write_edge_text(const char* path, const uint32_t* u, const uint32_t* v, const int8_t* s,
+                        uint64_t m);
+
 #ifdef __cplusplus
 }
 #endif

@@ -34,6 +34,7 @@
 // flight per thread.  Counters: per-thread packed 16-bit fields by number of
 // negative edges, widened into u64 per vertex, then warp shuffle + block
 // reduction and one atomic per counter per CTA.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -1539,46 +1540,104 @@ struct NoAllocScratch {
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
 
-// Input checks on the device: offsets start at 0, never decrease and end at
-// m; every head is below n, above its tail and above the previous head of
-// its list.  Any violation sets ctr[C_ERROR] = kDeviceErrCsr.
-__global__ void k_check_oriented(const uint64_t* __restrict__ off, const uint32_t* __restrict__ heads,
-                                 uint32_t n, uint64_t m, unsigned long long* __restrict__ ctr) {
+// Input checks on the device, in two grid-stride passes with coalesced
+// reads and no per-list loop, so that a long list (a hub keeps its whole
+// degree under an id-ordered orientation) costs no more than other entries.
+// Any violation sets ctr[C_ERROR] = kDeviceErrCsr.
+// Per vertex: offsets start at 0, never decrease and end at m, and the first
+// head of a non-empty list is above its tail.
+__global__ void k_check_offsets(const uint64_t* __restrict__ off, const uint32_t* __restrict__ heads,
+                                uint32_t n, uint64_t m, unsigned long long* __restrict__ ctr) {
   const uint32_t stride = gridDim.x * blockDim.x;
   if (blockIdx.x == 0 && threadIdx.x == 0 && (off[0] != 0 || off[n] != m))
     atomicExch(ctr + C_ERROR, (unsigned long long)kDeviceErrCsr);
   for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += stride) {
     const uint64_t b = off[u], e = off[u + 1];
-    bool bad = e < b || e > m;
-    if (!bad) {
-      uint32_t prev = u;
-      for (uint64_t i = b; i < e; i++) {
-        const uint32_t h = heads[i];
-        if (h >= n || h <= prev) {
-          bad = true;
-          break;
-        }
-        prev = h;
+    const bool bad = e < b || e > m || (e > b && heads[b] <= u);
+    if (bad) atomicExch(ctr + C_ERROR, (unsigned long long)kDeviceErrCsr);
+  }
+}
+
+// Per arc: every head is below n and above the head before it, unless it
+// starts its list (then the pass above compared it with its tail).  Only a
+// head not above its predecessor looks up its list, by a binary search of
+// the offsets: in a valid CSR that happens at most once per list.
+__global__ void k_check_heads(const uint64_t* __restrict__ off, const uint32_t* __restrict__ heads,
+                              uint32_t n, uint64_t m, unsigned long long* __restrict__ ctr) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
+    const uint32_t h = heads[i];
+    bool bad = h >= n;
+    if (!bad && i > 0 && h <= heads[i - 1]) {
+      uint32_t lo = 0, hi = n;  // largest u in [0, n) with off[u] <= i
+      while (hi - lo > 1) {
+        const uint32_t mid = lo + ((hi - lo) >> 1);
+        if (off[mid] <= i) lo = mid; else hi = mid;
       }
+      bad = off[lo] != i;  // i must start the list of u
     }
     if (bad) atomicExch(ctr + C_ERROR, (unsigned long long)kDeviceErrCsr);
   }
 }
 
-std::mutex g_noalloc_mu;
-void* g_noalloc_addr[kNoAllocMaxDevices] = {};
+// The scratch array's device address in the current context.  It is looked
+// up (cudaGetSymbolAddress) once per CUDA context: the first call in a
+// context, with that context current, and again whenever the current
+// context differs from the last one seen on that device, as after
+// cudaDeviceReset or under a caller's own context.  Contexts are told apart
+// by the driver's context id, reached through the runtime's driver entry
+// points (so libstc needs no link to the driver library); without them the
+// address is looked up on every call.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
 
-// Device address of the scratch array on the current device (looked up once
-// per device with that device current).
+std::mutex g_noalloc_mu;
+struct NoAllocSlot {
+  unsigned long long ctx_id = 0;
+  bool valid = false;
+  void* addr = nullptr;
+};
+NoAllocSlot g_noalloc_slot[kNoAllocMaxDevices];
+
+bool current_context_id(unsigned long long* id) {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    cudaDriverEntryPointQueryResult q1 = cudaDriverEntryPointSymbolNotFound, q2 = q1;
+    void* f1 = nullptr;
+    void* f2 = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f1, 12000, cudaEnableDefault, &q1) ==
+            cudaSuccess &&
+        cudaGetDriverEntryPointByVersion("cuCtxGetId", &f2, 12000, cudaEnableDefault, &q2) ==
+            cudaSuccess &&
+        q1 == cudaDriverEntryPointSuccess && q2 == cudaDriverEntryPointSuccess) {
+      get_current = reinterpret_cast<CtxGetCurrentFn>(f1);
+      get_id = reinterpret_cast<CtxGetIdFn>(f2);
+    }
+    (void)cudaGetLastError();
+  }
+  if (!get_current || !get_id) return false;
+  CUcontext cx = nullptr;
+  if (get_current(&cx) != CUDA_SUCCESS || cx == nullptr) return false;
+  return get_id(cx, id) == CUDA_SUCCESS;
+}
+
 cudaError_t noalloc_scratch(int device, NoAllocScratch** out) {
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_addr[device]) {
+  unsigned long long id = 0;
+  const bool have_id = current_context_id(&id);
+  NoAllocSlot& slot = g_noalloc_slot[device];
+  if (!have_id || !slot.valid || slot.ctx_id != id) {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return e;
-    g_noalloc_addr[device] = p;
+    slot.addr = p;
+    slot.ctx_id = id;
+    slot.valid = have_id;
   }
-  *out = static_cast<NoAllocScratch*>(g_noalloc_addr[device]);
+  *out = static_cast<NoAllocScratch*>(slot.addr);
   return cudaSuccess;
 }
 
@@ -1616,7 +1675,8 @@ extern "C" stc_status stc_count_oriented_csr_noalloc(const uint64_t* d_offsets,
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   unsigned long long* ctr = scr->ctr;
   STC_NA(cudaMemsetAsync(ctr, 0, sizeof(scr->ctr), st));
-  k_check_oriented<<<kSMs * 4, 256, 0, st>>>(d_offsets, d_heads, n, m, ctr);
+  k_check_offsets<<<kSMs * 4, 256, 0, st>>>(d_offsets, d_heads, n, m, ctr);
+  if (m) k_check_heads<<<kSMs * 8, 256, 0, st>>>(d_offsets, d_heads, n, m, ctr);
   STC_NA(cudaGetLastError());
   uint64_t slots[C_SLOTS];
   STC_NA(cudaMemcpyAsync(slots, ctr, sizeof(slots), cudaMemcpyDeviceToHost, st));

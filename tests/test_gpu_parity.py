@@ -143,6 +143,23 @@ def test_vertex_counts(ctx):
     np.testing.assert_array_equal(got, want)
 
 
+@pytest.mark.skipif(not oracle.ref_available(), reason="oracle/_ref is not built")
+@pytest.mark.parametrize("family", ["er", "rmat", "skew"])
+def test_vertex_counts_equal_reference_cnt(ctx, family):
+    # The reference's own per-source counts cnt[4n] (tc_serial.cpp:141-158),
+    # taken from its unchanged count_triangles as differences of prefix
+    # counts, against stc_vertex_counts vertex by vertex.
+    if family == "er":
+        el = synth.er(41, 1500, 12000, 0.7)
+    elif family == "rmat":
+        el = synth.rmat(42, 10, 1 << 10, 16 << 10)
+    else:
+        el = synth.skew(43, 1 << 11, 1 << 13, 4, 100, 600, 0.8)
+    with oracle.RefKeptCSR(el.src, el.dst, el.sign) as ref:
+        want = ref.vertex_counts().reshape(-1, 4)
+    np.testing.assert_array_equal(ctx.vertex_counts(el.src, el.dst, el.sign), want)
+
+
 def test_batch_graphs(ctx):
     graphs = [small_graph(f, seed=10 + i) for i, f in enumerate(FAMILIES)]
     got = ctx.count_batch([(g.src, g.dst, g.sign) for g in graphs])

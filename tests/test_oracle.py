@@ -89,3 +89,36 @@ def test_oracle_csr_equals_reference_csr(family):
         assert mine[k] == ref[k]
     for k in ("offsets", "edges", "signs", "fdeg", "rank"):
         np.testing.assert_array_equal(mine[k], ref[k], err_msg=k)
+
+
+@pytest.mark.parametrize("scale,n,samples,p", [(10, 1 << 10, 16 << 10, 0.5),
+                                                (14, 1 << 14, 16 << 14, 0.5),
+                                                (12, 3000, 8 << 12, 0.3)])
+def test_oracle_rmat_generator_equals_package_generator(scale, n, samples, p):
+    # The bench's CPU baseline feeds the reference with the oracle's
+    # generator, which must give the package's edge list bit for bit.
+    el = synth.rmat(1003, scale, n, samples, p_pos=p)
+    src, dst, sign = oracle.synth_rmat(1003, scale, n, samples, p_pos=p)
+    np.testing.assert_array_equal(src, el.src)
+    np.testing.assert_array_equal(dst, el.dst)
+    np.testing.assert_array_equal(sign, el.sign)
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="oracle/_ref not built here")
+@pytest.mark.parametrize("family", ["er", "rmat", "delaunay", "skew"])
+def test_oracle_vertex_counts_equal_reference_cnt(family):
+    # The reference's per-source counts cnt[4n] (tc_serial.cpp:141-158),
+    # recovered from its own count_triangles as differences of prefix counts,
+    # equal the oracle's restatement vertex by vertex.
+    if family == "er":
+        el = synth.er(31, 1500, 12000, 0.7)
+    elif family == "rmat":
+        el = synth.rmat(32, 10, 1 << 10, 16 << 10)
+    elif family == "delaunay":
+        el = synth.delaunay(33, 1500)
+    else:
+        el = synth.skew(34, 1 << 11, 1 << 13, 4, 100, 600, 0.8)
+    with oracle.RefKeptCSR(el.src, el.dst, el.sign) as ref:
+        want = ref.vertex_counts().reshape(-1, 4)
+    got = oracle.ForwardCSR(el.src, el.dst, el.sign).vertex_counts()
+    np.testing.assert_array_equal(got, want)

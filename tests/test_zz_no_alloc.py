@@ -1,4 +1,5 @@
-"""The no-allocation entry point, checked against the regular counting path.
+"""The no-allocation entry point, checked against the regular counting path
+and the oracle, and shown to leave the device's free memory unchanged.
 
 stc_count_oriented_csr_noalloc serves callers that cannot let a library call
 cudaMalloc (they hand out all device memory from their own pool, or run under
@@ -12,6 +13,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
+import oracle
 import signed_triangle_counting_b200 as stc
 from signed_triangle_counting_b200 import _capi, synth
 
@@ -64,15 +66,26 @@ def test_noalloc_matches_regular_path_twice(family):
         el = synth.delaunay(42, 30000, 0.2, 0.6)
     else:
         el = synth.skew(43, 1 << 16, 1 << 17, 4, 3000, 30000, 0.8)
+    import torch
     with stc.Context(0) as ctx:
         want = ctx.count(el.src, el.dst, el.sign).as_tuple()
     assert sum(want) > 0
+    assert want == oracle.count_arrays(el.src, el.dst, el.sign)
     n, offsets, heads, signs = oriented_csr(el)
     d_off, d_heads, d_signs = to_device(offsets, heads, signs)
+    # A first call loads the module and looks up the scratch address; after
+    # it, calls take no device memory: the free memory the driver reports is
+    # the same before and after two more calls.
+    st, got = noalloc_count(n, len(heads), d_off, d_heads, d_signs)
+    assert st == _capi.STC_OK and got == want
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
     for _ in range(2):  # the shared scratch must start clean on every call
         st, got = noalloc_count(n, len(heads), d_off, d_heads, d_signs)
         assert st == _capi.STC_OK
         assert got == want
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free_before
 
 
 def test_noalloc_rejects_bad_input():
