@@ -93,12 +93,19 @@ typedef enum stc_strategy {
   STC_STRATEGY_MERGE = 1,  /* force the warp-cooperative sorted merge */
   STC_STRATEGY_HASH = 2,   /* force the shared-memory hash probe */
   STC_STRATEGY_SEARCH = 3, /* force binary search / galloping */
-  STC_STRATEGY_SPLIT = 4   /* force the sign-split stream: B is read from a copy of the
+  STC_STRATEGY_SPLIT = 4,  /* force the sign-split stream: B is read from a copy of the
                               forward CSR whose lists hold their positive heads, then
                               their negative heads, so a head's sign follows from its
                               position and no sign byte is loaded; each element is
                               probed in the staged hash of N+(u)
                               (MC/tc_merge_sign_split.cpp:20-146, GM/signed_tc.hxx:302-396) */
+  STC_STRATEGY_HEAD = 5    /* force the head-side probe where it applies: the arc u -> v
+                              is counted while the head's list N+(v) is staged as a
+                              shared-memory hash, by streaming A' (the part of N+(u) after
+                              v) through it; the other probe direction of the reference's
+                              hash program, which iterates the shorter list and probes the
+                              other's table (MC/tc_hash_sign_enu.cpp:146-160).  It applies
+                              to arcs with 1 <= |N+(v)| <= 4095; other arcs run HASH */
 } stc_strategy;
 
 typedef enum stc_dispatch {
@@ -300,7 +307,8 @@ stc_status stc_count_batch_packed(stc_ctx* ctx, const uint32_t* src, const uint3
  * all strategies give the same counts, so a table changes only speed. */
 #define STC_DISPATCH_CELLS 1024
 #define STC_DISPATCH_FEATURES 6
-#define STC_DISPATCH_MODEL_PARAMS 180
+#define STC_DISPATCH_STRATEGIES 5
+#define STC_DISPATCH_MODEL_PARAMS 197
 
 /* Timing recorder: the whole path as stc_count (opts->strategy is usually
  * forced to one strategy), with every arc of the staged and giant classes
@@ -324,15 +332,16 @@ stc_status stc_dispatch_features(float* out);
 
 /* Trains the dispatcher's perceptron on the device.  The perceptron has
  * STC_DISPATCH_FEATURES inputs, 16 hidden ReLU units and one output per
- * strategy (MERGE, HASH, SEARCH, SPLIT): the predicted log2 of the SM cycles
- * one arc of the cell costs under that strategy.  Training is full-batch Adam
- * over `samples` rows of `features`, `targets` (samples x 4 measured log2
- * cycles per arc, NaN where a strategy is unavailable) and non-negative
- * `weights`, minimising the weighted squared error plus weight_decay / 2
- * times the squared weights.  Deterministic for a given seed.  `params`
- * receives the STC_DISPATCH_MODEL_PARAMS trained parameters (W1[16][6],
- * b1[16], W2[4][16], b2[4]) and `loss` (optional) the final weighted squared
- * error.  samples <= 4096. */
+ * strategy (STC_DISPATCH_STRATEGIES: MERGE, HASH, SEARCH, SPLIT, HEAD): the
+ * predicted log2 of the SM cycles one arc of the cell costs under that
+ * strategy.  Training is full-batch Adam over `samples` rows of `features`,
+ * `targets` (samples x STC_DISPATCH_STRATEGIES measured log2 cycles per arc,
+ * NaN where a strategy is unavailable) and non-negative `weights`,
+ * minimising the weighted squared error plus weight_decay / 2 times the
+ * squared weights.  Deterministic for a given seed.  `params` receives the
+ * STC_DISPATCH_MODEL_PARAMS trained parameters (W1[16][6], b1[16], W2[5][16],
+ * b2[5]) and `loss` (optional) the final weighted squared error.
+ * samples <= 4096. */
 stc_status stc_dispatcher_train(stc_ctx* ctx, const float* features, const float* targets,
                                 const float* weights, uint32_t samples, uint32_t epochs,
                                 float learning_rate, float weight_decay, uint64_t seed,
@@ -343,7 +352,7 @@ stc_status stc_dispatcher_train(stc_ctx* ctx, const float* features, const float
  * the strategy of least predicted cost where that is predicted at least 5%
  * cheaper than the fixed table's choice, and keeps the fixed choice
  * elsewhere (the giant class, which stages no hash, never gets HASH or
- * SPLIT).  `support` (optional, STC_DISPATCH_CELLS bytes) limits the
+ * SPLIT; HEAD goes only to cells with |B| <= 4095).  `support` (optional, STC_DISPATCH_CELLS bytes) limits the
  * overrides to the cells marked non-zero, normally the cells the model's
  * training data covered, so that the model is not trusted where it would
  * extrapolate; NULL allows them everywhere.  Calls with dispatch

@@ -433,7 +433,7 @@ class Context:
                          weight_decay=1e-3, seed=1):
         """Trains the dispatcher's perceptron on the device: features
         (samples, DISPATCH_FEATURES), targets (samples, DISPATCH_OUTPUTS)
-        measured log2 cycles per arc of MERGE / HASH / SEARCH / SPLIT (NaN =
+        measured log2 cycles per arc of MERGE / HASH / SEARCH / SPLIT / HEAD (NaN =
         unavailable), weights
         (samples,).  Returns (parameters, final weighted squared error)."""
         X = np.ascontiguousarray(features, np.float32)

@@ -79,11 +79,11 @@ STC_ERR_DEVICE_TIMEOUT = 6
 STC_ERR_NO_DEVICE = 7
 STC_ERR_INTERNAL = 8
 
-STRATEGY = {"auto": 0, "merge": 1, "hash": 2, "search": 3, "split": 4}
+STRATEGY = {"auto": 0, "merge": 1, "hash": 2, "search": 3, "split": 4, "head": 5}
 DISPATCH_CELLS = 1024
 DISPATCH_FEATURES = 6
-DISPATCH_MODEL_PARAMS = 180
-DISPATCH_OUTPUTS = 4  # merge, hash, search, split
+DISPATCH_MODEL_PARAMS = 197
+DISPATCH_OUTPUTS = 5  # merge, hash, search, split, head
 DISPATCH = {"fixed": 0, "learned": 1}
 F_DEVICE_INPUT = 0x1
 F_TIMING = 0x2

@@ -214,11 +214,13 @@ struct EmitOffset {
   __device__ void operator()(uint64_t i, uint64_t pos, uint32_t) const { off[i] = pos; }
 };
 
-// Splits sorted arc keys into the neighbour and sign arrays and accumulates
-// the merge-model byte count 5 (d+(u) + d+(v)) + 25 per arc.
+// Splits sorted arc keys into the neighbour, sign and tail arrays (the tail
+// array only when `asrc` is given) and accumulates the merge-model byte count
+// 5 (d+(u) + d+(v)) + 25 per arc.
 __global__ void k_csr_fill(const uint64_t* __restrict__ akeys, uint64_t ma, uint32_t bits,
                            const uint32_t* __restrict__ fdeg, uint32_t* __restrict__ nbr,
-                           int8_t* __restrict__ sgn, unsigned long long* __restrict__ ctr) {
+                           int8_t* __restrict__ sgn, uint32_t* __restrict__ asrc,
+                           unsigned long long* __restrict__ ctr) {
   const uint64_t idmask = (1ull << bits) - 1;
   unsigned long long bytes = 0;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
@@ -227,6 +229,7 @@ __global__ void k_csr_fill(const uint64_t* __restrict__ akeys, uint64_t ma, uint
     const uint32_t src = (uint32_t)((k >> bits) & idmask), dst = (uint32_t)(k & idmask);
     nbr[i] = dst;
     sgn[i] = (k >> 63) ? (int8_t)-1 : (int8_t)1;
+    if (asrc) asrc[i] = src;
     bytes += 5ull * ((unsigned long long)fdeg[src] + fdeg[dst]) + 25ull;
   }
   bytes = warp_sum(bytes);
@@ -288,8 +291,10 @@ void finish_csr_from_arc_keys(stc_ctx* c, DeviceGraph& g, uint64_t* akeys, uint6
                            sizeof(uint64_t), cudaMemcpyDeviceToDevice, c->stream));
   g.nbr = buffer<uint32_t>(c, B_NBR, g.m_fwd + 4);  // + 4: the engine reads whole int4 chunks
   g.sgn = buffer<int8_t>(c, B_SGN, g.m_fwd + 4);
+  g.asrc = buffer<uint32_t>(c, B_ASRC, g.m_fwd);
   k_csr_fill<<<grid_for(g.m_fwd, 4), kThreads, 0, c->stream>>>(sorted, g.m_fwd, g.bits, g.fdeg,
-                                                               g.nbr, g.sgn, (unsigned long long*)counters(c));
+                                                               g.nbr, g.sgn, g.asrc,
+                                                               (unsigned long long*)counters(c));
   c->launches += 1;
   STC_CUDA(cudaGetLastError());
 }
@@ -380,10 +385,278 @@ __global__ void k_batch_vertex_graph(uint64_t* __restrict__ vkeys, uint32_t n,
   }
 }
 
+// ------------------------------------------------------- totals path ----
+// A count of totals needs an acyclic orientation, not the reference's: every
+// total order of the vertices counts each triangle once, from its lowest
+// vertex.  So the totals path orders vertices by (degree counted over the
+// input's edge copies, id) instead of (unique degree, id), which needs no
+// dedup before the orientation: the arc sort that builds the CSR brings the
+// copies of an edge together, and the first of each run is kept, the
+// dedup's own rule (the sort is stable, so it is the first in input order).
+// This removes the dedup sort of all input edges.
+
+// Global ids of input edge i: the edge's own ids, plus the vertex base of
+// its graph for a batch (found once per thread by a binary search, then by
+// a cursor that only moves forward, as every thread's indices grow).
+struct EdgeIds {
+  const uint32_t* __restrict__ u;
+  const uint32_t* __restrict__ v;
+  const uint64_t* __restrict__ eoff;   // G + 1 edge offsets, or null for one graph
+  const uint64_t* __restrict__ vbase;  // G + 1 vertex bases
+  uint32_t G;
+};
+
+struct EdgeCursor {
+  uint32_t g = 0;
+  __device__ void start(const EdgeIds& e, uint64_t i) {
+    if (e.eoff) g = first_segment(e.eoff, e.G, i);
+  }
+  __device__ void at(const EdgeIds& e, uint64_t i, uint32_t& a, uint32_t& b) {
+    a = e.u[i];
+    b = e.v[i];
+    if (e.eoff) {
+      while (e.eoff[g + 1] <= i) g++;
+      const uint32_t base = (uint32_t)e.vbase[g];
+      a += base;
+      b += base;
+    }
+  }
+};
+
+// Degree of every vertex over the input's edge copies (self-loops skipped).
+// Endpoints are scattered and a few hubs own millions of copies, so each CTA
+// first adds them in a shared-memory table per tile of kRawTile edges and
+// flushes the slots it used with one global atomic each (an endpoint that
+// finds no free slot within kDegProbes probes is added directly).
+constexpr int kRawTile = 512;
+constexpr int kRawSlots = 2048;  // 2 kRawTile endpoints per tile: load <= 1/2
+
+__global__ void __launch_bounds__(kThreads) k_degree_raw(EdgeIds e, uint64_t m, uint64_t per_cta,
+                                                         uint32_t* __restrict__ deg) {
+  __shared__ uint32_t tkey[kRawSlots], tcnt[kRawSlots], used[kRawSlots];
+  __shared__ uint32_t nused;
+  constexpr uint32_t kFree = 0xFFFFFFFFu;
+  for (int i = threadIdx.x; i < kRawSlots; i += kThreads) {
+    tkey[i] = kFree;
+    tcnt[i] = 0;
+  }
+  if (threadIdx.x == 0) nused = 0;
+  __syncthreads();
+  const uint64_t begin = (uint64_t)blockIdx.x * per_cta;
+  const uint64_t end = begin + per_cta < m ? begin + per_cta : m;
+  EdgeCursor cur;
+  if (begin < end) cur.start(e, begin);
+  for (uint64_t t = begin; t < end; t += kRawTile) {
+#pragma unroll
+    for (int r = 0; r < kRawTile / kThreads; r++) {
+      const uint64_t i = t + (uint64_t)r * kThreads + threadIdx.x;
+      uint32_t a = kFree, b = kFree;
+      if (i < end) {
+        cur.at(e, i, a, b);
+        if (a == b) a = b = kFree;
+      }
+#pragma unroll
+      for (int side = 0; side < 2; side++) {
+        const uint32_t x = side ? b : a;
+        const unsigned px = __match_any_sync(kFull, x);
+        if (x != kFree && (px & lanemask_lt()) == 0) {
+          const uint32_t add = (uint32_t)__popc(px);
+          uint32_t slot = (x * 0x9E3779B1u) >> (32 - 11);
+          bool placed = false;
+          for (int p = 0; p < kDegProbes && !placed; p++) {
+            uint32_t c = tkey[slot];
+            if (c == kFree) {  // claim the slot, or see who claimed it first
+              const uint32_t old = atomicCAS(&tkey[slot], kFree, x);
+              if (old == kFree) used[atomicAdd(&nused, 1u)] = slot;
+              c = old == kFree ? x : old;
+            }
+            if (c == x) {
+              atomicAdd(&tcnt[slot], add);
+              placed = true;
+            }
+            slot = (slot + 1) & (kRawSlots - 1);
+          }
+          if (!placed) atomicAdd(deg + x, add);
+        }
+      }
+    }
+    __syncthreads();
+    const uint32_t nu = nused;
+    for (uint32_t j = threadIdx.x; j < nu; j += kThreads) {
+      const uint32_t slot = used[j];
+      atomicAdd(deg + tkey[slot], tcnt[slot]);
+      tkey[slot] = kFree;
+      tcnt[slot] = 0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) nused = 0;
+    __syncthreads();
+  }
+}
+
+// Arc keys of the input's edge copies in rank space: (rank lo << bits |
+// rank hi), the negative flag in bit 63; a self-loop becomes the all-ones
+// sentinel of the 2 * bits window, which sorts after every real key.
+__global__ void k_arc_keys_raw(EdgeIds e, const int8_t* __restrict__ sign, uint64_t m,
+                               uint64_t per_cta, uint32_t bits, const uint32_t* __restrict__ rank,
+                               uint64_t* __restrict__ akeys) {
+  const uint64_t sentinel = (bits * 2 >= 64) ? ~0ull >> 1 : ((1ull << (2 * bits)) - 1);
+  const uint64_t begin = (uint64_t)blockIdx.x * per_cta;
+  const uint64_t end = begin + per_cta < m ? begin + per_cta : m;
+  if (begin >= end) return;
+  EdgeCursor cur;
+  cur.start(e, begin);
+  for (uint64_t i = begin + threadIdx.x; i < end; i += blockDim.x) {
+    uint32_t a, b;
+    cur.at(e, i, a, b);
+    uint64_t k = sentinel;
+    if (a != b) {
+      const uint32_t ra = rank[a], rb = rank[b];
+      k = ((uint64_t)min(ra, rb) << bits) | max(ra, rb) | ((uint64_t)(sign[i] < 0) << 63);
+    }
+    akeys[i] = k;
+  }
+}
+
+// The first key of each run of equal (lo, hi) in the sorted arc keys becomes
+// arc `pos` of the CSR: head, sign and tail.
+struct EmitArc {
+  const uint64_t* keys;
+  uint32_t bits;
+  uint32_t* nbr;
+  int8_t* sgn;
+  uint32_t* asrc;
+  __device__ void operator()(uint64_t i, uint64_t pos, uint32_t flag) const {
+    if (!flag) return;
+    const uint64_t k = keys[i];
+    const uint64_t idmask = (1ull << bits) - 1;
+    nbr[pos] = (uint32_t)(k & idmask);
+    sgn[pos] = (k >> 63) ? (int8_t)-1 : (int8_t)1;
+    asrc[pos] = (uint32_t)((k >> bits) & idmask);
+  }
+};
+
+// Out-degree of every tail from the sorted arcs: lanes take consecutive
+// arcs, so a warp adds each run of equal tails with one atomic.
+__global__ void k_fdeg_count(const uint32_t* __restrict__ asrc, uint64_t m,
+                             uint32_t* __restrict__ fdeg) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < m;
+       base += stride) {
+    const uint64_t p = base + lane_id();
+    const uint32_t t = p < m ? asrc[p] : 0xFFFFFFFFu;
+    const unsigned peers = __match_any_sync(kFull, t);
+    if (p < m && (peers & lanemask_lt()) == 0) atomicAdd(fdeg + t, (uint32_t)__popc(peers));
+  }
+}
+
+// The merge-model byte count 5 (d+(u) + d+(v)) + 25 per arc.
+__global__ void k_alg_bytes(const uint32_t* __restrict__ asrc, const uint32_t* __restrict__ nbr,
+                            uint64_t m, const uint32_t* __restrict__ fdeg,
+                            unsigned long long* __restrict__ ctr) {
+  unsigned long long bytes = 0;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride)
+    bytes += 5ull * ((unsigned long long)fdeg[asrc[i]] + fdeg[nbr[i]]) + 25ull;
+  bytes = warp_sum(bytes);
+  if (lane_id() == 0 && bytes) atomicAdd(ctr + C_ALG_BYTES, bytes);
+}
+
+// Steps 2-6 of the totals path, after the ids (g.n, g.bits, g.m_valid set):
+// degrees over the edge copies, (degree, id) rank (graph-major for a batch
+// with vertex bases d_vbase), arc keys of every copy, their sort, the first
+// of each run of equal arcs, offsets.  g.ukeys stays null.
+void build_totals(stc_ctx* c, const EdgeIds& e, const int8_t* d_sign, uint64_t m, DeviceGraph& g,
+                  const uint64_t* d_vbase, uint32_t G) {
+  cudaStream_t st = c->stream;
+  unsigned long long* ctr = (unsigned long long*)counters(c);
+  uint32_t* sort_counts = buffer<uint32_t>(c, B_SORT_COUNTS, (size_t)kRadix * kMaxSortGrid);
+  uint64_t* sums = buffer<uint64_t>(c, B_SCAN_SUMS, kMaxSortGrid + 1);
+  g.ukeys = nullptr;
+  g.deg = buffer<uint32_t>(c, B_DEG, g.n);
+  g.rank = buffer<uint32_t>(c, B_RANK, g.n);
+  g.verts = buffer<uint32_t>(c, B_VERTS, g.n);
+  g.fdeg = buffer<uint32_t>(c, B_FDEG, g.n);
+  const RangePartition ep = range_partition(m, kSortTile, kMaxSortGrid);
+  if (g.n) {
+    STC_CUDA(cudaMemsetAsync(g.deg, 0, (size_t)g.n * sizeof(uint32_t), st));
+    STC_CUDA(cudaMemsetAsync(g.fdeg, 0, (size_t)g.n * sizeof(uint32_t), st));
+  }
+  if (g.m_valid) {
+    k_degree_raw<<<ep.grid, kThreads, 0, st>>>(e, m, ep.per_cta, g.deg);
+    c->launches++;
+  }
+  STC_CUDA(cudaGetLastError());
+  mark(c, 2);
+
+  if (g.n) {
+    uint64_t* va = buffer<uint64_t>(c, B_VKEYS_A, g.n);
+    uint64_t* vb = buffer<uint64_t>(c, B_VKEYS_B, g.n);
+    k_vertex_keys<<<grid_for(g.n, 4), kThreads, 0, st>>>(g.deg, g.n, va, ctr);
+    c->launches++;
+    read_counters(c, C_MAX_DEG, 1);
+    g.max_deg = (uint32_t)c->h_pinned[C_MAX_DEG];
+    const int dbits = (int)bit_width64(g.max_deg);
+    const int gbits = d_vbase ? (int)bit_width64(G > 1 ? G - 1 : 0) : 0;
+    if (32 + dbits + gbits > 64) fail(STC_ERR_LIMIT, "batch too large for the vertex sort key");
+    if (gbits) {
+      const RangePartition vp = range_partition(g.n, kSortTile, kMaxSortGrid);
+      k_batch_vertex_graph<<<vp.grid, kThreads, 0, st>>>(va, g.n, d_vbase, G, vp.per_cta,
+                                                         32 + dbits);
+      c->launches++;
+    }
+    uint64_t* vs = radix_sort(va, vb, g.n, 32, 32 + dbits + gbits, sort_counts, st, &c->launches);
+    k_rank<<<grid_for(g.n, 4), kThreads, 0, st>>>(vs, g.n, g.verts, g.rank);
+    c->launches++;
+  }
+  STC_CUDA(cudaGetLastError());
+  mark(c, 3);
+
+  g.m_unique = g.m_fwd = 0;
+  if (g.m_valid) {
+    uint64_t* ka = buffer<uint64_t>(c, B_KEYS_A, m);
+    uint64_t* kb = buffer<uint64_t>(c, B_KEYS_B, m);
+    k_arc_keys_raw<<<ep.grid, kThreads, 0, st>>>(e, d_sign, m, ep.per_cta, g.bits, g.rank, ka);
+    c->launches++;
+    uint64_t* sorted = radix_sort(ka, kb, m, 0, 2 * (int)g.bits, sort_counts, st, &c->launches);
+    // Self-loops sorted last: the first m_valid keys are the real arcs.
+    const UniqueFlag flag{sorted, (1ull << (2 * g.bits)) - 1};
+    const uint32_t grid = range_reduce_scan(flag, g.m_valid, sums, st, &c->launches);
+    STC_CUDA(cudaMemcpyAsync(c->h_pinned + C_WORK, sums + grid, sizeof(uint64_t),
+                             cudaMemcpyDeviceToHost, st));
+    STC_CUDA(cudaStreamSynchronize(st));
+    g.m_unique = g.m_fwd = c->h_pinned[C_WORK];
+    g.nbr = buffer<uint32_t>(c, B_NBR, g.m_fwd + 4);  // + 4: the engine reads whole int4 chunks
+    g.sgn = buffer<int8_t>(c, B_SGN, g.m_fwd + 4);
+    g.asrc = buffer<uint32_t>(c, B_ASRC, g.m_fwd);
+    range_apply(flag, EmitArc{sorted, g.bits, g.nbr, g.sgn, g.asrc}, g.m_valid, sums, st,
+                &c->launches);
+    k_fdeg_count<<<grid_for(g.m_fwd, 4), kThreads, 0, st>>>(g.asrc, g.m_fwd, g.fdeg);
+    c->launches++;
+  }
+  g.off = buffer<uint64_t>(c, B_OFF, (size_t)g.n + 1);
+  if (g.n) {
+    range_scan(LoadU32{g.fdeg}, EmitOffset{g.off}, g.n, sums, st, &c->launches);
+    STC_CUDA(cudaMemcpyAsync(g.off + g.n, sums + range_partition(g.n, kScanTile, kMaxSortGrid).grid,
+                             sizeof(uint64_t), cudaMemcpyDeviceToDevice, st));
+  } else {
+    STC_CUDA(cudaMemsetAsync(g.off, 0, sizeof(uint64_t), st));
+  }
+  if (g.m_fwd) {
+    k_alg_bytes<<<grid_for(g.m_fwd, 4), kThreads, 0, st>>>(g.asrc, g.nbr, g.m_fwd, g.fdeg, ctr);
+    c->launches++;
+  } else {
+    g.nbr = buffer<uint32_t>(c, B_NBR, 4);
+    g.sgn = buffer<int8_t>(c, B_SGN, 4);
+  }
+  STC_CUDA(cudaGetLastError());
+  mark(c, 4);
+}
+
 }  // namespace
 
 void build_graph(stc_ctx* c, const uint32_t* d_src, const uint32_t* d_dst, const int8_t* d_sign,
-                 uint64_t m, DeviceGraph& g) {
+                 uint64_t m, DeviceGraph& g, bool totals) {
   cudaStream_t st = c->stream;
   unsigned long long* ctr = (unsigned long long*)counters(c);
   g = DeviceGraph{};
@@ -405,6 +678,10 @@ void build_graph(stc_ctx* c, const uint32_t* d_src, const uint32_t* d_dst, const
   g.n = m ? (uint32_t)max_id + 1 : 0;
   g.m_valid = m - self;
   g.bits = std::max<uint32_t>(1, bit_width64(max_id));
+  if (totals) {
+    build_totals(c, EdgeIds{d_src, d_dst, nullptr, nullptr, 0}, d_sign, m, g, nullptr, 0);
+    return;
+  }
   uint32_t* sort_counts = buffer<uint32_t>(c, B_SORT_COUNTS, (size_t)kRadix * kMaxSortGrid);
   uint64_t* sums = buffer<uint64_t>(c, B_SCAN_SUMS, kMaxSortGrid + 1);
 
@@ -509,7 +786,7 @@ void graph_from_forward_csr(stc_ctx* c, uint32_t n, uint64_t m, const uint64_t* 
 
 void build_graph_batch(stc_ctx* c, const uint32_t* d_src, const uint32_t* d_dst,
                        const int8_t* d_sign, uint64_t m, const uint64_t* h_eoff, uint32_t G,
-                       DeviceGraph& g) {
+                       DeviceGraph& g, bool totals) {
   cudaStream_t st = c->stream;
   unsigned long long* ctr = (unsigned long long*)counters(c);
   g = DeviceGraph{};
@@ -543,6 +820,10 @@ void build_graph_batch(stc_ctx* c, const uint32_t* d_src, const uint32_t* d_dst,
   g.m_valid = m - c->h_pinned[C_SELF];
   g.bits = std::max<uint32_t>(1, bit_width64(ntot ? ntot - 1 : 0));
   g.gbase = d_vbase;
+  if (totals) {
+    build_totals(c, EdgeIds{d_src, d_dst, d_eoff, d_vbase, G}, d_sign, m, g, d_vbase, G);
+    return;
+  }
   uint32_t* sort_counts = buffer<uint32_t>(c, B_SORT_COUNTS, (size_t)kRadix * kMaxSortGrid);
   uint64_t* sums = buffer<uint64_t>(c, B_SCAN_SUMS, kMaxSortGrid + 1);
 
@@ -641,7 +922,7 @@ void export_forward_csr(stc_ctx* c, const DeviceGraph& g, stc_forward_csr* out) 
   }
   if (mu) {
     k_csr_fill<<<grid_for(mu, 4), kThreads, 0, st>>>(sorted, mu, g.bits, fdeg_id, edges, signs,
-                                                     (unsigned long long*)counters(c));
+                                                     nullptr, (unsigned long long*)counters(c));
   }
   STC_CUDA(cudaGetLastError());
   out->n = n;

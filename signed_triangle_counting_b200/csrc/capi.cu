@@ -135,7 +135,7 @@ constexpr uint64_t kBatchGroupEdges = 1536ull << 20;
 CountConfig count_config(const stc_opts* o) {
   CountConfig cfg;
   if (o) {
-    if (o->strategy > STC_STRATEGY_SPLIT) fail(STC_ERR_INVALID_ARGUMENT, "unknown strategy");
+    if (o->strategy > STC_STRATEGY_HEAD) fail(STC_ERR_INVALID_ARGUMENT, "unknown strategy");
     if (o->dispatch > STC_DISPATCH_LEARNED) fail(STC_ERR_INVALID_ARGUMENT, "unknown dispatch");
     cfg.strategy = o->strategy;
     cfg.dispatch = o->dispatch;
@@ -261,7 +261,7 @@ stc_status stc_count(stc_ctx* c, const uint32_t* src, const uint32_t* dst, const
     begin_call(c, o);
     DeviceInput in = stage_input(c, src, dst, sign, m, o);
     DeviceGraph g;
-    build_graph(c, in.src, in.dst, in.sign, m, g);
+    build_graph(c, in.src, in.dst, in.sign, m, g, /*totals=*/true);
     count_triangles(c, g, cfg);
     mark(c, 5);
     end_call(c, g, out);
@@ -328,7 +328,7 @@ stc_status stc_count_text(stc_ctx* c, const char* data, uint64_t size, const stc
     uint32_t n = 0;
     const uint64_t m = stage_and_parse_text(c, data, size, o, &in, &lines, &n);
     DeviceGraph g;
-    build_graph(c, in.src, in.dst, in.sign, m, g);
+    build_graph(c, in.src, in.dst, in.sign, m, g, /*totals=*/true);
     count_triangles(c, g, cfg);
     mark(c, 5);
     end_call(c, g, out);
@@ -497,7 +497,7 @@ stc_status stc_count_batch_packed(stc_ctx* c, const uint32_t* src, const uint32_
         in = stage_input(c, src + e0, dst + e0, sign + e0, me, o);
       }
       DeviceGraph g;
-      build_graph_batch(c, in.src, in.dst, in.sign, me, eoff.data(), gn, g);
+      build_graph_batch(c, in.src, in.dst, in.sign, me, eoff.data(), gn, g, /*totals=*/true);
       uint64_t* gc = buffer<uint64_t>(c, B_BATCH_COUNTS, 4ull * gn);
       STC_CUDA(cudaMemsetAsync(gc, 0, 4ull * gn * sizeof(uint64_t), c->stream));
       cfg.graph_counts = gc;

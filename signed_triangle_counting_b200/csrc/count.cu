@@ -283,7 +283,8 @@ __device__ __forceinline__ void stage(const Csr& g, uint64_t ub, uint32_t d, uin
            atomicCAS(&m.hk[2 * b + 1], kEmpty, key) != kEmpty)
       b = (b + 1) & (geo.nb - 1);
     const uint32_t blen = m.hi[i] - m.lo[i];
-    const uint8_t st = (i + 1 < d && blen) ? table[size_bucket(d - i - 1)][size_bucket(blen)] : kNoArc;
+    uint8_t st = (i + 1 < d && blen) ? table[size_bucket(d - i - 1)][size_bucket(blen)] : kNoArc;
+    if (st == STC_STRATEGY_HEAD) st = kNoArc;  // counted by the head-side pass
     m.st[i] = st;
     if (st == STC_STRATEGY_SPLIT) m.sp[i] = m.lo[i] + g.psplit[x];
   }
@@ -724,16 +725,19 @@ __device__ __forceinline__ void source_range(const unsigned long long* range, ui
   u1 = range ? (uint32_t)range[1] : n;
 }
 
+// `need` (optional): a vertex whose flag is 0 has no arc for the tail side
+// (the head-side pass counts all of them) and joins no class.
 __global__ void k_classify_count(const uint64_t* __restrict__ off, uint32_t n, ClassBounds cb,
                                  unsigned long long* __restrict__ ctr,
-                                 const unsigned long long* __restrict__ range) {
+                                 const unsigned long long* __restrict__ range,
+                                 const uint8_t* __restrict__ need = nullptr) {
   uint32_t cnt[kClasses] = {0, 0, 0, 0, 0};
   uint32_t dmax = 0;
   uint32_t u0, u1;
   source_range(range, n, u0, u1);
   for (uint32_t u = u0 + blockIdx.x * blockDim.x + threadIdx.x; u < u1; u += gridDim.x * blockDim.x) {
     const uint32_t d = (uint32_t)(off[u + 1] - off[u]);
-    const uint32_t c = cb.of(d);
+    const uint32_t c = (need && !need[u]) ? 5u : cb.of(d);
     dmax = max(dmax, d);
 #pragma unroll
     for (int i = 0; i < kClasses; i++) cnt[i] += c == (uint32_t)i;
@@ -752,13 +756,14 @@ __global__ void k_classify_count(const uint64_t* __restrict__ off, uint32_t n, C
 __global__ void k_classify_fill(const uint64_t* __restrict__ off, uint32_t n, ClassBounds cb,
                                 uint32_t* __restrict__ lists, const uint32_t* __restrict__ starts,
                                 unsigned long long* __restrict__ cursor,
-                                const unsigned long long* __restrict__ range) {
+                                const unsigned long long* __restrict__ range,
+                                const uint8_t* __restrict__ need = nullptr) {
   uint32_t u0, u1;
   source_range(range, n, u0, u1);
   for (uint32_t base = u0 + blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < u1;
        base += gridDim.x * blockDim.x) {
     const uint32_t u = base + lane_id();
-    const uint32_t c = u < u1 ? cb.of((uint32_t)(off[u + 1] - off[u])) : 5u;
+    const uint32_t c = (u >= u1 || (need && !need[u])) ? 5u : cb.of((uint32_t)(off[u + 1] - off[u]));
     const unsigned peers = __match_any_sync(kFull, c);
     const uint32_t leader = __ffs(peers) - 1;
     uint32_t pos = 0;
@@ -770,10 +775,11 @@ __global__ void k_classify_fill(const uint64_t* __restrict__ off, uint32_t n, Cl
 
 // Tiny class: one thread per vertex, A in registers, B in global memory.
 // One tiny list (one thread): A in registers, a monotone binary search of
-// each later A' element in B.
+// each later A' element in B; arcs whose cell in `table` (the warp class's)
+// is HEAD are left to the head-side pass.
 template <int TMAX, class Sink>
 __device__ __forceinline__ void tiny_vertex(const Csr& g, uint32_t u, const Sink& sink,
-                                            TypeCounts& tc) {
+                                            const uint8_t (*table)[16], TypeCounts& tc) {
   constexpr bool kVC = Sink::kPerVertex;
   const uint64_t ub = g.off[u];
   const uint32_t d = (uint32_t)(g.off[u + 1] - ub);
@@ -790,6 +796,7 @@ __device__ __forceinline__ void tiny_vertex(const Csr& g, uint32_t u, const Sink
     if (k + 1 >= (int)d) break;
     const uint64_t vb = g.off[a[k]];
     const uint32_t blen = (uint32_t)(g.off[a[k] + 1] - vb);
+    if (table[size_bucket(d - k - 1)][size_bucket(blen)] == STC_STRATEGY_HEAD) continue;
     const uint32_t* b = g.nbr + vb;
     uint32_t pos = 0;
 #pragma unroll
@@ -809,10 +816,14 @@ __device__ __forceinline__ void tiny_vertex(const Csr& g, uint32_t u, const Sink
 // Tiny class: one thread per vertex, A in registers, B in global memory.
 template <int TMAX, class Sink>
 __global__ void __launch_bounds__(256) k_tiny(Csr g, const uint32_t* __restrict__ list, uint32_t cnt,
-                                              unsigned long long* __restrict__ ctr, Sink sink) {
+                                              unsigned long long* __restrict__ ctr, Sink sink,
+                                              const uint8_t* __restrict__ gtable) {
+  __shared__ uint8_t table[16][16];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) (&table[0][0])[i] = gtable[i];
+  __syncthreads();
   TypeCounts tc;
   for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < cnt; idx += gridDim.x * blockDim.x)
-    tiny_vertex<TMAX>(g, list[idx], sink, tc);
+    tiny_vertex<TMAX>(g, list[idx], sink, table, tc);
   if (!Sink::kPerVertex) flush_counts<256>(tc, ctr);
 }
 
@@ -987,6 +998,7 @@ __global__ void __launch_bounds__(THREADS) k_giant(Csr g, const uint32_t* __rest
       const uint32_t blen = (uint32_t)(g.off[v + 1] - vb);
       if (blen == 0) continue;
       const uint32_t st = table[size_bucket(d - k - 1)][size_bucket(blen)];
+      if (st == STC_STRATEGY_HEAD) continue;  // counted by the head-side pass
       long long t0 = 0;
       if (kTime) {
         __syncwarp();
@@ -1045,7 +1057,8 @@ void launch_classes(cudaStream_t st, const Csr& csr, const uint32_t* lists, cons
                     const Tuning& tu, uint32_t mask, int& launches) {
   if (counts[0] && (mask & 1u)) {
     const uint32_t grid = std::min<uint32_t>((counts[0] + 255) / 256, kSMs * 8);
-    k_tiny<kTinyMax, Sink><<<grid, 256, 0, st>>>(csr, lists + starts[0], counts[0], ctr, sink);
+    k_tiny<kTinyMax, Sink><<<grid, 256, 0, st>>>(csr, lists + starts[0], counts[0], ctr, sink,
+                                                  d_tables + 256 * kTableWarp);
     launches++;
   }
   if (counts[1] && (mask & 2u)) {
@@ -1119,6 +1132,443 @@ void launch_classes(cudaStream_t st, const Csr& csr, const uint32_t* lists, cons
   }
 }
 
+// ------------------------------------------------------- head side ----
+// Arcs whose dispatch cell says STC_STRATEGY_HEAD are counted from their
+// head.  For the arc u -> v, the third vertex w of a triangle lies in
+// A' = the part of N+(u) after v and in B = N+(v).  The tail side (the
+// kernels above) stages N+(u) and streams B; the head side stages N+(v) as
+// the shared-memory hash and streams A' through it, so an arc costs |A'|
+// probes instead of |B|.  Over a power-law graph in (degree, id) order,
+// A' is the shorter list for almost every arc (the reference's hash
+// program iterates the shorter of its two lists for the same reason,
+// MC/tc_hash_sign_enu.cpp:146-160).
+//
+// The head side finds each vertex's in-arcs by a sort: every HEAD arc i
+// (its index in the CSR) becomes the key v << 32 | i, every other arc the
+// sentinel, whose vertex field (all ones) is above every real head's (the
+// last vertex in rank order has no out-arcs, so no HEAD arc ends there); a
+// stable radix sort over the vertex bits groups each head's in-arcs, and
+// the runs of equal v are its in-arc ranges.  Head vertices are classed by
+// |N+(v)|, the list they stage: warp (<= 128), block (<= 1024) and large
+// (<= 4095).  Each in-arc is one "arc" of the staged tile with extent
+// [i + 1, end of u's list), its sign s(u, v), strategy HASH: the tail
+// side's stream pass then runs unchanged, with the hash keys carrying
+// s(v, w), the streamed sign bytes s(u, w) and the arc's sign s(u, v).
+constexpr uint32_t kHeadMaxB = kLargeCap - 1;  // |N+(v)| of a HEAD arc: bucket <= 12
+static_assert(32 - __builtin_clz(kHeadMaxB) == 12 && 32 - __builtin_clz(kHeadMaxB + 1) == 13,
+              "HEAD cells (bucket |B| <= 12) are exactly the arcs whose head fits the large class");
+constexpr int kHeadClasses = 3;
+// Head list buffer: plan words first (start of class c's list, then from
+// kHeadPlanCount its count), the class lists after them, then one byte per
+// vertex: whether it keeps arcs for the tail side.
+constexpr uint32_t kHeadPlanCount = 4;
+constexpr uint32_t kHeadPlanWords = 8;
+
+// Table class of a list of d arcs (tiny lists use the warp class's table).
+__device__ __forceinline__ uint32_t table_class(uint32_t d) {
+  return d <= kWarpCap ? kTableWarp : d <= kBlockCap ? kTableBlock
+                                    : d <= kLargeCap ? kTableLarge : kTableGiant;
+}
+// Head class of a head vertex with d = |N+(v)| in [1, kHeadMaxB].
+__device__ __forceinline__ uint32_t head_class(uint32_t d) {
+  return d <= kWarpCap ? 0u : d <= kBlockCap ? 1u : 2u;
+}
+
+struct HeadArcs {
+  const uint64_t* __restrict__ keys;  // sorted: v << 32 | arc index
+  const uint32_t* __restrict__ aend;  // per arc: end of its tail's list in the CSR
+  const uint32_t* __restrict__ beg;   // per head vertex: its first in-arc entry
+  const uint32_t* __restrict__ end;   // ... and one past its last
+  const uint32_t* __restrict__ asrc;  // per arc: its tail (timing recorder only)
+};
+
+// Keys of the HEAD arcs (and sentinels), every arc's list end, and need[u]
+// = 1 for each tail u with an arc left to the tail side (the array starts at
+// 0; tails without such arcs are not staged there).  `range` (a sharded
+// count) keeps only tails in [range[0], range[1]).
+__global__ void __launch_bounds__(256) k_head_keys(Csr g, const uint32_t* __restrict__ asrc,
+                                                   uint64_t m, const uint8_t* __restrict__ gtables,
+                                                   uint32_t vbits,
+                                                   const unsigned long long* __restrict__ range,
+                                                   uint64_t* __restrict__ keys,
+                                                   uint32_t* __restrict__ aend,
+                                                   uint8_t* __restrict__ need) {
+  __shared__ uint8_t tab[kTableBytes];
+  for (uint32_t i = threadIdx.x; i < kTableBytes; i += blockDim.x) tab[i] = gtables[i];
+  __syncthreads();
+  const uint64_t sentinel = ((1ull << vbits) - 1) << 32;
+  const uint32_t r0 = range ? (uint32_t)range[0] : 0u;
+  const uint32_t r1 = range ? (uint32_t)range[1] : 0xFFFFFFFFu;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
+    const uint32_t u = asrc[i], v = g.nbr[i];
+    const uint64_t ub = g.off[u], ue = g.off[u + 1];
+    const uint32_t alen = (uint32_t)(ue - i - 1);
+    const uint32_t blen = (uint32_t)(g.off[v + 1] - g.off[v]);
+    bool head = false;
+    if (alen && blen && u >= r0 && u < r1) {
+      head = tab[256 * table_class((uint32_t)(ue - ub)) + 16 * size_bucket(alen) +
+                 size_bucket(blen)] == STC_STRATEGY_HEAD;
+      if (!head) need[u] = 1;  // u keeps an arc for the tail side
+    }
+    keys[i] = head ? (((uint64_t)v << 32) | i) : sentinel;
+    aend[i] = (uint32_t)ue;
+  }
+}
+
+// Runs of equal head vertex in the sorted keys.  Without kFill: counts the
+// head vertices of each class.  With kFill: appends each head vertex to its
+// class list and records its in-arc range [beg, end).
+template <bool kFill>
+__global__ void __launch_bounds__(256) k_head_runs(const uint64_t* __restrict__ keys, uint64_t m,
+                                                   uint32_t vbits, const uint64_t* __restrict__ off,
+                                                   unsigned long long* __restrict__ ctr,
+                                                   uint32_t* __restrict__ hl,
+                                                   uint32_t* __restrict__ beg,
+                                                   uint32_t* __restrict__ end) {
+  const uint64_t none = (1ull << vbits) - 1;
+  const uint32_t lane = lane_id();
+  uint32_t cnt[kHeadClasses] = {0, 0, 0};
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < m;
+       base += stride) {
+    const uint64_t j = base + lane;
+    uint32_t c = kHeadClasses;  // not a run start
+    uint32_t v = 0;
+    if (j < m) {
+      const uint64_t kv = keys[j] >> 32;
+      if (kv != none) {
+        v = (uint32_t)kv;
+        if (j == 0 || (keys[j - 1] >> 32) != kv) c = head_class((uint32_t)(off[v + 1] - off[v]));
+        if (kFill && (j + 1 == m || (keys[j + 1] >> 32) != kv)) end[v] = (uint32_t)(j + 1);
+      }
+    }
+    if (!kFill) {
+#pragma unroll
+      for (int k = 0; k < kHeadClasses; k++) cnt[k] += c == (uint32_t)k;
+    } else {
+      const unsigned peers = __match_any_sync(kFull, c);
+      const uint32_t leader = __ffs(peers) - 1;
+      uint32_t pos = 0;
+      if (c < kHeadClasses && lane == leader)
+        pos = (uint32_t)atomicAdd(ctr + C_HEAD_CURSOR + c, (unsigned long long)__popc(peers));
+      pos = __shfl_sync(kFull, pos, leader) + __popc(peers & lanemask_lt());
+      if (c < kHeadClasses) {
+        hl[kHeadPlanWords + hl[c] + pos] = v;
+        beg[v] = (uint32_t)j;
+      }
+    }
+  }
+  if (!kFill) {
+#pragma unroll
+    for (int k = 0; k < kHeadClasses; k++) {
+      const uint32_t s = __reduce_add_sync(kFull, cnt[k]);
+      if (lane == 0 && s) atomicAdd(ctr + C_HEAD_COUNT + k, (unsigned long long)s);
+    }
+  }
+}
+
+// Class list starts from the counts; clears the fill cursors and queues.
+__global__ void k_head_plan(unsigned long long* __restrict__ ctr, uint32_t* __restrict__ hl) {
+  if (threadIdx.x != 0) return;
+  uint32_t start = 0;
+  for (int c = 0; c < kHeadClasses; c++) {
+    const uint32_t n = (uint32_t)ctr[C_HEAD_COUNT + c];
+    hl[c] = start;
+    hl[kHeadPlanCount + c] = n;
+    start += n;
+    ctr[C_HEAD_CURSOR + c] = 0;
+    ctr[C_HEAD_QUEUE + c] = 0;
+  }
+}
+
+// N+(v) (d entries from vb) as the staged hash of a team of TS threads.
+template <int TS, class Sync>
+__device__ __forceinline__ void stage_hash(const Csr& g, uint64_t vb, uint32_t d, uint32_t t,
+                                           const StageMem& m, const Geo& geo, Sync sync) {
+  for (uint32_t i = t; i < 2 * geo.nb; i += TS) m.hk[i] = kEmpty;
+  sync();
+  for (uint32_t i = t; i < d; i += TS) {
+    const uint32_t x = g.nbr[vb + i];
+    const uint32_t key = (x << 1) | (uint32_t)(g.sgn[vb + i] < 0);
+    uint32_t b = hash_slot(x, geo.shift);
+    while (atomicCAS(&m.hk[2 * b], kEmpty, key) != kEmpty &&
+           atomicCAS(&m.hk[2 * b + 1], kEmpty, key) != kEmpty)
+      b = (b + 1) & (geo.nb - 1);
+  }
+  sync();
+}
+
+// In-arcs [j0, j0 + tn) of a head vertex as the arcs of the staged tile.
+template <int TS, class Sync>
+__device__ __forceinline__ void stage_in_arcs(const Csr& g, const HeadArcs& h, uint32_t j0,
+                                              uint32_t tn, uint32_t t, const StageMem& m,
+                                              Sync sync) {
+  for (uint32_t k = t; k < tn; k += TS) {
+    const uint32_t i = (uint32_t)h.keys[j0 + k];
+    m.lo[k] = i + 1;
+    m.hi[k] = h.aend[i];  // > i + 1: a HEAD arc has a non-empty A'
+    m.s[k] = g.sgn[i];
+    m.st[k] = STC_STRATEGY_HASH;
+  }
+  sync();
+}
+
+// Timing recorder, head side: each in-arc of the tile alone on one warp,
+// timed and charged as a streamed arc is; its cell is that of the arc
+// u -> v (class of N+(u), bucket |A'|, bucket |B| = |N+(v)|).
+__device__ __forceinline__ void timed_head_pass(const Csr& g, const HeadArcs& h, const StageMem& m,
+                                                uint32_t tn, uint32_t dv, uint32_t warp,
+                                                uint32_t warps, uint32_t lane, const Geo& geo,
+                                                PackedCounts& pc, TypeCounts& tc,
+                                                const ArcTimes& at) {
+  for (uint32_t k = warp; k < tn; k += warps) {
+    const uint32_t lo = m.lo[k], hi = m.hi[k];
+    __syncwarp();
+    const long long t0 = clock_after(0);
+    arc_stream(g, m, tn, k, lane, geo, pc);
+    unsigned dt = __reduce_max_sync(kFull, (unsigned)(clock_after(pc.w) - t0));
+    const uint32_t chunks = ((hi + 3) >> 2) - (lo >> 2);
+    dt = (unsigned)((unsigned long long)dt * chunks / (32ull * ((chunks + 31) >> 5)));
+    pc.drain(tc);
+    if (lane == 0) {
+      const uint32_t u = h.asrc[lo - 1];
+      record_arc(at, table_class((uint32_t)(hi - g.off[u])), hi - lo, dv, max(dt, 1u));
+    }
+  }
+}
+
+// Head vertices of the warp class: one warp per vertex from a dynamic
+// queue, N+(v) and up to kWarpCap in-arcs at a time staged in the warp's
+// slice of shared memory.
+template <class Sink, bool kTime, int U>
+__global__ void __launch_bounds__(256) k_head_warp(Csr g, HeadArcs h, const uint32_t* __restrict__ hl,
+                                                   unsigned long long* __restrict__ ctr, Sink sink,
+                                                   ArcTimes at, uint32_t hf) {
+  constexpr bool kVC = Sink::kPerVertex;
+  constexpr int kWarps = 8;
+  __shared__ __align__(16) unsigned char smem[kWarps * kWarpStageBytes];
+  const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
+  const StageMem m = StageMem::carve(smem + w * kWarpStageBytes, kWarpCap, kWarpBuckets);
+  const uint32_t* list = hl + kHeadPlanWords + hl[0];
+  const uint32_t cnt = hl[kHeadPlanCount + 0];
+  TypeCounts tc;
+  while (true) {
+    uint32_t item = 0;
+    if (lane == 0) item = (uint32_t)atomicAdd(ctr + C_HEAD_QUEUE + 0, 1ull);
+    item = __shfl_sync(kFull, item, 0);
+    if (item >= cnt) break;
+    const uint32_t v = list[item];
+    const uint64_t vb = g.off[v];
+    const uint32_t d = (uint32_t)(g.off[v + 1] - vb);
+    if (d > kWarpCap) {  // uniform over the warp
+      if (lane == 0) atomicExch(ctr + C_ERROR, kErrStageCapacity);
+      continue;
+    }
+    const Geo geo = Geo::of(d, kWarpBuckets, hf);
+    stage_hash<32>(g, vb, d, lane, m, geo, WarpSync{});
+    TypeCounts vc;
+    TypeCounts& out = kVC ? vc : tc;
+    PackedCounts pc;
+    const uint32_t j1 = h.end[v];
+    for (uint32_t j0 = h.beg[v]; j0 < j1; j0 += kWarpCap) {
+      const uint32_t tn = min(kWarpCap, j1 - j0);
+      stage_in_arcs<32>(g, h, j0, tn, lane, m, WarpSync{});
+      if (kTime) {
+        timed_head_pass(g, h, m, tn, d, 0, 1, lane, geo, pc, out, at);
+      } else {
+        warp_chunk_scan(m, tn, lane);
+        stream_pass<U, false>(g, m, tn, 0, 1, lane, geo, out, nullptr);
+      }
+      __syncwarp();
+    }
+    pc.drain(out);
+    if (kVC) warp_vertex_flush(vc, v, lane, sink);
+    __syncwarp();
+  }
+  if (!kVC) flush_counts<256>(tc, ctr);
+}
+
+// Head vertices of the block and large classes: one CTA per vertex from a
+// dynamic queue, N+(v) (up to `cap` entries, `nb` buckets) and up to `cap`
+// in-arcs at a time staged in dynamic shared memory.
+template <int THREADS, class Sink, bool kTime, int U>
+__global__ void __launch_bounds__(THREADS) k_head_block(Csr g, HeadArcs h,
+                                                        const uint32_t* __restrict__ hl,
+                                                        uint32_t hclass, uint32_t cap, uint32_t nb,
+                                                        uint32_t hf,
+                                                        unsigned long long* __restrict__ ctr,
+                                                        Sink sink, ArcTimes at) {
+  constexpr bool kVC = Sink::kPerVertex;
+  constexpr uint32_t kWarps = THREADS / 32;
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ uint32_t scan_tmp[THREADS / 32 + 2];
+  __shared__ uint32_t s_item;
+  const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
+  const StageMem m = StageMem::carve(smem, cap, nb);
+  const uint32_t* list = hl + kHeadPlanWords + hl[hclass];
+  const uint32_t cnt = hl[kHeadPlanCount + hclass];
+  unsigned long long* queue = ctr + C_HEAD_QUEUE + hclass;
+  uint32_t* next = scan_tmp + kWarps + 1;  // the stream's claim counter
+  TypeCounts tc;
+  while (true) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_item = (uint32_t)atomicAdd(queue, 1ull);
+    __syncthreads();
+    const uint32_t item = s_item;
+    if (item >= cnt) break;
+    const uint32_t v = list[item];
+    const uint64_t vb = g.off[v];
+    const uint32_t d = (uint32_t)(g.off[v + 1] - vb);
+    if (d > cap) {  // uniform over the CTA
+      if (threadIdx.x == 0) atomicExch(ctr + C_ERROR, kErrStageCapacity);
+      continue;
+    }
+    const Geo geo = Geo::of(d, nb, hf);
+    stage_hash<THREADS>(g, vb, d, threadIdx.x, m, geo, BlockSync{});
+    TypeCounts vc;
+    TypeCounts& out = kVC ? vc : tc;
+    PackedCounts pc;
+    const uint32_t j1 = h.end[v];
+    for (uint32_t j0 = h.beg[v]; j0 < j1; j0 += cap) {
+      const uint32_t tn = min(cap, j1 - j0);
+      // Every warp left the previous tile's stream (barrier at its end), and
+      // the staging below passes a barrier before the counter is used.
+      if (threadIdx.x == 0) *next = 0;
+      stage_in_arcs<THREADS>(g, h, j0, tn, threadIdx.x, m, BlockSync{});
+      if (kTime) {
+        timed_head_pass(g, h, m, tn, d, w, kWarps, lane, geo, pc, out, at);
+      } else {
+        block_chunk_scan<THREADS>(m, tn, scan_tmp);
+        stream_pass<U, false>(g, m, tn, w, kWarps, lane, geo, out, next);
+      }
+      __syncthreads();
+    }
+    pc.drain(out);
+    if (kVC) block_vertex_flush<THREADS>(vc, v, sink);
+  }
+  if (!kVC) flush_counts<THREADS>(tc, ctr);
+}
+
+// Device buffers of the head-side pass (allocated before any capture).
+struct HeadBufs {
+  uint64_t* keys = nullptr;
+  uint64_t* alt = nullptr;
+  uint32_t* aend = nullptr;
+  uint32_t* runs = nullptr;  // beg[n], end[n]
+  uint32_t* hl = nullptr;    // plan words, class lists
+  uint8_t* need = nullptr;   // per tail: it keeps arcs for the tail side
+  uint32_t* sort_counts = nullptr;
+};
+
+HeadBufs head_buffers(stc_ctx* c, const DeviceGraph& g) {
+  HeadBufs b;
+  b.keys = buffer<uint64_t>(c, B_KEYS_A, g.m_fwd);
+  b.alt = buffer<uint64_t>(c, B_KEYS_B, g.m_fwd);
+  b.aend = buffer<uint32_t>(c, B_HEAD_END, g.m_fwd);
+  b.runs = buffer<uint32_t>(c, B_HEAD_RUNS, 2ull * g.n);
+  b.hl = buffer<uint32_t>(c, B_HEAD_LIST, (size_t)g.n + kHeadPlanWords + (g.n + 3) / 4);
+  b.need = reinterpret_cast<uint8_t*>(b.hl + g.n + kHeadPlanWords);
+  b.sort_counts = buffer<uint32_t>(c, B_SORT_COUNTS, (size_t)kRadix * kMaxSortGrid);
+  return b;
+}
+
+// Shared-memory limits of the head-class kernels a head-side pass with this
+// tuning launches; called before the pass is enqueued (or captured).
+template <class Sink, bool kTime>
+void prepare_head(const Tuning& tu) {
+  const size_t sb =
+      block_stage_bytes(kBlockCap, fit_hash_factor(tu.hash_factor[1], kBlockCap) * kBlockCap);
+  const size_t sl =
+      block_stage_bytes(kLargeCap, fit_hash_factor(tu.hash_factor[2], kLargeCap) * kLargeCap);
+  with_block_threads(kTime ? 256 : tu.block_threads, [&](auto T) {
+    with_unroll(kTime ? kStreamUnroll : tu.unroll[1], [&](auto U) {
+      constexpr int kT = decltype(T)::value, kU = decltype(U)::value;
+      if constexpr (!kTime || (kT == 256 && kU == kStreamUnroll))
+        STC_CUDA(cudaFuncSetAttribute(k_head_block<kT, Sink, kTime, kU>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb));
+    });
+  });
+  with_unroll(kTime ? kStreamUnroll : tu.unroll[2], [&](auto U) {
+    constexpr int kU = decltype(U)::value;
+    if constexpr (!kTime || kU == kStreamUnroll)
+      STC_CUDA(cudaFuncSetAttribute(k_head_block<512, Sink, kTime, kU>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sl));
+  });
+}
+
+// The head-side pass is enqueued on `st` (no host synchronisation) in two
+// parts: the keys (before the tail side is classified, which skips the
+// tails left without arcs), then the sort, runs, plan and the three
+// head-class kernels.  The launch parameters of the block and large classes
+// follow the tuning of the tail side's same classes.
+inline void enqueue_head_keys(cudaStream_t st, const Csr& csr, const uint32_t* asrc, uint64_t m,
+                              const HeadBufs& b, const uint8_t* d_tables,
+                              const unsigned long long* range, unsigned long long* ctr,
+                              int& launches) {
+  const uint32_t vbits = std::max<uint32_t>(1, bit_width64(csr.n - 1));
+  STC_CUDA(cudaMemsetAsync(ctr + C_HEAD_COUNT, 0, 9 * sizeof(unsigned long long), st));
+  STC_CUDA(cudaMemsetAsync(b.need, 0, csr.n, st));
+  const uint32_t grid = (uint32_t)std::min<uint64_t>((m + 1023) / 1024, kSMs * 16);
+  k_head_keys<<<std::max(1u, grid), 256, 0, st>>>(csr, asrc, m, d_tables, vbits, range, b.keys,
+                                                  b.aend, b.need);
+  launches++;
+}
+
+template <class Sink, bool kTime>
+void enqueue_head(cudaStream_t st, const Csr& csr, const uint32_t* asrc, uint64_t m,
+                  const HeadBufs& b, unsigned long long* ctr, const Sink& sink,
+                  const ArcTimes& at, const Tuning& tu, int& launches) {
+  const uint32_t n = csr.n;
+  const uint32_t vbits = std::max<uint32_t>(1, bit_width64(n - 1));
+  int sort_launches = 0;
+  const uint64_t* sorted =
+      radix_sort(b.keys, b.alt, m, 32, 32 + (int)vbits, b.sort_counts, st, &sort_launches);
+  uint32_t* beg = b.runs;
+  uint32_t* end = b.runs + n;
+  k_head_runs<false><<<kSMs * 4, 256, 0, st>>>(sorted, m, vbits, csr.off, ctr, b.hl, beg, end);
+  k_head_plan<<<1, 32, 0, st>>>(ctr, b.hl);
+  k_head_runs<true><<<kSMs * 4, 256, 0, st>>>(sorted, m, vbits, csr.off, ctr, b.hl, beg, end);
+  const HeadArcs h{sorted, b.aend, beg, end, asrc};
+  launches += 3 + sort_launches;
+  with_unroll(kTime ? kStreamUnroll : tu.unroll[0], [&](auto U) {
+    constexpr int kU = decltype(U)::value;
+    if constexpr (!kTime || kU == kStreamUnroll)
+      k_head_warp<Sink, kTime, kU><<<kSMs * 4, 256, 0, st>>>(csr, h, b.hl, ctr, sink, at,
+                                                             tu.hash_factor[0]);
+  });
+  {
+    const uint32_t cap = kBlockCap;
+    const uint32_t hf = fit_hash_factor(tu.hash_factor[1], cap);
+    const uint32_t nb = hf * cap;
+    const size_t smem = block_stage_bytes(cap, nb);
+    with_block_threads(kTime ? 256 : tu.block_threads, [&](auto T) {
+      with_unroll(kTime ? kStreamUnroll : tu.unroll[1], [&](auto U) {
+        constexpr int kT = decltype(T)::value, kU = decltype(U)::value;
+        if constexpr (!kTime || (kT == 256 && kU == kStreamUnroll)) {
+          const uint32_t per_sm = smem <= 110 * 1024 ? 2 : 1;
+          k_head_block<kT, Sink, kTime, kU><<<kSMs * per_sm, kT, smem, st>>>(
+              csr, h, b.hl, 1, cap, nb, hf, ctr, sink, at);
+        }
+      });
+    });
+  }
+  {
+    const uint32_t cap = kLargeCap;
+    const uint32_t hf = fit_hash_factor(tu.hash_factor[2], cap);
+    const uint32_t nb = hf * cap;
+    const size_t smem = block_stage_bytes(cap, nb);
+    with_unroll(kTime ? kStreamUnroll : tu.unroll[2], [&](auto U) {
+      constexpr int kU = decltype(U)::value;
+      if constexpr (!kTime || kU == kStreamUnroll)
+        k_head_block<512, Sink, kTime, kU><<<kSMs, 512, smem, st>>>(csr, h, b.hl, 2, cap, nb, hf,
+                                                                     ctr, sink, at);
+    });
+  }
+  launches += 3;
+  STC_CUDA(cudaGetLastError());
+}
+
 // ------------------------------------------------------- persistent ----
 // The persistent engine: the whole count as one sequence without host
 // synchronisation, so that it can be captured once in a CUDA graph and
@@ -1188,22 +1638,36 @@ __global__ void __launch_bounds__(256, 4) k_persistent(Csr g, const uint32_t* __
                                               ArcTimes{nullptr, nullptr}, tc);
     } else {
       const uint32_t idx = (item - nw) * 32 + lane;
-      if (idx < nt) tiny_vertex<kTinyMax>(g, lists[plan[0] + idx], sink, tc);
+      if (idx < nt) tiny_vertex<kTinyMax>(g, lists[plan[0] + idx], sink, tw, tc);
     }
   }
   if (!Sink::kPerVertex) flush_counts<256>(tc, ctr);
 }
 
+// The head-side pass of a persistent count: its buffers and the arcs.
+struct HeadPlan {
+  const HeadBufs* bufs = nullptr;  // null: the tables send no arc to the head side
+  const uint32_t* asrc = nullptr;
+  uint64_t m = 0;
+  Tuning tuning;
+};
+
 // Enqueues the persistent sequence on `st` (no host synchronisation).
 template <class Sink>
 void enqueue_persistent(cudaStream_t st, const Csr& csr, const ClassBounds& cb, uint32_t* lists,
                         uint32_t* plan, unsigned long long* ctr, const uint8_t* d_tables,
-                        const Sink& sink) {
+                        const Sink& sink, const HeadPlan& hp, int& launches) {
   const ArcTimes none{nullptr, nullptr};
+  const uint8_t* need = nullptr;
+  if (hp.bufs) {
+    enqueue_head_keys(st, csr, hp.asrc, hp.m, *hp.bufs, d_tables, nullptr, ctr, launches);
+    need = hp.bufs->need;
+  }
   STC_CUDA(cudaMemsetAsync(ctr + C_WORK, 0, 8 * sizeof(uint64_t), st));
-  k_classify_count<<<kSMs * 4, 256, 0, st>>>(csr.off, csr.n, cb, ctr, nullptr);
+  k_classify_count<<<kSMs * 4, 256, 0, st>>>(csr.off, csr.n, cb, ctr, nullptr, need);
   k_plan<<<1, 32, 0, st>>>(ctr, plan);
-  k_classify_fill<<<kSMs * 4, 256, 0, st>>>(csr.off, csr.n, cb, lists, plan, ctr + C_WORK, nullptr);
+  k_classify_fill<<<kSMs * 4, 256, 0, st>>>(csr.off, csr.n, cb, lists, plan, ctr + C_WORK, nullptr,
+                                            need);
   k_persistent<Sink><<<kSMs * 4, 256, kPersistentSmem, st>>>(csr, lists, plan, ctr, sink,
                                                              d_tables);
   k_block<512, Sink, false, kStreamUnroll, false>
@@ -1212,53 +1676,67 @@ void enqueue_persistent(cudaStream_t st, const Csr& csr, const ClassBounds& cb, 
       d_tables + 256 * kTableLarge, none, kTableLarge, plan, 3);
   k_giant<512, Sink, false><<<kSMs * 2, 512, 0, st>>>(csr, lists, 0, ctr + C_WORK + 7, ctr, sink,
                                                       d_tables + 256 * kTableGiant, none, plan, 4);
+  launches += 6;
+  if (hp.bufs)
+    enqueue_head<Sink, false>(st, csr, hp.asrc, hp.m, *hp.bufs, ctr, sink, none, hp.tuning,
+                              launches);
   STC_CUDA(cudaGetLastError());
 }
 
 // Identity of a captured persistent sequence: every pointer and size its
 // kernels were given.
 struct PersistentKey {
-  const void* p[9];
-  uint64_t v[4];
-  bool operator==(const PersistentKey& o) const { return memcmp(this, &o, sizeof(*this)) == 0; }
+  const void* p[15];
+  uint64_t v[6];
 };
 
 template <class Sink>
 void count_persistent(stc_ctx* c, const Csr& csr, const ClassBounds& cb, uint32_t* lists,
                       uint32_t* plan, unsigned long long* ctr, const uint8_t* d_tables,
-                      const Sink& sink, const void* s0, const void* s1, uint64_t s2) {
+                      const Sink& sink, const void* s0, const void* s1, uint64_t s2,
+                      const HeadPlan& hp) {
   cudaStream_t st = c->stream;
   STC_CUDA(cudaFuncSetAttribute(k_persistent<Sink>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)kPersistentSmem));
   STC_CUDA(cudaFuncSetAttribute(k_block<512, Sink, false, kStreamUnroll, false>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)StageMem::bytes(kLargeCap, 2 * kLargeCap)));
-  c->launches += 6;
+  if (hp.bufs) prepare_head<Sink, false>(hp.tuning);
   // The legacy default stream cannot be captured: launch directly there.
   if (st == nullptr || st == cudaStreamLegacy || st == cudaStreamPerThread) {
-    enqueue_persistent(st, csr, cb, lists, plan, ctr, d_tables, sink);
+    enqueue_persistent(st, csr, cb, lists, plan, ctr, d_tables, sink, hp, c->launches);
     return;
   }
   PersistentKey key{};
-  const void* ptrs[9] = {csr.off, csr.nbr, csr.sgn, csr.verts, lists, plan, ctr, d_tables, s0};
+  const HeadBufs hb = hp.bufs ? *hp.bufs : HeadBufs{};
+  const void* ptrs[15] = {csr.off, csr.nbr, csr.sgn, csr.verts, lists, plan, ctr, d_tables, s0,
+                          hp.asrc, hb.keys, hb.alt, hb.aend, hb.runs, hb.hl};
   memcpy(key.p, ptrs, sizeof(ptrs));
   key.v[0] = csr.n;
   key.v[1] = cb.tiny_max;
   key.v[2] = s2;
   key.v[3] = reinterpret_cast<uint64_t>(s1);
+  key.v[4] = hp.m;
+  key.v[5] = reinterpret_cast<uint64_t>(hb.sort_counts) ^
+             ((uint64_t)hp.tuning.block_threads << 48) ^ ((uint64_t)hp.tuning.unroll[0] << 56) ^
+             ((uint64_t)hp.tuning.unroll[1] << 58) ^ ((uint64_t)hp.tuning.unroll[2] << 60) ^
+             ((uint64_t)hp.tuning.hash_factor[0] << 40) ^ ((uint64_t)hp.tuning.hash_factor[1] << 42) ^
+             ((uint64_t)hp.tuning.hash_factor[2] << 44);
   static_assert(sizeof(PersistentKey) <= sizeof(c->graph_key), "graph key size");
   if (c->graph_exec && memcmp(c->graph_key, &key, sizeof(key)) == 0) {
     STC_CUDA(cudaGraphLaunch(c->graph_exec, st));
+    c->launches += c->graph_launches;
     return;
   }
   if (c->graph_exec) {
     STC_CUDA(cudaGraphExecDestroy(c->graph_exec));
     c->graph_exec = nullptr;
   }
+  int launches = 0;
   cudaGraph_t graph = nullptr;
   STC_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
   try {
-    enqueue_persistent(st, csr, cb, lists, plan, ctr, d_tables, sink);
+    enqueue_persistent(st, csr, cb, lists, plan, ctr, d_tables, sink, hp, launches);
   } catch (...) {
     cudaStreamEndCapture(st, &graph);
     if (graph) cudaGraphDestroy(graph);
@@ -1269,7 +1747,9 @@ void count_persistent(stc_ctx* c, const Csr& csr, const ClassBounds& cb, uint32_
   cudaGraphDestroy(graph);
   STC_CUDA(e);
   memcpy(c->graph_key, &key, sizeof(key));
+  c->graph_launches = launches;
   STC_CUDA(cudaGraphLaunch(c->graph_exec, st));
+  c->launches += launches;
 }
 
 // ------------------------------------------------------------- split ----
@@ -1389,40 +1869,71 @@ void shard_range(stc_ctx* c, const DeviceGraph& g, uint32_t shard, uint32_t shar
 
 }  // namespace
 
-// Fixed degree-threshold dispatch, the same for every class: SEARCH when B
-// is at least 16x longer than A', MERGE when both are short, HASH otherwise
-// (the giant class, which stages no hash, merges instead of hashing).
-void fixed_dispatch_tables(uint8_t* out) {
+// Fixed degree-threshold dispatch, the same for every class: HEAD when A' is
+// not the longer list (bucket |A'| <= bucket |B|) and |B| <= 4095, SEARCH
+// when B is at least 16x longer than A', MERGE when both are short, HASH
+// otherwise (the giant class, which stages no hash, merges instead of
+// hashing).  Without `head`, the tail-side table of the first version
+// (no HEAD cells), which per-vertex counts and the no-allocation path use.
+void fixed_dispatch_tables(uint8_t* out, bool head) {
   for (int t = 0; t < kTableClasses; t++)
     for (int a = 0; a < 16; a++)
       for (int b = 0; b < 16; b++) {
         uint8_t s = STC_STRATEGY_HASH;
-        if (b >= a + 4) s = STC_STRATEGY_SEARCH;
+        if (head && b >= 1 && b <= 12 && a <= b) s = STC_STRATEGY_HEAD;
+        else if (b >= a + 4) s = STC_STRATEGY_SEARCH;
         else if (a <= 3 && b <= 5) s = STC_STRATEGY_MERGE;
         out[256 * t + 16 * a + b] = s;
       }
 }
 
+namespace {
+// Cached tables in B_DISPATCH_FIXED: the fixed tables with and without HEAD,
+// and the forced-HEAD tables (HEAD wherever it applies, HASH elsewhere).
+enum { kFixedHead = 0, kFixedNoHead = 1, kForcedHead = 2, kCachedTables = 3 };
+}  // namespace
+
 // Device copy of the dispatch tables a call uses: a forced strategy fills
-// every cell; otherwise the learned tables when the context holds a model
-// and the call asks for them, else the fixed ones.
-const uint8_t* dispatch_tables(stc_ctx* c, const CountConfig& cfg) {
+// every cell (HEAD only the cells where it applies); otherwise the learned
+// tables when the context holds a model and the call asks for them, else
+// the fixed ones.  Per-vertex counts take tables without HEAD (the head
+// side reports per graph, not per source vertex).  `uses_head` (optional)
+// receives whether the tables send any cell to the head side.
+const uint8_t* dispatch_tables(stc_ctx* c, const CountConfig& cfg, bool* uses_head) {
+  const bool head_ok = cfg.vertex_counts == nullptr;
+  if (uses_head) *uses_head = false;
+  if (!c->fixed_ready) {
+    uint8_t h[kCachedTables * kTableBytes];
+    fixed_dispatch_tables(h + kFixedHead * kTableBytes, true);
+    fixed_dispatch_tables(h + kFixedNoHead * kTableBytes, false);
+    for (size_t i = 0; i < kTableBytes; i++)
+      h[kForcedHead * kTableBytes + i] =
+          (i & 15) <= 12 ? (uint8_t)STC_STRATEGY_HEAD : (uint8_t)STC_STRATEGY_HASH;
+    uint8_t* t = buffer<uint8_t>(c, B_DISPATCH_FIXED, sizeof(h));
+    STC_CUDA(cudaMemcpyAsync(t, h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
+    STC_CUDA(cudaStreamSynchronize(c->stream));  // `h` is pageable and leaves scope
+    c->fixed_ready = true;
+  }
+  const uint8_t* cached = buffer<uint8_t>(c, B_DISPATCH_FIXED, kCachedTables * kTableBytes);
+  if (cfg.strategy == STC_STRATEGY_HEAD) {
+    if (uses_head) *uses_head = head_ok;
+    if (head_ok) return cached + kForcedHead * kTableBytes;
+    uint8_t* t = buffer<uint8_t>(c, B_WORK2, kTableBytes);
+    STC_CUDA(cudaMemsetAsync(t, (int)STC_STRATEGY_HASH, kTableBytes, c->stream));
+    return t;
+  }
   if (cfg.strategy != STC_STRATEGY_AUTO) {
     uint8_t* t = buffer<uint8_t>(c, B_WORK2, kTableBytes);
     STC_CUDA(cudaMemsetAsync(t, (int)cfg.strategy, kTableBytes, c->stream));
     return t;
   }
-  if (cfg.dispatch == STC_DISPATCH_LEARNED && c->model_loaded)
+  if (!head_ok) return cached + kFixedNoHead * kTableBytes;
+  if (cfg.dispatch == STC_DISPATCH_LEARNED && c->model_loaded) {
+    if (uses_head) *uses_head = c->learned_uses_head;
     return buffer<uint8_t>(c, B_DISPATCH, kTableBytes);
-  if (!c->fixed_ready) {
-    uint8_t h[kTableBytes];
-    fixed_dispatch_tables(h);
-    uint8_t* t = buffer<uint8_t>(c, B_DISPATCH_FIXED, kTableBytes);
-    STC_CUDA(cudaMemcpyAsync(t, h, kTableBytes, cudaMemcpyHostToDevice, c->stream));
-    STC_CUDA(cudaStreamSynchronize(c->stream));  // `h` is pageable and leaves scope
-    c->fixed_ready = true;
   }
-  return buffer<uint8_t>(c, B_DISPATCH_FIXED, kTableBytes);
+  if (uses_head) *uses_head = true;
+  return cached + kFixedHead * kTableBytes;
 }
 
 // Builds the sign-split copy of g's heads on the context's stream.
@@ -1445,7 +1956,13 @@ void count_triangles(stc_ctx* c, const DeviceGraph& gin, const CountConfig& cfg)
   if (split) build_split(c, g);
   Csr csr{g.off, g.nbr, g.sgn, g.verts, g.n, g.nbr_split, g.psplit};
   unsigned long long* ctr = (unsigned long long*)counters(c);
-  const uint8_t* d_table = dispatch_tables(c, cfg);
+  bool uses_head = false;
+  const uint8_t* d_table = dispatch_tables(c, cfg, &uses_head);
+  // The head-side pass runs when the tables send arcs there (never for
+  // per-vertex counts, whose tables have no HEAD cells).
+  const bool head = uses_head && (cfg.class_mask & 0x20u) && g.asrc != nullptr && g.n >= 2;
+  HeadBufs hb;
+  if (head) hb = head_buffers(c, g);
   const bool timed = cfg.arc_cycles != nullptr;
   const ArcTimes at{(unsigned long long*)cfg.arc_cycles, (unsigned long long*)cfg.arc_counts};
   const unsigned long long* range = nullptr;
@@ -1466,19 +1983,32 @@ void count_triangles(stc_ctx* c, const DeviceGraph& gin, const CountConfig& cfg)
   if (cfg.persistent && !timed && cfg.shards <= 1 && !split) {
     uint32_t* lists = buffer<uint32_t>(c, B_WORK, (size_t)g.n + kPlanWords + 8);
     uint32_t* plan = lists + g.n + 4;
+    HeadPlan hp;
+    if (head) {
+      hp.bufs = &hb;
+      hp.asrc = g.asrc;
+      hp.m = g.m_fwd;
+      hp.tuning = c->tuning;
+    }
     if (cfg.vertex_counts) {
       const VertexSink sink{(unsigned long long*)cfg.vertex_counts, g.verts};
-      count_persistent(c, csr, cb, lists, plan, ctr, d_table, sink, sink.vcounts, nullptr, 1);
+      count_persistent(c, csr, cb, lists, plan, ctr, d_table, sink, sink.vcounts, nullptr, 1, hp);
     } else if (cfg.graph_counts) {
       const GraphSink sink{(unsigned long long*)cfg.graph_counts, g.gbase, g.G};
       count_persistent(c, csr, cb, lists, plan, ctr, d_table, sink, sink.gcounts, sink.gbase,
-                       2 + ((uint64_t)g.G << 8));
+                       2 + ((uint64_t)g.G << 8), hp);
     } else {
-      count_persistent(c, csr, cb, lists, plan, ctr, d_table, TotalSink{}, nullptr, nullptr, 0);
+      count_persistent(c, csr, cb, lists, plan, ctr, d_table, TotalSink{}, nullptr, nullptr, 0,
+                       hp);
     }
     return;
   }
-  k_classify_count<<<kSMs * 4, 256, 0, st>>>(g.off, g.n, cb, ctr, range);
+  const uint8_t* need = nullptr;
+  if (head) {
+    enqueue_head_keys(st, csr, g.asrc, g.m_fwd, hb, d_table, range, ctr, c->launches);
+    need = hb.need;
+  }
+  k_classify_count<<<kSMs * 4, 256, 0, st>>>(g.off, g.n, cb, ctr, range, need);
   STC_CUDA(cudaMemcpyAsync(c->h_pinned + C_WORK, counters(c) + C_WORK,
                            (C_MAX_FDEG + 1 - C_WORK) * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
   STC_CUDA(cudaStreamSynchronize(st));
@@ -1494,24 +2024,30 @@ void count_triangles(stc_ctx* c, const DeviceGraph& gin, const CountConfig& cfg)
   STC_CUDA(cudaMemcpyAsync(d_starts, starts, kClasses * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
   // Cursors of the fill, then the dynamic queues, live in C_WORK ...
   STC_CUDA(cudaMemsetAsync(counters(c) + C_WORK, 0, 8 * sizeof(uint64_t), st));
-  k_classify_fill<<<kSMs * 4, 256, 0, st>>>(g.off, g.n, cb, lists, d_starts, ctr + C_WORK, range);
+  k_classify_fill<<<kSMs * 4, 256, 0, st>>>(g.off, g.n, cb, lists, d_starts, ctr + C_WORK, range,
+                                            need);
   STC_CUDA(cudaMemsetAsync(counters(c) + C_WORK, 0, 8 * sizeof(uint64_t), st));
   c->launches += 2;
 
+  auto run = [&](const auto& sink, auto time_tag) {
+    using Sink = std::decay_t<decltype(sink)>;
+    constexpr bool kT = decltype(time_tag)::value;
+    launch_classes<Sink, kT>(st, csr, lists, counts, starts, max_fdeg, ctr, d_table, sink, at,
+                             c->tuning, cfg.class_mask, c->launches);
+    if (head) {
+      prepare_head<Sink, kT>(c->tuning);
+      enqueue_head<Sink, kT>(st, csr, g.asrc, g.m_fwd, hb, ctr, sink, at, c->tuning,
+                             c->launches);
+    }
+  };
   if (timed) {
-    launch_classes<TotalSink, true>(st, csr, lists, counts, starts, max_fdeg, ctr, d_table,
-                                    TotalSink{}, at, c->tuning, cfg.class_mask, c->launches);
+    run(TotalSink{}, std::true_type{});
   } else if (cfg.vertex_counts) {
-    const VertexSink sink{(unsigned long long*)cfg.vertex_counts, g.verts};
-    launch_classes<VertexSink, false>(st, csr, lists, counts, starts, max_fdeg, ctr, d_table, sink,
-                                      at, c->tuning, cfg.class_mask, c->launches);
+    run(VertexSink{(unsigned long long*)cfg.vertex_counts, g.verts}, std::false_type{});
   } else if (cfg.graph_counts) {
-    const GraphSink sink{(unsigned long long*)cfg.graph_counts, g.gbase, g.G};
-    launch_classes<GraphSink, false>(st, csr, lists, counts, starts, max_fdeg, ctr, d_table, sink,
-                                     at, c->tuning, cfg.class_mask, c->launches);
+    run(GraphSink{(unsigned long long*)cfg.graph_counts, g.gbase, g.G}, std::false_type{});
   } else {
-    launch_classes<TotalSink, false>(st, csr, lists, counts, starts, max_fdeg, ctr, d_table,
-                                     TotalSink{}, at, c->tuning, cfg.class_mask, c->launches);
+    run(TotalSink{}, std::false_type{});
   }
   STC_CUDA(cudaGetLastError());
 }
@@ -1685,7 +2221,7 @@ extern "C" stc_status stc_count_oriented_csr_noalloc(const uint64_t* d_offsets,
   if (m == 0) return STC_OK;
 
   uint8_t table[kTableBytes];
-  fixed_dispatch_tables(table);
+  fixed_dispatch_tables(table, false);
   STC_NA(cudaMemcpyAsync(scr->table, table, sizeof(table), cudaMemcpyHostToDevice, st));
   const ClassBounds cb{kTinyMax, kWarpCap, kBlockCap, kLargeCap};
   k_classify_count<<<kSMs * 4, 256, 0, st>>>(d_offsets, n, cb, ctr, nullptr);

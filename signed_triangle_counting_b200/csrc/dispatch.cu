@@ -3,7 +3,8 @@
 // that turns a model into dispatch tables on the device.
 //
 // A dispatch cell is (class of u's list, bucket |A'|, bucket |B|); a table
-// maps every cell to MERGE, HASH or SEARCH.  All three give identical counts,
+// maps every cell to a strategy (MERGE, HASH, SEARCH, SPLIT or HEAD).  All
+// give identical counts,
 // so the model decides only speed.  The model predicts, per strategy, the
 // log2 of the SM cycles an arc of the cell costs, and a cell's table entry
 // is the strategy of least predicted cost.  Training regresses the timing
@@ -33,7 +34,7 @@ constexpr uint32_t kMaxTrainSamples = 4096;
 constexpr uint64_t kStreamMlpInit = 11;  // generator stream of the initial weights
 
 // Parameter offsets (layout W1[hidden][in], b1[hidden], W2[out][hidden], b2[out];
-// outputs MERGE, HASH, SEARCH, SPLIT).
+// outputs MERGE, HASH, SEARCH, SPLIT, HEAD).
 constexpr int kOffB1 = kMlpHidden * kMlpIn;
 constexpr int kOffW2 = kOffB1 + kMlpHidden;
 constexpr int kOffB2 = kOffW2 + kMlpOut * kMlpHidden;
@@ -85,7 +86,8 @@ constexpr float kOverrideMargin = 0.0704f;
 // in the model's support and that strategy beats the fixed table's choice by
 // the margin, else the fixed choice.  The giant
 // class stages no hash, so it never takes HASH or SPLIT (its fixed HASH
-// cells run MERGE, and are compared as such).
+// cells run MERGE, and are compared as such); HEAD needs |B| <= 4095, so it
+// is open to cells with b <= 12 only.
 __global__ void k_mlp_tables(const float* __restrict__ params, const uint8_t* __restrict__ fixed,
                              const uint8_t* __restrict__ support, uint8_t* __restrict__ tables) {
   __shared__ float p[kMlpParams];
@@ -97,10 +99,12 @@ __global__ void k_mlp_tables(const float* __restrict__ params, const uint8_t* __
   cell_features(cell, f);
   mlp_forward(p, f, h, z);
   const bool giant = (cell >> 8) == kTableGiant;
+  const bool head_ok = (cell & 15) <= 12;
   auto staged_only = [](int o) { return o == STC_STRATEGY_HASH - 1 || o == STC_STRATEGY_SPLIT - 1; };
   int best = 0;
   for (int o = 1; o < kMlpOut; o++) {
     if (giant && staged_only(o)) continue;
+    if (!head_ok && o == STC_STRATEGY_HEAD - 1) continue;
     if (z[o] < z[best]) best = o;
   }
   int fx = fixed[cell] - 1;
@@ -284,7 +288,11 @@ void load_dispatch_model(stc_ctx* c, const float* params, const uint8_t* support
   // Counts with these tables build the sign-split heads only if some cell
   // picks SPLIT.
   c->learned_uses_split = false;
-  for (size_t i = 0; i < kTableBytes; i++) c->learned_uses_split |= h[i] == STC_STRATEGY_SPLIT;
+  c->learned_uses_head = false;
+  for (size_t i = 0; i < kTableBytes; i++) {
+    c->learned_uses_split |= h[i] == STC_STRATEGY_SPLIT;
+    c->learned_uses_head |= h[i] == STC_STRATEGY_HEAD;
+  }
 }
 
 void train_dispatcher(stc_ctx* c, const float* features, const float* targets,

@@ -44,6 +44,9 @@ enum BufId {
   B_TEXT,                         // text input of the GPU parser (padded to 16 bytes)
   B_SPLIT_NBR,                    // sign-split copy of the arc heads (m + 4)
   B_SPLIT_POS,                    // positive arcs per vertex (n)
+  B_HEAD_END,                     // head-side pass: end of each arc's tail list (m)
+  B_HEAD_RUNS,                    // head-side pass: in-arc range per head vertex (2 n)
+  B_HEAD_LIST,                    // head-side pass: head vertices by class, plan, flags
   B_COUNT_
 };
 
@@ -65,6 +68,9 @@ enum CounterSlot {
   C_SHARD_LO = 18,             // rank range [lo, hi) of a sharded count
   C_SHARD_HI = 19,
   C_QUEUE_WARP = 20,           // warp-granular work queue of the persistent engine
+  C_HEAD_COUNT = 21,           // head-side pass: head vertices per class (3 slots),
+  C_HEAD_CURSOR = 24,          // their list fill cursors (3 slots)
+  C_HEAD_QUEUE = 27,           // and the classes' work queues (3 slots)
   C_SLOTS = 32
 };
 
@@ -83,11 +89,11 @@ static_assert(kTableBytes == STC_DISPATCH_CELLS, "one table byte per dispatch ce
 
 // The dispatcher's multilayer perceptron: STC_DISPATCH_FEATURES inputs, one
 // hidden ReLU layer, one predicted log2 cost per strategy (MERGE, HASH,
-// SEARCH, SPLIT).
+// SEARCH, SPLIT, HEAD).
 // Parameter layout: W1[hidden][in], b1[hidden], W2[out][hidden], b2[out].
 constexpr int kMlpIn = STC_DISPATCH_FEATURES;
 constexpr int kMlpHidden = 16;
-constexpr int kMlpOut = 4;
+constexpr int kMlpOut = STC_DISPATCH_STRATEGIES;
 constexpr int kMlpParams = kMlpHidden * kMlpIn + kMlpHidden + kMlpOut * kMlpHidden + kMlpOut;
 static_assert(kMlpParams == STC_DISPATCH_MODEL_PARAMS, "parameter count of the ABI");
 
@@ -117,10 +123,12 @@ struct stc_ctx {
   bool fixed_ready = false;   // B_DISPATCH_FIXED holds the fixed tables
   bool model_loaded = false;  // B_DISPATCH holds the tables of a loaded model
   bool learned_uses_split = false;  // the learned tables pick STC_STRATEGY_SPLIT somewhere
+  bool learned_uses_head = false;   // ... STC_STRATEGY_HEAD somewhere
   // The persistent count captured in a CUDA graph, and the pointers and
   // sizes it was captured with (replayed while they stay the same).
   cudaGraphExec_t graph_exec = nullptr;
-  uint64_t graph_key[16] = {};
+  uint64_t graph_key[24] = {};
+  int graph_launches = 0;  // kernels per replay of graph_exec
   stc::Tuning tuning;
 };
 
@@ -170,6 +178,7 @@ struct DeviceGraph {
   uint32_t* nbr = nullptr;    // arcs: head vertex (rank), sorted within each list
   int8_t* sgn = nullptr;      // arcs: +1 / -1
   uint32_t* fdeg = nullptr;   // out-degree by rank
+  uint32_t* asrc = nullptr;   // arcs: tail vertex (rank)
   // Batches: G graphs whose vertices (ids and ranks) are contiguous; graph
   // g owns [gbase[g], gbase[g + 1]).  G == 0 for a single graph.
   uint32_t G = 0;
@@ -184,9 +193,14 @@ struct DeviceGraph {
 // Stage timing helper: records an event when the context is timing.
 void mark(stc_ctx* c, int slot);
 
-// Graph build: input device arrays -> DeviceGraph (all fields).
+// Graph build: input device arrays -> DeviceGraph (all fields).  With
+// `totals`, for counts of totals only: the vertex order is (degree over the
+// input's edge copies, id), so no dedup runs before the orientation (the
+// arc sort drops the copies, keeping the first), and g.ukeys stays null.
+// Without it, the reference's (unique degree, id) order, which per-vertex
+// counts, shards, CSR export, the timing recorder and the autotuner use.
 void build_graph(stc_ctx* c, const uint32_t* d_src, const uint32_t* d_dst, const int8_t* d_sign,
-                 uint64_t m, DeviceGraph& g);
+                 uint64_t m, DeviceGraph& g, bool totals = false);
 // Rank-space CSR from a reference-layout forward CSR already on the device.
 void graph_from_forward_csr(stc_ctx* c, uint32_t n, uint64_t m, const uint64_t* d_off,
                             const uint32_t* d_edges, const int8_t* d_signs, const uint32_t* d_rank,
@@ -195,7 +209,7 @@ void graph_from_forward_csr(stc_ctx* c, uint32_t n, uint64_t m, const uint64_t* 
 // entries): the disjoint union with graph-major ranks; sets g.G / g.gbase.
 void build_graph_batch(stc_ctx* c, const uint32_t* d_src, const uint32_t* d_dst,
                        const int8_t* d_sign, uint64_t m, const uint64_t* h_eoff, uint32_t G,
-                       DeviceGraph& g);
+                       DeviceGraph& g, bool totals = false);
 // GPU text ingest: parses `size` bytes at d_text (device, padded to a
 // multiple of 16 bytes) into the device input arrays; returns the kept edge
 // count, the data line count and n.
@@ -222,17 +236,18 @@ struct CountConfig {
   // Persistent engine captured in a CUDA graph (STC_F_PERSISTENT).
   bool persistent = false;
   // Vertex classes to count (bit c: class c = tiny, warp, block, large,
-  // giant); the autotuner times one class at a time.
-  uint32_t class_mask = 0x1F;
+  // giant; bit 5: the head-side pass); the autotuner times one class at a
+  // time.
+  uint32_t class_mask = 0x3F;
 };
 void count_triangles(stc_ctx* c, const DeviceGraph& g, const CountConfig& cfg);
 
 // Dispatch: the fixed tables (kTableBytes, host), the per-cell features
 // (kTableBytes x kMlpIn, host), the learned tables of a model computed on
 // the device into B_DISPATCH, and the on-device training of a model.
-void fixed_dispatch_tables(uint8_t* out);
+void fixed_dispatch_tables(uint8_t* out, bool head = true);
 void dispatch_features(float* out);
-const uint8_t* dispatch_tables(stc_ctx* c, const CountConfig& cfg);
+const uint8_t* dispatch_tables(stc_ctx* c, const CountConfig& cfg, bool* uses_head = nullptr);
 void load_dispatch_model(stc_ctx* c, const float* params, const uint8_t* support);
 void train_dispatcher(stc_ctx* c, const float* features, const float* targets,
                       const float* weights, uint32_t samples, uint32_t epochs, float lr, float wd,

@@ -2,7 +2,7 @@
 // (MC/tc_serial.cpp:172-210, MC/tc_merge_sign_enu.cpp:46-154,
 // MC/tc_hash_sign_enu.cpp:76-177).
 //
-//   stc [--strategy auto|merge|hash|search|split] [--dispatch fixed|learned]
+//   stc [--strategy auto|merge|hash|search|split|head] [--dispatch fixed|learned]
 //       [--model PATH] [--zero-negative] [--host-ingest] [--device N] [--json]
 //       <graph_file>
 //
@@ -44,7 +44,7 @@ void stage(const char* label, double seconds) { std::printf("[%s] took %.4f seco
 
 int usage(const char* prog) {
   std::fprintf(stderr,
-               "usage: %s [--strategy auto|merge|hash|search|split] [--dispatch fixed|learned] "
+               "usage: %s [--strategy auto|merge|hash|search|split|head] [--dispatch fixed|learned] "
                "[--model PATH] [--zero-negative] [--host-ingest] [--device N] [--json] "
                "<graph_file>\n",
                prog);
@@ -162,6 +162,7 @@ int main(int argc, char** argv) {
       else if (v == "hash") opts.strategy = STC_STRATEGY_HASH;
       else if (v == "search") opts.strategy = STC_STRATEGY_SEARCH;
       else if (v == "split") opts.strategy = STC_STRATEGY_SPLIT;
+      else if (v == "head") opts.strategy = STC_STRATEGY_HEAD;
       else return usage(argv[0]);
     } else if (a == "--dispatch" && i + 1 < argc) {
       std::string v = argv[++i];

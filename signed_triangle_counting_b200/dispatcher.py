@@ -4,11 +4,14 @@ on the device, model files, and regret against exhaustive per-cell timing.
 The reference runs one intersection strategy per program (merge in
 "Signed_TC/Multicore Implementations/tc_merge_sign_enu.cpp:12-44", hash in
 "tc_hash_sign_enu.cpp:125-165"); this engine picks one per dispatch cell
-(class of u's list, bucket |A'|, bucket |B|).  All strategies give the same
-counts, so a dispatch table changes only speed.
+(class of u's list, bucket |A'|, bucket |B|): MERGE, HASH, SEARCH and SPLIT
+on the tail side, HEAD (A' streamed through the head's staged list) on the
+head side.  All strategies give the same counts, so a dispatch table
+changes only speed.
 
 * ``record`` runs the timing recorder once per forced strategy: exhaustive
-  per-cell timing of one graph.
+  per-cell timing of one graph (HEAD applies only to cells with |B| <= 4095;
+  elsewhere its forced run times HASH, so its cost there is unavailable).
 * ``samples`` turns a recording into training rows: the cell's features, the
   measured log2 cycles per arc of each strategy as targets, and a weight that
   grows with the cell's number of arcs.
@@ -30,17 +33,21 @@ import numpy as np
 
 from . import _capi, dispatch_features, synth
 
-STRATEGIES = ("merge", "hash", "search", "split")  # output k is strategy code k + 1
+STRATEGIES = ("merge", "hash", "search", "split", "head")  # output k is strategy code k + 1
 STAGED_ONLY = (1, 3)  # outputs (HASH, SPLIT) that need the staged hash
+SPLIT, HEAD = 3, 4    # outputs of the SPLIT and HEAD strategies
+HEAD_MAX_BUCKET = 12  # HEAD applies to cells whose bucket |B| is at most this
 GIANT = 3                                  # class index whose lists stage no hash
+DEFAULT_STRATEGIES = ("merge", "hash", "search", "head")  # what the shipped model chooses from
 DEFAULT_MODEL = Path(__file__).resolve().parent / "dispatch_model.json"
-FORMAT_VERSION = 3
+FORMAT_VERSION = 4
 
 
 def record(ctx, src, dst, sign) -> dict:
-    """Per-cell cycles of every strategy on one graph (four timed runs).
+    """Per-cell cycles of every strategy on one graph (one timed run per
+    strategy).
 
-    Returns {"cycles": (4, CELLS) float64, "arcs": (CELLS,) float64,
+    Returns {"cycles": (5, CELLS) float64, "arcs": (CELLS,) float64,
     "counts": GlobalTriCounts}; raises if the strategies disagree on the
     counts or on which arcs they timed."""
     cycles, arcs, counts = [], None, None
@@ -60,13 +67,14 @@ def merge(records) -> dict:
 
 
 def cell_costs(rec) -> np.ndarray:
-    """Mean cycles per arc, (4, CELLS); HASH and SPLIT are unavailable in the
-    giant class (its arcs run MERGE), so they cost infinity there; empty
-    cells cost 0."""
+    """Mean cycles per arc, (5, CELLS); HASH and SPLIT are unavailable in the
+    giant class (its arcs run MERGE), and HEAD in cells with bucket |B| > 12,
+    so they cost infinity there; empty cells cost 0."""
     arcs = rec["arcs"]
     cost = np.divide(rec["cycles"], np.maximum(arcs, 1.0)[None, :])
     for k in STAGED_ONLY:
         cost[k, GIANT * 256:(GIANT + 1) * 256] = np.inf
+    cost[HEAD, (np.arange(cost.shape[1]) & 15) > HEAD_MAX_BUCKET] = np.inf
     return cost
 
 
@@ -89,9 +97,9 @@ def samples(rec, min_arcs: int = 32, weight_power: float = 0.5):
     return X, targets.astype(np.float32), w.astype(np.float32), cells
 
 
-def regret(rec, tables, strategies=STRATEGIES[:3]) -> dict:
+def regret(rec, tables, strategies=DEFAULT_STRATEGIES) -> dict:
     """Cycles a dispatch table would spend on a recording, relative to the
-    per-cell best of ``strategies`` (by default the three the shipped model
+    per-cell best of ``strategies`` (by default the four the shipped model
     chooses from).  ``tables``: strategy codes, (4, 16, 16) or flat."""
     t = np.asarray(tables).reshape(-1).astype(np.int64)
     arcs = rec["arcs"]
@@ -101,8 +109,10 @@ def regret(rec, tables, strategies=STRATEGIES[:3]) -> dict:
         if name not in strategies:
             best_cost[k] = np.inf
     k = t - 1
-    # The giant class runs MERGE where a table says HASH or SPLIT.
+    # The giant class runs MERGE where a table says HASH or SPLIT; a HEAD
+    # cell beyond bucket |B| 12 runs HASH (MERGE in the giant class).
     giant = np.arange(len(t)) // 256 == GIANT
+    k = np.where((k == HEAD) & ((np.arange(len(t)) & 15) > HEAD_MAX_BUCKET), 1, k)
     k = np.where(giant & np.isin(k, STAGED_ONLY), 0, k)
     used = arcs > 0
     chosen = cost[k, np.arange(len(t))]
@@ -130,12 +140,12 @@ def train(ctx, rec, *, epochs: int = 3000, lr: float = 0.02, weight_decay: float
     X, T, w, cells = samples(rec, min_arcs, weight_power)
     if not use_split:
         T = T.copy()
-        T[:, 3] = np.nan
+        T[:, SPLIT] = np.nan
     params, loss = ctx.train_dispatcher(X, T, w, epochs=epochs, lr=lr, weight_decay=weight_decay,
                                         seed=seed)
     if not use_split:
         params = params.copy()
-        params[-1] = EXCLUDED_BIAS
+        params[len(params) - len(STRATEGIES) + SPLIT] = EXCLUDED_BIAS
     # The model overrides the fixed tables only on the cells its training
     # data covered.
     ctx.set_dispatch_model(params, cells)
@@ -144,7 +154,7 @@ def train(ctx, rec, *, epochs: int = 3000, lr: float = 0.02, weight_decay: float
     acc = float((w * (pred == best)).sum())
     info = {"samples": int(len(cells)), "support": [int(c) for c in cells], "loss": loss,
             "weighted_accuracy": acc,
-            "strategies": list(STRATEGIES if use_split else STRATEGIES[:3]),
+            "strategies": list(STRATEGIES if use_split else DEFAULT_STRATEGIES),
             "objective": "log2 cycles per arc, weighted squared error", "epochs": epochs,
             "lr": lr, "weight_decay": weight_decay, "seed": seed, "min_arcs": min_arcs,
             "weight_power": weight_power}
@@ -153,8 +163,8 @@ def train(ctx, rec, *, epochs: int = 3000, lr: float = 0.02, weight_decay: float
 
 def save(path, params, meta: dict) -> None:
     doc = {"format": FORMAT_VERSION, "kind": "stc-dispatch-mlp",
-           "layout": "W1[16][6], b1[16], W2[4][16], b2[4]; outputs: log2 cycles per arc "
-                     "of merge, hash, search, split",
+           "layout": "W1[16][6], b1[16], W2[5][16], b2[5]; outputs: log2 cycles per arc "
+                     "of merge, hash, search, split, head",
            "params": [float(x) for x in np.asarray(params, np.float32)]}
     doc.update(meta)
     Path(path).write_text(json.dumps(doc, indent=1) + "\n")
@@ -241,9 +251,11 @@ def _main() -> None:
             np.savez(a.save_recording, names=np.array([f"workload{a.workload}"]),
                      cycles=rec["cycles"][None], arcs=rec["arcs"][None])
         out = {"gpu": gpu, "workload": a.workload, "model_trained_on": model.get("trained_on"),
-               "fixed": regret(rec, ctx.dispatch_tables("fixed"), model.get("strategies", STRATEGIES[:3])),
-               "learned": regret(rec, ctx.dispatch_tables("learned"), model.get("strategies", STRATEGIES[:3])),
-               "learned_vs_all_four": regret(rec, ctx.dispatch_tables("learned"), STRATEGIES),
+               "fixed": regret(rec, ctx.dispatch_tables("fixed"),
+                               model.get("strategies", DEFAULT_STRATEGIES)),
+               "learned": regret(rec, ctx.dispatch_tables("learned"),
+                                 model.get("strategies", DEFAULT_STRATEGIES)),
+               "learned_vs_all": regret(rec, ctx.dispatch_tables("learned"), STRATEGIES),
                "counts": rec["counts"].as_tuple()}
         print(json.dumps(out), flush=True)
 

@@ -25,21 +25,32 @@ def fake_recording(seed=0):
     rng = np.random.default_rng(seed)
     arcs = rng.integers(0, 200, _capi.DISPATCH_CELLS).astype(np.float64)
     arcs[rng.random(_capi.DISPATCH_CELLS) < 0.3] = 0
-    per_arc = rng.uniform(100, 1000, (4, _capi.DISPATCH_CELLS))
+    per_arc = rng.uniform(100, 1000, (5, _capi.DISPATCH_CELLS))
     per_arc[1, 768:] = per_arc[0, 768:]  # giant: HASH and SPLIT run as MERGE
     per_arc[3, 768:] = per_arc[0, 768:]
+    wide = (np.arange(_capi.DISPATCH_CELLS) & 15) > 12  # HEAD runs as HASH where |B| > 4095
+    per_arc[4, wide] = per_arc[1, wide]
     return {"cycles": per_arc * arcs, "arcs": arcs}
+
+
+def unavailable():
+    """(strategy, cell) pairs a recording cannot price: HASH and SPLIT in the
+    giant class, HEAD where bucket |B| > 12."""
+    na = np.zeros((5, _capi.DISPATCH_CELLS), bool)
+    na[[1, 3], 768:] = True
+    na[4, (np.arange(_capi.DISPATCH_CELLS) & 15) > 12] = True
+    return na
 
 
 def test_samples_targets_and_weights():
     rec = fake_recording()
     X, T, w, cells = dispatcher.samples(rec, min_arcs=32)
     assert (rec["arcs"][cells] >= 32).all()
-    assert len(X) == len(T) == len(w) == len(cells) and T.shape[1] == 4
+    assert len(X) == len(T) == len(w) == len(cells) and T.shape[1] == 5
     cost = rec["cycles"][:, cells] / rec["arcs"][cells]
-    giant = cells >= 768
-    np.testing.assert_allclose(T[~giant], np.log2(cost[:, ~giant]).T, rtol=1e-6)
-    assert np.isnan(T[giant][:, [1, 3]]).all() and not np.isnan(T[giant][:, [0, 2]]).any()
+    na = unavailable()[:, cells].T
+    np.testing.assert_allclose(T[~na], np.log2(cost.T[~na]), rtol=1e-6)
+    assert np.isnan(T[na]).all()
     np.testing.assert_allclose(w, np.sqrt(rec["arcs"][cells]) / np.sqrt(rec["arcs"][cells]).sum(),
                                rtol=1e-5)
     np.testing.assert_array_equal(X, stc.dispatch_features()[cells])
@@ -48,11 +59,10 @@ def test_samples_targets_and_weights():
 def test_regret_of_best_and_worst_tables():
     rec = fake_recording(1)
     cost = rec["cycles"] / np.maximum(rec["arcs"], 1)
-    cost[1, 768:] = np.inf
-    cost[3, 768:] = np.inf
+    cost[unavailable()] = np.inf
     best = np.argmin(cost, axis=0) + 1
     assert dispatcher.regret(rec, best, dispatcher.STRATEGIES)["ratio"] == pytest.approx(1.0)
-    # Judged against three strategies, a table that uses SPLIT may beat 1.0.
+    # Judged against four strategies, a table that uses SPLIT may beat 1.0.
     assert dispatcher.regret(rec, best)["ratio"] <= 1.0 + 1e-12
     worst = np.argmax(np.where(np.isfinite(cost), cost, -np.inf), axis=0) + 1
     assert dispatcher.regret(rec, worst, dispatcher.STRATEGIES)["ratio"] > 1.2
@@ -64,6 +74,11 @@ def test_regret_of_best_and_worst_tables():
         t = best.copy()
         t[768:] = code
         assert dispatcher.regret(rec, t)["cycles"] == pytest.approx(dispatcher.regret(rec, t2)["cycles"])
+    # A HEAD cell beyond bucket |B| 12 is charged the HASH cost.
+    wide = ((np.arange(_capi.DISPATCH_CELLS) & 15) > 12) & (np.arange(_capi.DISPATCH_CELLS) < 768)
+    th, tg = best.copy(), best.copy()
+    th[wide], tg[wide] = 5, 2
+    assert dispatcher.regret(rec, th)["cycles"] == pytest.approx(dispatcher.regret(rec, tg)["cycles"])
 
 
 def test_model_file_round_trip(tmp_path):

@@ -52,7 +52,7 @@ def test_recorder_counts_and_cells(ctx, name):
     el = GRAPHS[name]()
     want = oracle.count_arrays(el.src, el.dst, el.sign)
     cells = expected_cells(el)
-    for s in ("merge", "hash", "search", "split", "auto"):
+    for s in ("merge", "hash", "search", "split", "head", "auto"):
         cycles, arcs, c = ctx.record_bucket_times(el.src, el.dst, el.sign, strategy=s)
         assert c.as_tuple() == want, s
         np.testing.assert_array_equal(arcs, cells, err_msg=s)
@@ -62,10 +62,16 @@ def test_recorder_counts_and_cells(ctx, name):
 
 
 def fixed_rule():
+    """The fixed table: HEAD where |A'| is not the longer list and |B| <= 4095
+    (bucket a <= b <= 12), SEARCH where B is 16x longer, MERGE where both
+    are short, HASH elsewhere."""
     t = np.zeros((4, 16, 16), np.uint8)
     for a in range(16):
         for b in range(16):
-            t[:, a, b] = 3 if b >= a + 4 else (1 if a <= 3 and b <= 5 else 2)
+            if 1 <= b <= 12 and a <= b:
+                t[:, a, b] = 5
+            else:
+                t[:, a, b] = 3 if b >= a + 4 else (1 if a <= 3 and b <= 5 else 2)
     return t
 
 
@@ -82,16 +88,19 @@ MARGIN = np.log2(1.05)
 def numpy_tables(params, support=None):
     """The inference kernel restated: the least predicted cost where it beats
     the fixed table's choice by the margin, else the fixed choice; no HASH or
-    SPLIT in the giant class.  Also returns each cell's decision gap (near
-    zero: float rounding may decide either way)."""
+    SPLIT in the giant class, no HEAD where bucket |B| > 12.  Also returns
+    each cell's decision gap (near zero: float rounding may decide either
+    way)."""
     p = np.asarray(params, np.float64)
     W1, b1 = p[:96].reshape(16, 6), p[96:112]
-    W2, b2 = p[112:176].reshape(4, 16), p[176:180]
+    W2, b2 = p[112:192].reshape(5, 16), p[192:197]
     X = stc.dispatch_features().astype(np.float64)
     z = np.maximum(X @ W1.T + b1, 0) @ W2.T + b2
-    giant = np.arange(len(X)) // 256 == 3
+    cell = np.arange(len(X))
+    giant = cell // 256 == 3
     z[giant, 1] = np.inf
     z[giant, 3] = np.inf
+    z[(cell & 15) > 12, 4] = np.inf
     fixed = fixed_rule().reshape(-1).astype(np.int64)
     fx = np.where(giant & np.isin(fixed, (2, 4)), 1, fixed) - 1
     best = np.argmin(z, axis=1)
@@ -99,7 +108,8 @@ def numpy_tables(params, support=None):
     take = zb + MARGIN < zf
     if support is not None:
         take &= np.asarray(support, bool)
-    gap = np.minimum(np.abs(zf - zb - MARGIN), np.sort(z, axis=1)[:, 1] - np.sort(z, axis=1)[:, 0])
+    zs = np.sort(z, axis=1)
+    gap = np.minimum(np.abs(zf - zb - MARGIN), zs[:, 1] - zs[:, 0])
     return np.where(take, best + 1, fixed), gap
 
 
@@ -120,25 +130,29 @@ def test_inference_matches_numpy(ctx):
         want_s, gap_s = numpy_tables(params, support)
         assert ((got_s == want_s) | (gap_s < 1e-4)).all(), trial
         assert (got_s[~support] == fixed_rule().reshape(-1)[~support]).all()
-        assert set(np.unique(got)) <= {1, 2, 3, 4}
+        assert set(np.unique(got)) <= {1, 2, 3, 4, 5}
         # Giant lists stage no hash: never SPLIT, and HASH only where the
-        # fixed table (whose giant HASH cells run MERGE) already holds it.
+        # fixed table (whose giant HASH cells run MERGE) already holds it;
+        # HEAD only where |B| <= 4095.
         fixed = fixed_rule().reshape(-1)
         assert not (got[768:] == 4).any()
         assert ((got[768:] != 2) | (fixed[768:] == 2)).all()
+        assert not (got[(np.arange(len(got)) & 15) > 12] == 5).any()
     ctx.set_dispatch_model(None)
 
 
 def synthetic_costs():
     """log2 cycles per arc of a made-up cost model over every cell:
     merge ~ |A'| + |B|, hash ~ 2 |B|, search ~ 4 |A'| log |B|, split ~
-    1.2 |B| + 2^8; HASH and SPLIT are unavailable (NaN) in the giant class."""
+    1.2 |B| + 2^8, head ~ 2 |A'| + 2^6; HASH and SPLIT are unavailable (NaN)
+    in the giant class, HEAD where bucket |B| > 12."""
     cell = np.arange(_capi.DISPATCH_CELLS)
     a, b = ((cell >> 4) & 15).astype(float), (cell & 15).astype(float)
     T = np.stack([np.log2(2 ** a + 2 ** b), 1 + b, 2 + a + np.log2(1 + b),
-                  np.log2(1.2 * 2 ** b + 256)], axis=1)
+                  np.log2(1.2 * 2 ** b + 256), np.log2(2 * 2 ** a + 64)], axis=1)
     T[768:, 1] = np.nan
     T[768:, 3] = np.nan
+    T[(cell & 15) > 12, 4] = np.nan
     return stc.dispatch_features(), T.astype(np.float32)
 
 
@@ -170,6 +184,7 @@ def test_training_fits_and_is_deterministic(ctx):
     rows = np.arange(len(T))
     assert (2.0 ** Tm[rows, pe]).sum() < (2.0 ** Tm[rows, fx]).sum()
     assert not (pred[768:] == 4).any() and ((pred[768:] != 2) | (fixed[768:] == 2)).all()
+    assert not (pred[(np.arange(len(pred)) & 15) > 12] == 5).any()
     assert (best == 4).any() and (pred == 4).any()  # the model picks SPLIT where it is cheapest
     ctx.set_dispatch_model(None)
 
@@ -184,7 +199,7 @@ def test_training_rejects_bad_input(ctx):
     with pytest.raises(stc.StcError):
         ctx.train_dispatcher(X, T, -w)
     with pytest.raises(stc.StcError):
-        ctx.train_dispatcher(np.zeros((5000, 6), np.float32), np.zeros((5000, 4), np.float32),
+        ctx.train_dispatcher(np.zeros((5000, 6), np.float32), np.zeros((5000, 5), np.float32),
                              np.ones(5000, np.float32))
     with pytest.raises(stc.StcError):
         ctx.set_dispatch_model(np.full(_capi.DISPATCH_MODEL_PARAMS, np.nan, np.float32))
@@ -204,8 +219,9 @@ def test_learned_dispatch_is_exact(ctx, name):
 def test_shipped_model(ctx):
     model = ctx.load_dispatch_model()
     t = ctx.dispatch_tables("learned")
-    assert set(np.unique(t)) <= {1, 2, 3, 4} and not (t[3] == 4).any()
+    assert set(np.unique(t)) <= {1, 2, 3, 4, 5} and not (t[3] == 4).any()
     assert ((t[3] != 2) | (fixed_rule()[3] == 2)).all()
+    assert not (t[:, :, 13:] == 5).any()
     # Judged by regret on its training recordings (near-ties make per-cell
     # accuracy a poor measure): learned must beat the fixed tables.
     assert model["train_regret_learned"] < model["train_regret_fixed"]
@@ -239,7 +255,7 @@ def test_giant_class_dense_clique(ctx):
     want = clique_counts(S)
     perm = rng.permutation(k).astype(np.uint32)  # ids not in degree order
     src, dst = perm[a], perm[b]
-    for strategy in ("auto", "merge", "hash", "search", "split"):
+    for strategy in ("auto", "merge", "hash", "search", "split", "head"):
         assert ctx.count(src, dst, s, strategy=strategy).as_tuple() == want, strategy
     _, arcs, c = ctx.record_bucket_times(src, dst, s, strategy="search")
     assert c.as_tuple() == want

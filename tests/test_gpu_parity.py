@@ -20,7 +20,7 @@ pytestmark = pytest.mark.gpu
 
 ROOT = Path(__file__).resolve().parents[1]
 CLI = ROOT / "signed_triangle_counting_b200" / "stc"
-STRATEGIES = ["auto", "merge", "hash", "search", "split"]
+STRATEGIES = ["auto", "merge", "hash", "search", "split", "head"]
 
 
 def small_graph(family: str, seed: int = 1):
