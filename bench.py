@@ -458,12 +458,13 @@ def run_gpu(args) -> None:
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    count_ms, launches, alg_bytes = [], 0, 0
+    count_ms, launches, alg_bytes, probe_bytes = [], 0, 0, 0
     for _ in range(args.steps):
         counts, st = step()
         count_ms.append(st.ms_count)
         launches += st.kernel_launches
         alg_bytes = st.alg_bytes
+        probe_bytes = st.probe_bytes
     e1.record(stream)
     torch.cuda.synchronize()
     clocks = sampler.stop()
@@ -537,7 +538,8 @@ def run_gpu(args) -> None:
     if rank == 0:
         peaks = load_peaks()
         cms = statistics.mean(count_ms)
-        achieved = alg_bytes / (cms / 1e3) / 1e9
+        achieved = probe_bytes / (cms / 1e3) / 1e9
+        merge_achieved = alg_bytes / (cms / 1e3) / 1e9
         traffic = load_traffic(args.workload, args.rmat_scale)
         cpu = None
         if world == 1 and args.workload == 3 and not args.skip_cpu:
@@ -573,8 +575,11 @@ def run_gpu(args) -> None:
             "roofline": {"bound": "hbm", "kernel": "intersection engine (count)",
                          "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
-                         "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
-                         "count_ms": cms},
+                         "traffic": traffic, "model": "probe: 5 min(|A'|, |B|) + 30 per arc",
+                         "alg_bytes_per_launch": probe_bytes, "count_ms": cms,
+                         "merge_model_bytes": alg_bytes,
+                         "merge_model_achieved": merge_achieved,
+                         "merge_model_frac": merge_achieved / peaks["hbm_gbs"]},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(m_input) * 9,
                     "d2h_bytes_per_step": 32 * G_run, "steps": e2e_steps,

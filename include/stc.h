@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define STC_ABI_VERSION 1
+#define STC_ABI_VERSION 2
 
 typedef enum stc_status {
   STC_OK = 0,
@@ -146,6 +146,9 @@ typedef struct stc_stats {
   double ms_total;        /* whole call on the device */
   uint32_t kernel_launches;
   uint32_t reserved;
+  uint64_t probe_bytes;   /* probe-model bytes: sum over arcs of 5 min(|A'|, |B|) + 30, the
+                             shorter list of each arc streamed once (A' = the part of N+(u)
+                             after v, B = N+(v)), the arc's 25 bytes and its entry staged */
 } stc_stats;
 
 typedef struct stc_ctx stc_ctx;

@@ -115,6 +115,7 @@ class Stats:
     ms_count: float
     ms_total: float
     kernel_launches: int
+    probe_bytes: int
 
 
 def _check(status: int, ctx=None) -> None:

@@ -214,15 +214,30 @@ struct EmitOffset {
   __device__ void operator()(uint64_t i, uint64_t pos, uint32_t) const { off[i] = pos; }
 };
 
+// Algorithmic bytes of the arc at position i (tail u, head v) of a sorted
+// CSR: the merge model, 5 (d+(u) + d+(v)) + 25, which a merge of both lists
+// reads, and the probe model, 5 min(|A'|, |B|) + 30 (A' = the part of N+(u)
+// after v, B = N+(v)), which a hash probe that streams the shorter list
+// reads, with the arc's own 25 bytes and its entry staged once.
+__device__ __forceinline__ void arc_bytes(uint64_t i, uint32_t u, uint32_t v,
+                                          const uint64_t* __restrict__ off,
+                                          const uint32_t* __restrict__ fdeg,
+                                          unsigned long long& merge, unsigned long long& probe) {
+  const uint64_t du = fdeg[u], dv = fdeg[v];
+  merge += 5ull * (du + dv) + 25ull;
+  const uint64_t alen = off[u + 1] - i - 1;
+  probe += 5ull * (alen < dv ? alen : dv) + 30ull;
+}
+
 // Splits sorted arc keys into the neighbour, sign and tail arrays (the tail
-// array only when `asrc` is given) and accumulates the merge-model byte count
-// 5 (d+(u) + d+(v)) + 25 per arc.
+// array only when `asrc` is given) and accumulates the merge-model and
+// probe-model bytes of every arc (arc_bytes).
 __global__ void k_csr_fill(const uint64_t* __restrict__ akeys, uint64_t ma, uint32_t bits,
-                           const uint32_t* __restrict__ fdeg, uint32_t* __restrict__ nbr,
-                           int8_t* __restrict__ sgn, uint32_t* __restrict__ asrc,
-                           unsigned long long* __restrict__ ctr) {
+                           const uint32_t* __restrict__ fdeg, const uint64_t* __restrict__ off,
+                           uint32_t* __restrict__ nbr, int8_t* __restrict__ sgn,
+                           uint32_t* __restrict__ asrc, unsigned long long* __restrict__ ctr) {
   const uint64_t idmask = (1ull << bits) - 1;
-  unsigned long long bytes = 0;
+  unsigned long long bytes = 0, probe = 0;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ma; i += stride) {
     const uint64_t k = akeys[i];
@@ -230,10 +245,14 @@ __global__ void k_csr_fill(const uint64_t* __restrict__ akeys, uint64_t ma, uint
     nbr[i] = dst;
     sgn[i] = (k >> 63) ? (int8_t)-1 : (int8_t)1;
     if (asrc) asrc[i] = src;
-    bytes += 5ull * ((unsigned long long)fdeg[src] + fdeg[dst]) + 25ull;
+    arc_bytes(i, src, dst, off, fdeg, bytes, probe);
   }
   bytes = warp_sum(bytes);
-  if (lane_id() == 0 && bytes) atomicAdd(ctr + C_ALG_BYTES, bytes);
+  probe = warp_sum(probe);
+  if (lane_id() == 0 && bytes) {
+    atomicAdd(ctr + C_ALG_BYTES, bytes);
+    atomicAdd(ctr + C_PROBE_BYTES, probe);
+  }
 }
 
 // Arc keys of a reference-layout CSR: one warp per vertex.
@@ -293,7 +312,7 @@ void finish_csr_from_arc_keys(stc_ctx* c, DeviceGraph& g, uint64_t* akeys, uint6
   g.sgn = buffer<int8_t>(c, B_SGN, g.m_fwd + 4);
   g.asrc = buffer<uint32_t>(c, B_ASRC, g.m_fwd);
   k_csr_fill<<<grid_for(g.m_fwd, 4), kThreads, 0, c->stream>>>(sorted, g.m_fwd, g.bits, g.fdeg,
-                                                               g.nbr, g.sgn, g.asrc,
+                                                               g.off, g.nbr, g.sgn, g.asrc,
                                                                (unsigned long long*)counters(c));
   c->launches += 1;
   STC_CUDA(cudaGetLastError());
@@ -423,15 +442,29 @@ struct EdgeCursor {
   }
 };
 
-// Degree of every vertex over the input's edge copies (self-loops skipped).
-// Endpoints are scattered and a few hubs own millions of copies, so each CTA
-// first adds them in a shared-memory table per tile of kRawTile edges and
-// flushes the slots it used with one global atomic each (an endpoint that
-// finds no free slot within kDegProbes probes is added directly).
+// Degree of every vertex over the input's edge copies (self-loops skipped),
+// or over a sample of them: with `shift` > 0, only the copies of the edges
+// {a, b} whose hash has its top `shift` bits clear, 1 in 2^shift of the
+// distinct edges (every copy of an edge is in or out together).  The order
+// only has to be a total order for exact counts; on dense power-law graphs
+// a sampled degree orders the vertices nearly as well (at RMAT scale 20 a
+// 1/4 sample moves the intersection work by under 0.1%) for a quarter of
+// the atomics.  Endpoints are scattered and a few hubs own millions of
+// copies, so each CTA first adds them in a shared-memory table per tile of
+// kRawTile edges and flushes the slots it used with one global atomic each
+// (an endpoint that finds no free slot within kDegProbes probes is added
+// directly).
 constexpr int kRawTile = 512;
 constexpr int kRawSlots = 2048;  // 2 kRawTile endpoints per tile: load <= 1/2
 
+__device__ __forceinline__ bool sampled_edge(uint32_t a, uint32_t b, uint32_t shift) {
+  if (shift == 0) return true;
+  const uint32_t lo = min(a, b), hi = max(a, b);
+  return ((lo * 0x9E3779B1u) ^ (hi * 0x7FEB352Du) ^ ((lo ^ hi) >> 15)) >> (32 - shift) == 0;
+}
+
 __global__ void __launch_bounds__(kThreads) k_degree_raw(EdgeIds e, uint64_t m, uint64_t per_cta,
+                                                         uint32_t shift,
                                                          uint32_t* __restrict__ deg) {
   __shared__ uint32_t tkey[kRawSlots], tcnt[kRawSlots], used[kRawSlots];
   __shared__ uint32_t nused;
@@ -453,7 +486,7 @@ __global__ void __launch_bounds__(kThreads) k_degree_raw(EdgeIds e, uint64_t m, 
       uint32_t a = kFree, b = kFree;
       if (i < end) {
         cur.at(e, i, a, b);
-        if (a == b) a = b = kFree;
+        if (a == b || !sampled_edge(a, b, shift)) a = b = kFree;
       }
 #pragma unroll
       for (int side = 0; side < 2; side++) {
@@ -550,20 +583,25 @@ __global__ void k_fdeg_count(const uint32_t* __restrict__ asrc, uint64_t m,
   }
 }
 
-// The merge-model byte count 5 (d+(u) + d+(v)) + 25 per arc.
+// The merge-model and probe-model bytes of every arc (arc_bytes).
 __global__ void k_alg_bytes(const uint32_t* __restrict__ asrc, const uint32_t* __restrict__ nbr,
-                            uint64_t m, const uint32_t* __restrict__ fdeg,
-                            unsigned long long* __restrict__ ctr) {
-  unsigned long long bytes = 0;
+                            uint64_t m, const uint64_t* __restrict__ off,
+                            const uint32_t* __restrict__ fdeg, unsigned long long* __restrict__ ctr) {
+  unsigned long long bytes = 0, probe = 0;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride)
-    bytes += 5ull * ((unsigned long long)fdeg[asrc[i]] + fdeg[nbr[i]]) + 25ull;
+    arc_bytes(i, asrc[i], nbr[i], off, fdeg, bytes, probe);
   bytes = warp_sum(bytes);
-  if (lane_id() == 0 && bytes) atomicAdd(ctr + C_ALG_BYTES, bytes);
+  probe = warp_sum(probe);
+  if (lane_id() == 0 && bytes) {
+    atomicAdd(ctr + C_ALG_BYTES, bytes);
+    atomicAdd(ctr + C_PROBE_BYTES, probe);
+  }
 }
 
 // Steps 2-6 of the totals path, after the ids (g.n, g.bits, g.m_valid set):
-// degrees over the edge copies, (degree, id) rank (graph-major for a batch
+// degrees over the edge copies (sampled on dense graphs), (degree, id) rank
+// (graph-major for a batch
 // with vertex bases d_vbase), arc keys of every copy, their sort, the first
 // of each run of equal arcs, offsets.  g.ukeys stays null.
 void build_totals(stc_ctx* c, const EdgeIds& e, const int8_t* d_sign, uint64_t m, DeviceGraph& g,
@@ -583,7 +621,12 @@ void build_totals(stc_ctx* c, const EdgeIds& e, const int8_t* d_sign, uint64_t m
     STC_CUDA(cudaMemsetAsync(g.fdeg, 0, (size_t)g.n * sizeof(uint32_t), st));
   }
   if (g.m_valid) {
-    k_degree_raw<<<ep.grid, kThreads, 0, st>>>(e, m, ep.per_cta, g.deg);
+    // Sample 1 in 2^shift edges once the average degree reaches 16 (2 m / n
+    // >= 16): shift = bit width of m / n, less 3, at most 3.
+    const uint64_t ratio = g.m_valid / std::max<uint64_t>(1, g.n);
+    const uint32_t bw = bit_width64(ratio);
+    const uint32_t shift = bw > 3 ? std::min<uint32_t>(3, bw - 3) : 0;
+    k_degree_raw<<<ep.grid, kThreads, 0, st>>>(e, m, ep.per_cta, shift, g.deg);
     c->launches++;
   }
   STC_CUDA(cudaGetLastError());
@@ -643,7 +686,8 @@ void build_totals(stc_ctx* c, const EdgeIds& e, const int8_t* d_sign, uint64_t m
     STC_CUDA(cudaMemsetAsync(g.off, 0, sizeof(uint64_t), st));
   }
   if (g.m_fwd) {
-    k_alg_bytes<<<grid_for(g.m_fwd, 4), kThreads, 0, st>>>(g.asrc, g.nbr, g.m_fwd, g.fdeg, ctr);
+    k_alg_bytes<<<grid_for(g.m_fwd, 4), kThreads, 0, st>>>(g.asrc, g.nbr, g.m_fwd, g.off, g.fdeg,
+                                                           ctr);
     c->launches++;
   } else {
     g.nbr = buffer<uint32_t>(c, B_NBR, 4);
@@ -921,8 +965,9 @@ void export_forward_csr(stc_ctx* c, const DeviceGraph& g, stc_forward_csr* out) 
                              sizeof(uint64_t), cudaMemcpyDeviceToDevice, st));
   }
   if (mu) {
-    k_csr_fill<<<grid_for(mu, 4), kThreads, 0, st>>>(sorted, mu, g.bits, fdeg_id, edges, signs,
-                                                     nullptr, (unsigned long long*)counters(c));
+    k_csr_fill<<<grid_for(mu, 4), kThreads, 0, st>>>(sorted, mu, g.bits, fdeg_id, off_id, edges,
+                                                     signs, nullptr,
+                                                     (unsigned long long*)counters(c));
   }
   STC_CUDA(cudaGetLastError());
   out->n = n;

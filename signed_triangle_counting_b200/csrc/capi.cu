@@ -94,6 +94,7 @@ void end_call(stc_ctx* c, const DeviceGraph& g, stc_counts* out) {
   s.m_unique = g.m_unique;
   s.m_forward = g.m_fwd;
   s.alg_bytes = c->h_pinned[C_ALG_BYTES];
+  s.probe_bytes = c->h_pinned[C_PROBE_BYTES];
   s.triangles = c->h_pinned[C_T0] + c->h_pinned[C_T1] + c->h_pinned[C_T2] + c->h_pinned[C_T3];
   s.kernel_launches = (uint32_t)c->launches;
   if (c->timing) {
@@ -530,6 +531,7 @@ stc_status stc_count_batch_packed(stc_ctx* c, const uint32_t* src, const uint32_
       total.m_unique += g.m_unique;
       total.m_forward += g.m_fwd;
       total.alg_bytes += c->h_pinned[C_ALG_BYTES];
+      total.probe_bytes += c->h_pinned[C_PROBE_BYTES];
       g0 = g1;
     }
     mark(c, 7);

@@ -1150,7 +1150,11 @@ void launch_classes(cudaStream_t st, const Csr& csr, const uint32_t* lists, cons
 // stable radix sort over the vertex bits groups each head's in-arcs, and
 // the runs of equal v are its in-arc ranges.  Head vertices are classed by
 // |N+(v)|, the list they stage: warp (<= 128), block (<= 1024) and large
-// (<= 4095).  Each in-arc is one "arc" of the staged tile with extent
+// (<= 4095).  A work item is a piece of one head's run that does not cross
+// a multiple of its class's item size (a hub with millions of in-arcs
+// becomes thousands of items, each staging its small N+(v) again), so no
+// warp or CTA is left with one huge run.  Each in-arc is one "arc" of the
+// staged tile with extent
 // [i + 1, end of u's list), its sign s(u, v), strategy HASH: the tail
 // side's stream pass then runs unchanged, with the hash keys carrying
 // s(v, w), the streamed sign bytes s(u, w) and the arc's sign s(u, v).
@@ -1163,6 +1167,12 @@ constexpr int kHeadClasses = 3;
 // vertex: whether it keeps arcs for the tail side.
 constexpr uint32_t kHeadPlanCount = 4;
 constexpr uint32_t kHeadPlanWords = 8;
+constexpr uint32_t kHeadItemMin = 2048;  // the smallest class item size
+
+// In-arcs per work item of head class c (powers of two).
+__host__ __device__ __forceinline__ uint32_t head_item(uint32_t c) {
+  return c == 0 ? kHeadItemMin : c == 1 ? 8192u : 16384u;
+}
 
 // Table class of a list of d arcs (tiny lists use the warp class's table).
 __device__ __forceinline__ uint32_t table_class(uint32_t d) {
@@ -1177,9 +1187,13 @@ __device__ __forceinline__ uint32_t head_class(uint32_t d) {
 struct HeadArcs {
   const uint64_t* __restrict__ keys;  // sorted: v << 32 | arc index
   const uint32_t* __restrict__ aend;  // per arc: end of its tail's list in the CSR
-  const uint32_t* __restrict__ beg;   // per head vertex: its first in-arc entry
-  const uint32_t* __restrict__ end;   // ... and one past its last
+  const uint32_t* __restrict__ end;   // per head vertex: one past its last in-arc entry
   const uint32_t* __restrict__ asrc;  // per arc: its tail (timing recorder only)
+  // Work item starting at entry j0 of head class c: its head and its end.
+  __device__ __forceinline__ void item(uint32_t j0, uint32_t c, uint32_t& v, uint32_t& j1) const {
+    v = (uint32_t)(keys[j0] >> 32);
+    j1 = min(end[v], (j0 | (head_item(c) - 1)) + 1);
+  }
 };
 
 // Keys of the HEAD arcs (and sentinels), every arc's list end, and need[u]
@@ -1216,15 +1230,15 @@ __global__ void __launch_bounds__(256) k_head_keys(Csr g, const uint32_t* __rest
   }
 }
 
-// Runs of equal head vertex in the sorted keys.  Without kFill: counts the
-// head vertices of each class.  With kFill: appends each head vertex to its
-// class list and records its in-arc range [beg, end).
+// Work items in the sorted keys: an entry starts one where its head's run
+// starts or where it is a multiple of its class's item size.  Without
+// kFill: counts the items of each class.  With kFill: appends each item's
+// first entry to its class list and records the end of every run.
 template <bool kFill>
 __global__ void __launch_bounds__(256) k_head_runs(const uint64_t* __restrict__ keys, uint64_t m,
                                                    uint32_t vbits, const uint64_t* __restrict__ off,
                                                    unsigned long long* __restrict__ ctr,
                                                    uint32_t* __restrict__ hl,
-                                                   uint32_t* __restrict__ beg,
                                                    uint32_t* __restrict__ end) {
   const uint64_t none = (1ull << vbits) - 1;
   const uint32_t lane = lane_id();
@@ -1233,13 +1247,13 @@ __global__ void __launch_bounds__(256) k_head_runs(const uint64_t* __restrict__ 
   for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < m;
        base += stride) {
     const uint64_t j = base + lane;
-    uint32_t c = kHeadClasses;  // not a run start
-    uint32_t v = 0;
+    uint32_t c = kHeadClasses;  // not an item start
     if (j < m) {
       const uint64_t kv = keys[j] >> 32;
       if (kv != none) {
-        v = (uint32_t)kv;
-        if (j == 0 || (keys[j - 1] >> 32) != kv) c = head_class((uint32_t)(off[v + 1] - off[v]));
+        const uint32_t v = (uint32_t)kv;
+        const uint32_t hc = head_class((uint32_t)(off[v + 1] - off[v]));
+        if (j == 0 || (keys[j - 1] >> 32) != kv || (j & (head_item(hc) - 1)) == 0) c = hc;
         if (kFill && (j + 1 == m || (keys[j + 1] >> 32) != kv)) end[v] = (uint32_t)(j + 1);
       }
     }
@@ -1253,10 +1267,7 @@ __global__ void __launch_bounds__(256) k_head_runs(const uint64_t* __restrict__ 
       if (c < kHeadClasses && lane == leader)
         pos = (uint32_t)atomicAdd(ctr + C_HEAD_CURSOR + c, (unsigned long long)__popc(peers));
       pos = __shfl_sync(kFull, pos, leader) + __popc(peers & lanemask_lt());
-      if (c < kHeadClasses) {
-        hl[kHeadPlanWords + hl[c] + pos] = v;
-        beg[v] = (uint32_t)j;
-      }
+      if (c < kHeadClasses) hl[kHeadPlanWords + hl[c] + pos] = (uint32_t)j;
     }
   }
   if (!kFill) {
@@ -1358,7 +1369,9 @@ __global__ void __launch_bounds__(256) k_head_warp(Csr g, HeadArcs h, const uint
     if (lane == 0) item = (uint32_t)atomicAdd(ctr + C_HEAD_QUEUE + 0, 1ull);
     item = __shfl_sync(kFull, item, 0);
     if (item >= cnt) break;
-    const uint32_t v = list[item];
+    uint32_t v, j1;
+    const uint32_t j00 = list[item];
+    h.item(j00, 0, v, j1);
     const uint64_t vb = g.off[v];
     const uint32_t d = (uint32_t)(g.off[v + 1] - vb);
     if (d > kWarpCap) {  // uniform over the warp
@@ -1370,8 +1383,7 @@ __global__ void __launch_bounds__(256) k_head_warp(Csr g, HeadArcs h, const uint
     TypeCounts vc;
     TypeCounts& out = kVC ? vc : tc;
     PackedCounts pc;
-    const uint32_t j1 = h.end[v];
-    for (uint32_t j0 = h.beg[v]; j0 < j1; j0 += kWarpCap) {
+    for (uint32_t j0 = j00; j0 < j1; j0 += kWarpCap) {
       const uint32_t tn = min(kWarpCap, j1 - j0);
       stage_in_arcs<32>(g, h, j0, tn, lane, m, WarpSync{});
       if (kTime) {
@@ -1417,7 +1429,9 @@ __global__ void __launch_bounds__(THREADS) k_head_block(Csr g, HeadArcs h,
     __syncthreads();
     const uint32_t item = s_item;
     if (item >= cnt) break;
-    const uint32_t v = list[item];
+    uint32_t v, j1;
+    const uint32_t j00 = list[item];
+    h.item(j00, hclass, v, j1);
     const uint64_t vb = g.off[v];
     const uint32_t d = (uint32_t)(g.off[v + 1] - vb);
     if (d > cap) {  // uniform over the CTA
@@ -1429,8 +1443,7 @@ __global__ void __launch_bounds__(THREADS) k_head_block(Csr g, HeadArcs h,
     TypeCounts vc;
     TypeCounts& out = kVC ? vc : tc;
     PackedCounts pc;
-    const uint32_t j1 = h.end[v];
-    for (uint32_t j0 = h.beg[v]; j0 < j1; j0 += cap) {
+    for (uint32_t j0 = j00; j0 < j1; j0 += cap) {
       const uint32_t tn = min(cap, j1 - j0);
       // Every warp left the previous tile's stream (barrier at its end), and
       // the staging below passes a barrier before the counter is used.
@@ -1455,8 +1468,8 @@ struct HeadBufs {
   uint64_t* keys = nullptr;
   uint64_t* alt = nullptr;
   uint32_t* aend = nullptr;
-  uint32_t* runs = nullptr;  // beg[n], end[n]
-  uint32_t* hl = nullptr;    // plan words, class lists
+  uint32_t* runs = nullptr;  // end of each head's run (n)
+  uint32_t* hl = nullptr;    // plan words, class lists of work items
   uint8_t* need = nullptr;   // per tail: it keeps arcs for the tail side
   uint32_t* sort_counts = nullptr;
 };
@@ -1466,9 +1479,12 @@ HeadBufs head_buffers(stc_ctx* c, const DeviceGraph& g) {
   b.keys = buffer<uint64_t>(c, B_KEYS_A, g.m_fwd);
   b.alt = buffer<uint64_t>(c, B_KEYS_B, g.m_fwd);
   b.aend = buffer<uint32_t>(c, B_HEAD_END, g.m_fwd);
-  b.runs = buffer<uint32_t>(c, B_HEAD_RUNS, 2ull * g.n);
-  b.hl = buffer<uint32_t>(c, B_HEAD_LIST, (size_t)g.n + kHeadPlanWords + (g.n + 3) / 4);
-  b.need = reinterpret_cast<uint8_t*>(b.hl + g.n + kHeadPlanWords);
+  b.runs = buffer<uint32_t>(c, B_HEAD_RUNS, g.n);
+  // Items: at most one per run (head) plus one per multiple of the
+  // smallest item size.
+  const size_t items = (size_t)g.n + g.m_fwd / kHeadItemMin + 1;
+  b.hl = buffer<uint32_t>(c, B_HEAD_LIST, kHeadPlanWords + items + (g.n + 3) / 4);
+  b.need = reinterpret_cast<uint8_t*>(b.hl + kHeadPlanWords + items);
   b.sort_counts = buffer<uint32_t>(c, B_SORT_COUNTS, (size_t)kRadix * kMaxSortGrid);
   return b;
 }
@@ -1524,12 +1540,11 @@ void enqueue_head(cudaStream_t st, const Csr& csr, const uint32_t* asrc, uint64_
   int sort_launches = 0;
   const uint64_t* sorted =
       radix_sort(b.keys, b.alt, m, 32, 32 + (int)vbits, b.sort_counts, st, &sort_launches);
-  uint32_t* beg = b.runs;
-  uint32_t* end = b.runs + n;
-  k_head_runs<false><<<kSMs * 4, 256, 0, st>>>(sorted, m, vbits, csr.off, ctr, b.hl, beg, end);
+  uint32_t* end = b.runs;
+  k_head_runs<false><<<kSMs * 4, 256, 0, st>>>(sorted, m, vbits, csr.off, ctr, b.hl, end);
   k_head_plan<<<1, 32, 0, st>>>(ctr, b.hl);
-  k_head_runs<true><<<kSMs * 4, 256, 0, st>>>(sorted, m, vbits, csr.off, ctr, b.hl, beg, end);
-  const HeadArcs h{sorted, b.aend, beg, end, asrc};
+  k_head_runs<true><<<kSMs * 4, 256, 0, st>>>(sorted, m, vbits, csr.off, ctr, b.hl, end);
+  const HeadArcs h{sorted, b.aend, end, asrc};
   launches += 3 + sort_launches;
   with_unroll(kTime ? kStreamUnroll : tu.unroll[0], [&](auto U) {
     constexpr int kU = decltype(U)::value;

@@ -71,6 +71,7 @@ enum CounterSlot {
   C_HEAD_COUNT = 21,           // head-side pass: head vertices per class (3 slots),
   C_HEAD_CURSOR = 24,          // their list fill cursors (3 slots)
   C_HEAD_QUEUE = 27,           // and the classes' work queues (3 slots)
+  C_PROBE_BYTES = 30,          // probe-model bytes of the CSR
   C_SLOTS = 32
 };
 

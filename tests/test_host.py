@@ -49,7 +49,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_status_strings_and_abi_version():
     lib = _capi.lib()
-    assert lib.stc_abi_version() == 1
+    assert lib.stc_abi_version() == 2
     for s in range(0, 9):
         assert lib.stc_status_string(s)
     assert lib.stc_status_string(0) == b"ok"
