@@ -639,6 +639,8 @@ __device__ __forceinline__ void flush_counts(const TypeCounts& tc, unsigned long
 struct TotalSink {  // only the four global counters
   static constexpr bool kPerVertex = false;
   __device__ void put(uint32_t, const unsigned long long*) const {}
+  __device__ uint32_t key(uint32_t) const { return 0; }
+  __device__ void put_key(uint32_t, const unsigned long long*) const {}
 };
 struct VertexSink {  // per-source counts by original id: vcounts[4 * id + type]
   static constexpr bool kPerVertex = true;
@@ -647,6 +649,13 @@ struct VertexSink {  // per-source counts by original id: vcounts[4 * id + type]
   __device__ void put(uint32_t u, const unsigned long long* c) const {
 #pragma unroll
     for (int k = 0; k < 4; k++) vcounts[4ull * verts[u] + (3 - k)] = c[k];
+  }
+  // Keyed form (the head side adds up the items of one key): the vertex.
+  __device__ uint32_t key(uint32_t u) const { return u; }
+  __device__ void put_key(uint32_t u, const unsigned long long* c) const {
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      if (c[k]) atomicAdd(vcounts + 4ull * verts[u] + (3 - k), c[k]);
   }
 };
 struct GraphSink {  // per-graph counts of a batch: gcounts[4 * graph + type]
@@ -662,8 +671,10 @@ struct GraphSink {  // per-graph counts of a batch: gcounts[4 * graph + type]
     }
     return lo;
   }
-  __device__ void put(uint32_t u, const unsigned long long* c) const {
-    const uint32_t g = graph_of(u);
+  __device__ void put(uint32_t u, const unsigned long long* c) const { put_key(graph_of(u), c); }
+  // Keyed form (the head side adds up the items of one key): the graph.
+  __device__ uint32_t key(uint32_t u) const { return graph_of(u); }
+  __device__ void put_key(uint32_t g, const unsigned long long* c) const {
 #pragma unroll
     for (int k = 0; k < 4; k++)
       if (c[k]) atomicAdd(gcounts + 4ull * g + (3 - k), c[k]);
@@ -686,6 +697,28 @@ __device__ __forceinline__ void block_vertex_flush(const TypeCounts& vc, uint32_
     for (int w = 0; w < THREADS / 32; w++)
       for (int k = 0; k < 4; k++) s[k] += red[w][k];
     sink.put(u, s);
+  }
+  __syncthreads();
+}
+
+// Reduces a key's counters over the CTA and hands them to the sink's keyed
+// form (every thread calls it, with the same key).
+template <int THREADS, class Sink>
+__device__ __forceinline__ void block_key_flush(const TypeCounts& vc, uint32_t key,
+                                                const Sink& sink) {
+  __shared__ unsigned long long red[THREADS / 32][4];
+  const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const unsigned long long v = warp_sum(vc.c[k]);
+    if (lane == 0) red[warp][k] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long s[4] = {0, 0, 0, 0};
+    for (int w = 0; w < THREADS / 32; w++)
+      for (int k = 0; k < 4; k++) s[k] += red[w][k];
+    sink.put_key(key, s);
   }
   __syncthreads();
 }
@@ -1364,6 +1397,19 @@ __global__ void __launch_bounds__(256) k_head_warp(Csr g, HeadArcs h, const uint
   const uint32_t* list = hl + kHeadPlanWords + hl[0];
   const uint32_t cnt = hl[kHeadPlanCount + 0];
   TypeCounts tc;
+  // Per-key counts (a sink that reports per graph): a warp's items come in
+  // increasing order of their heads, so the counts of one key are added up
+  // and handed to the sink once, when the key changes.
+  uint32_t cur = 0xFFFFFFFFu;
+  auto flush = [&]() {
+    if (kVC && cur != 0xFFFFFFFFu) {
+      unsigned long long s[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) s[k] = warp_sum(tc.c[k]);
+      if (lane == 0) sink.put_key(cur, s);
+      tc = TypeCounts{};
+    }
+  };
   while (true) {
     uint32_t item = 0;
     if (lane == 0) item = (uint32_t)atomicAdd(ctr + C_HEAD_QUEUE + 0, 1ull);
@@ -1378,10 +1424,16 @@ __global__ void __launch_bounds__(256) k_head_warp(Csr g, HeadArcs h, const uint
       if (lane == 0) atomicExch(ctr + C_ERROR, kErrStageCapacity);
       continue;
     }
+    if (kVC) {
+      const uint32_t key = sink.key(v);
+      if (key != cur) {
+        flush();
+        cur = key;
+      }
+    }
     const Geo geo = Geo::of(d, kWarpBuckets, hf);
     stage_hash<32>(g, vb, d, lane, m, geo, WarpSync{});
-    TypeCounts vc;
-    TypeCounts& out = kVC ? vc : tc;
+    TypeCounts& out = tc;
     PackedCounts pc;
     for (uint32_t j0 = j00; j0 < j1; j0 += kWarpCap) {
       const uint32_t tn = min(kWarpCap, j1 - j0);
@@ -1395,9 +1447,9 @@ __global__ void __launch_bounds__(256) k_head_warp(Csr g, HeadArcs h, const uint
       __syncwarp();
     }
     pc.drain(out);
-    if (kVC) warp_vertex_flush(vc, v, lane, sink);
     __syncwarp();
   }
+  flush();
   if (!kVC) flush_counts<256>(tc, ctr);
 }
 
@@ -1423,6 +1475,14 @@ __global__ void __launch_bounds__(THREADS) k_head_block(Csr g, HeadArcs h,
   unsigned long long* queue = ctr + C_HEAD_QUEUE + hclass;
   uint32_t* next = scan_tmp + kWarps + 1;  // the stream's claim counter
   TypeCounts tc;
+  // Per-key counts as in k_head_warp, reduced over the CTA at a key change.
+  uint32_t cur = 0xFFFFFFFFu;
+  auto flush = [&]() {
+    if (kVC && cur != 0xFFFFFFFFu) {
+      block_key_flush<THREADS>(tc, cur, sink);
+      tc = TypeCounts{};
+    }
+  };
   while (true) {
     __syncthreads();
     if (threadIdx.x == 0) s_item = (uint32_t)atomicAdd(queue, 1ull);
@@ -1438,10 +1498,16 @@ __global__ void __launch_bounds__(THREADS) k_head_block(Csr g, HeadArcs h,
       if (threadIdx.x == 0) atomicExch(ctr + C_ERROR, kErrStageCapacity);
       continue;
     }
+    if (kVC) {
+      const uint32_t key = sink.key(v);  // uniform over the CTA
+      if (key != cur) {
+        flush();
+        cur = key;
+      }
+    }
     const Geo geo = Geo::of(d, nb, hf);
     stage_hash<THREADS>(g, vb, d, threadIdx.x, m, geo, BlockSync{});
-    TypeCounts vc;
-    TypeCounts& out = kVC ? vc : tc;
+    TypeCounts& out = tc;
     PackedCounts pc;
     for (uint32_t j0 = j00; j0 < j1; j0 += cap) {
       const uint32_t tn = min(cap, j1 - j0);
@@ -1458,8 +1524,8 @@ __global__ void __launch_bounds__(THREADS) k_head_block(Csr g, HeadArcs h,
       __syncthreads();
     }
     pc.drain(out);
-    if (kVC) block_vertex_flush<THREADS>(vc, v, sink);
   }
+  flush();
   if (!kVC) flush_counts<THREADS>(tc, ctr);
 }
 
