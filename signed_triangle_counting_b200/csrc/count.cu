@@ -1177,11 +1177,11 @@ void launch_classes(cudaStream_t st, const Csr& csr, const uint32_t* lists, cons
 // MC/tc_hash_sign_enu.cpp:146-160).
 //
 // The head side finds each vertex's in-arcs by a sort: every HEAD arc i
-// (its index in the CSR) becomes the key v << 32 | i, every other arc the
-// sentinel, whose vertex field (all ones) is above every real head's (the
-// last vertex in rank order has no out-arcs, so no HEAD arc ends there); a
-// stable radix sort over the vertex bits groups each head's in-arcs, and
-// the runs of equal v are its in-arc ranges.  Head vertices are classed by
+// (its index in the CSR) is appended as the key v << 32 | i (a warp adds its
+// keys with one atomic, so their order varies from run to run; the counts
+// are sums and do not depend on it), a radix sort over the vertex bits of
+// the appended keys, their number known on the device only, groups each
+// head's in-arcs, and the runs of equal v are its in-arc ranges.  Head vertices are classed by
 // |N+(v)|, the list they stage: warp (<= 128), block (<= 1024) and large
 // (<= 4095).  A work item is a piece of one head's run that does not cross
 // a multiple of its class's item size (a hub with millions of in-arcs
@@ -1229,37 +1229,51 @@ struct HeadArcs {
   }
 };
 
-// Keys of the HEAD arcs (and sentinels), every arc's list end, and need[u]
-// = 1 for each tail u with an arc left to the tail side (the array starts at
-// 0; tails without such arcs are not staged there).  `range` (a sharded
-// count) keeps only tails in [range[0], range[1]).
+// Appends the keys of the HEAD arcs (count in ctr[C_HEAD_NKEYS]), records
+// the list end of each HEAD arc, and sets need[u] = 1 for each tail u with
+// an arc left to the tail side (the array starts at 0; tails without such
+// arcs are not staged there).  `range` (a sharded count) keeps only tails
+// in [range[0], range[1]).
 __global__ void __launch_bounds__(256) k_head_keys(Csr g, const uint32_t* __restrict__ asrc,
                                                    uint64_t m, const uint8_t* __restrict__ gtables,
-                                                   uint32_t vbits,
                                                    const unsigned long long* __restrict__ range,
                                                    uint64_t* __restrict__ keys,
                                                    uint32_t* __restrict__ aend,
-                                                   uint8_t* __restrict__ need) {
+                                                   uint8_t* __restrict__ need,
+                                                   unsigned long long* __restrict__ ctr) {
   __shared__ uint8_t tab[kTableBytes];
   for (uint32_t i = threadIdx.x; i < kTableBytes; i += blockDim.x) tab[i] = gtables[i];
   __syncthreads();
-  const uint64_t sentinel = ((1ull << vbits) - 1) << 32;
   const uint32_t r0 = range ? (uint32_t)range[0] : 0u;
   const uint32_t r1 = range ? (uint32_t)range[1] : 0xFFFFFFFFu;
+  const uint32_t lane = lane_id();
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
-    const uint32_t u = asrc[i], v = g.nbr[i];
-    const uint64_t ub = g.off[u], ue = g.off[u + 1];
-    const uint32_t alen = (uint32_t)(ue - i - 1);
-    const uint32_t blen = (uint32_t)(g.off[v + 1] - g.off[v]);
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < m;
+       base += stride) {
+    const uint64_t i = base + lane;
     bool head = false;
-    if (alen && blen && u >= r0 && u < r1) {
-      head = tab[256 * table_class((uint32_t)(ue - ub)) + 16 * size_bucket(alen) +
-                 size_bucket(blen)] == STC_STRATEGY_HEAD;
-      if (!head) need[u] = 1;  // u keeps an arc for the tail side
+    uint32_t v = 0, ue32 = 0;
+    if (i < m) {
+      const uint32_t u = asrc[i];
+      v = g.nbr[i];
+      const uint64_t ub = g.off[u], ue = g.off[u + 1];
+      ue32 = (uint32_t)ue;
+      const uint32_t alen = (uint32_t)(ue - i - 1);
+      const uint32_t blen = (uint32_t)(g.off[v + 1] - g.off[v]);
+      if (alen && blen && u >= r0 && u < r1) {
+        head = tab[256 * table_class((uint32_t)(ue - ub)) + 16 * size_bucket(alen) +
+                   size_bucket(blen)] == STC_STRATEGY_HEAD;
+        if (!head) need[u] = 1;  // u keeps an arc for the tail side
+      }
     }
-    keys[i] = head ? (((uint64_t)v << 32) | i) : sentinel;
-    aend[i] = (uint32_t)ue;
+    const unsigned hb = __ballot_sync(kFull, head);
+    uint32_t at = 0;
+    if (lane == 0 && hb) at = (uint32_t)atomicAdd(ctr + C_HEAD_NKEYS, (unsigned long long)__popc(hb));
+    at = __shfl_sync(kFull, at, 0);
+    if (head) {
+      keys[at + __popc(hb & lanemask_lt())] = ((uint64_t)v << 32) | i;
+      aend[i] = ue32;
+    }
   }
 }
 
@@ -1268,12 +1282,12 @@ __global__ void __launch_bounds__(256) k_head_keys(Csr g, const uint32_t* __rest
 // kFill: counts the items of each class.  With kFill: appends each item's
 // first entry to its class list and records the end of every run.
 template <bool kFill>
-__global__ void __launch_bounds__(256) k_head_runs(const uint64_t* __restrict__ keys, uint64_t m,
-                                                   uint32_t vbits, const uint64_t* __restrict__ off,
+__global__ void __launch_bounds__(256) k_head_runs(const uint64_t* __restrict__ keys,
+                                                   const uint64_t* __restrict__ off,
                                                    unsigned long long* __restrict__ ctr,
                                                    uint32_t* __restrict__ hl,
                                                    uint32_t* __restrict__ end) {
-  const uint64_t none = (1ull << vbits) - 1;
+  const uint64_t m = ctr[C_HEAD_NKEYS];
   const uint32_t lane = lane_id();
   uint32_t cnt[kHeadClasses] = {0, 0, 0};
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
@@ -1283,12 +1297,10 @@ __global__ void __launch_bounds__(256) k_head_runs(const uint64_t* __restrict__ 
     uint32_t c = kHeadClasses;  // not an item start
     if (j < m) {
       const uint64_t kv = keys[j] >> 32;
-      if (kv != none) {
-        const uint32_t v = (uint32_t)kv;
-        const uint32_t hc = head_class((uint32_t)(off[v + 1] - off[v]));
-        if (j == 0 || (keys[j - 1] >> 32) != kv || (j & (head_item(hc) - 1)) == 0) c = hc;
-        if (kFill && (j + 1 == m || (keys[j + 1] >> 32) != kv)) end[v] = (uint32_t)(j + 1);
-      }
+      const uint32_t v = (uint32_t)kv;
+      const uint32_t hc = head_class((uint32_t)(off[v + 1] - off[v]));
+      if (j == 0 || (keys[j - 1] >> 32) != kv || (j & (head_item(hc) - 1)) == 0) c = hc;
+      if (kFill && (j + 1 == m || (keys[j + 1] >> 32) != kv)) end[v] = (uint32_t)(j + 1);
     }
     if (!kFill) {
 #pragma unroll
@@ -1588,12 +1600,12 @@ inline void enqueue_head_keys(cudaStream_t st, const Csr& csr, const uint32_t* a
                               const HeadBufs& b, const uint8_t* d_tables,
                               const unsigned long long* range, unsigned long long* ctr,
                               int& launches) {
-  const uint32_t vbits = std::max<uint32_t>(1, bit_width64(csr.n - 1));
   STC_CUDA(cudaMemsetAsync(ctr + C_HEAD_COUNT, 0, 9 * sizeof(unsigned long long), st));
+  STC_CUDA(cudaMemsetAsync(ctr + C_HEAD_NKEYS, 0, sizeof(unsigned long long), st));
   STC_CUDA(cudaMemsetAsync(b.need, 0, csr.n, st));
   const uint32_t grid = (uint32_t)std::min<uint64_t>((m + 1023) / 1024, kSMs * 16);
-  k_head_keys<<<std::max(1u, grid), 256, 0, st>>>(csr, asrc, m, d_tables, vbits, range, b.keys,
-                                                  b.aend, b.need);
+  k_head_keys<<<std::max(1u, grid), 256, 0, st>>>(csr, asrc, m, d_tables, range, b.keys, b.aend,
+                                                  b.need, ctr);
   launches++;
 }
 
@@ -1604,12 +1616,12 @@ void enqueue_head(cudaStream_t st, const Csr& csr, const uint32_t* asrc, uint64_
   const uint32_t n = csr.n;
   const uint32_t vbits = std::max<uint32_t>(1, bit_width64(n - 1));
   int sort_launches = 0;
-  const uint64_t* sorted =
-      radix_sort(b.keys, b.alt, m, 32, 32 + (int)vbits, b.sort_counts, st, &sort_launches);
+  const uint64_t* sorted = radix_sort(b.keys, b.alt, m, 32, 32 + (int)vbits, b.sort_counts, st,
+                                      &sort_launches, ctr + C_HEAD_NKEYS);
   uint32_t* end = b.runs;
-  k_head_runs<false><<<kSMs * 4, 256, 0, st>>>(sorted, m, vbits, csr.off, ctr, b.hl, end);
+  k_head_runs<false><<<kSMs * 4, 256, 0, st>>>(sorted, csr.off, ctr, b.hl, end);
   k_head_plan<<<1, 32, 0, st>>>(ctr, b.hl);
-  k_head_runs<true><<<kSMs * 4, 256, 0, st>>>(sorted, m, vbits, csr.off, ctr, b.hl, end);
+  k_head_runs<true><<<kSMs * 4, 256, 0, st>>>(sorted, csr.off, ctr, b.hl, end);
   const HeadArcs h{sorted, b.aend, end, asrc};
   launches += 3 + sort_launches;
   with_unroll(kTime ? kStreamUnroll : tu.unroll[0], [&](auto U) {
@@ -1950,18 +1962,22 @@ void shard_range(stc_ctx* c, const DeviceGraph& g, uint32_t shard, uint32_t shar
 
 }  // namespace
 
-// Fixed degree-threshold dispatch, the same for every class: HEAD when A' is
-// not the longer list (bucket |A'| <= bucket |B|) and |B| <= 4095, SEARCH
+// Fixed degree-threshold dispatch: HEAD when A' is not the longer list
+// (bucket |A'| <= bucket |B|) and |B| <= 4095 (for lists of the warp class,
+// which also decides tiny lists, only when |B| >= 8: short arcs of short
+// lists cost less on the tail side than an entry in the head side's sort,
+// while a longer list would be staged there for a handful of them), SEARCH
 // when B is at least 16x longer than A', MERGE when both are short, HASH
 // otherwise (the giant class, which stages no hash, merges instead of
-// hashing).  Without `head`, the tail-side table of the first version
-// (no HEAD cells), which per-vertex counts and the no-allocation path use.
+// hashing).  Without `head`, the tail-side table of the first version (no
+// HEAD cells), which per-vertex counts and the no-allocation path use.
 void fixed_dispatch_tables(uint8_t* out, bool head) {
   for (int t = 0; t < kTableClasses; t++)
     for (int a = 0; a < 16; a++)
       for (int b = 0; b < 16; b++) {
         uint8_t s = STC_STRATEGY_HASH;
-        if (head && b >= 1 && b <= 12 && a <= b) s = STC_STRATEGY_HEAD;
+        const int bmin = t == kTableWarp ? 4 : 1;
+        if (head && b >= bmin && b <= 12 && a <= b) s = STC_STRATEGY_HEAD;
         else if (b >= a + 4) s = STC_STRATEGY_SEARCH;
         else if (a <= 3 && b <= 5) s = STC_STRATEGY_MERGE;
         out[256 * t + 16 * a + b] = s;

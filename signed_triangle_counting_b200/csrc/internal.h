@@ -72,6 +72,7 @@ enum CounterSlot {
   C_HEAD_CURSOR = 24,          // their list fill cursors (3 slots)
   C_HEAD_QUEUE = 27,           // and the classes' work queues (3 slots)
   C_PROBE_BYTES = 30,          // probe-model bytes of the CSR
+  C_HEAD_NKEYS = 31,           // head-side pass: keys (HEAD arcs) appended
   C_SLOTS = 32
 };
 

@@ -46,9 +46,11 @@ inline RangePartition range_partition(uint64_t m, uint64_t tile, uint32_t max_gr
 
 static __global__ void __launch_bounds__(kSortThreads) k_radix_upsweep(
     const uint64_t* __restrict__ keys, uint64_t m, uint64_t per_cta, int shift,
-    uint32_t dmask, uint32_t* __restrict__ counts, uint32_t grid) {
+    uint32_t dmask, uint32_t* __restrict__ counts, uint32_t grid,
+    const unsigned long long* __restrict__ m_dev) {
   __shared__ uint32_t hist[kSortWarps][kRadix + 1];
   const unsigned tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
+  if (m_dev && *m_dev < m) m = *m_dev;
   for (unsigned i = tid; i < kSortWarps * (kRadix + 1); i += kSortThreads) (&hist[0][0])[i] = 0;
   __syncthreads();
   const uint64_t begin = (uint64_t)blockIdx.x * per_cta;
@@ -93,13 +95,15 @@ static __global__ void __launch_bounds__(1024) k_scan_counts(uint32_t* __restric
 
 static __global__ void __launch_bounds__(kSortThreads, 2) k_radix_downsweep(
     const uint64_t* __restrict__ in, uint64_t* __restrict__ out, uint64_t m, uint64_t per_cta,
-    int shift, uint32_t dmask, const uint32_t* __restrict__ offsets, uint32_t grid) {
+    int shift, uint32_t dmask, const uint32_t* __restrict__ offsets, uint32_t grid,
+    const unsigned long long* __restrict__ m_dev) {
   __shared__ uint64_t sbuf[kSortTile];
   __shared__ uint16_t whist[kSortWarps][kRadix + 1];
   __shared__ uint32_t tile_start[kRadix];
   __shared__ uint32_t gofs[kRadix];
   __shared__ uint32_t scan_tmp[kSortWarps + 1];
   const unsigned tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
+  if (m_dev && *m_dev < m) m = *m_dev;
   const uint64_t begin = (uint64_t)blockIdx.x * per_cta;
   const uint64_t end = begin + per_cta < m ? begin + per_cta : m;
   for (unsigned d = tid; d < kRadix; d += kSortThreads) gofs[d] = offsets[(uint64_t)d * grid + blockIdx.x];
@@ -161,9 +165,12 @@ static __global__ void __launch_bounds__(kSortThreads, 2) k_radix_downsweep(
 
 // Scratch for radix_sort: `counts` holds kRadix * kMaxSortGrid words.
 // Sorts keys[0, m) by bits [lo, hi) stably; returns the buffer that holds the
-// result (`keys` or `alt`).  m must be below 2^32.
+// result (`keys` or `alt`).  m must be below 2^32.  With `m_dev`, the sort
+// covers only the first min(m, *m_dev) keys, a count known on the device
+// alone (the launches are sized for m, so the sequence can be captured).
 inline uint64_t* radix_sort(uint64_t* keys, uint64_t* alt, uint64_t m, int lo, int hi,
-                            uint32_t* counts, cudaStream_t st, int* launches = nullptr) {
+                            uint32_t* counts, cudaStream_t st, int* launches = nullptr,
+                            const unsigned long long* m_dev = nullptr) {
   if (m <= 1 || hi <= lo) return keys;
   RangePartition p = range_partition(m, kSortTile, kMaxSortGrid);
   uint64_t* src = keys;
@@ -171,10 +178,11 @@ inline uint64_t* radix_sort(uint64_t* keys, uint64_t* alt, uint64_t m, int lo, i
   for (int shift = lo; shift < hi; shift += 8) {
     const int w = hi - shift < 8 ? hi - shift : 8;
     const uint32_t dmask = (1u << w) - 1;
-    k_radix_upsweep<<<p.grid, kSortThreads, 0, st>>>(src, m, p.per_cta, shift, dmask, counts, p.grid);
+    k_radix_upsweep<<<p.grid, kSortThreads, 0, st>>>(src, m, p.per_cta, shift, dmask, counts, p.grid,
+                                                     m_dev);
     k_scan_counts<<<1, 1024, 0, st>>>(counts, kRadix * p.grid);
     k_radix_downsweep<<<p.grid, kSortThreads, 0, st>>>(src, dst, m, p.per_cta, shift, dmask, counts,
-                                                       p.grid);
+                                                       p.grid, m_dev);
     if (launches) *launches += 3;
     uint64_t* t = src;
     src = dst;

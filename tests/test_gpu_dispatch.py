@@ -63,15 +63,16 @@ def test_recorder_counts_and_cells(ctx, name):
 
 def fixed_rule():
     """The fixed table: HEAD where |A'| is not the longer list and |B| <= 4095
-    (bucket a <= b <= 12), SEARCH where B is 16x longer, MERGE where both
-    are short, HASH elsewhere."""
+    (bucket a <= b <= 12; in the warp class also b >= 4), SEARCH where B is
+    16x longer, MERGE where both are short, HASH elsewhere."""
     t = np.zeros((4, 16, 16), np.uint8)
-    for a in range(16):
-        for b in range(16):
-            if 1 <= b <= 12 and a <= b:
-                t[:, a, b] = 5
-            else:
-                t[:, a, b] = 3 if b >= a + 4 else (1 if a <= 3 and b <= 5 else 2)
+    for c in range(4):
+        for a in range(16):
+            for b in range(16):
+                if (4 if c == 0 else 1) <= b <= 12 and a <= b:
+                    t[c, a, b] = 5
+                else:
+                    t[c, a, b] = 3 if b >= a + 4 else (1 if a <= 3 and b <= 5 else 2)
     return t
 
 
