@@ -355,7 +355,8 @@ stc_status stc_dispatcher_train(stc_ctx* ctx, const float* features, const float
  * the strategy of least predicted cost where that is predicted at least 5%
  * cheaper than the fixed table's choice, and keeps the fixed choice
  * elsewhere (the giant class, which stages no hash, never gets HASH or
- * SPLIT; HEAD goes only to cells with |B| <= 4095).  `support` (optional, STC_DISPATCH_CELLS bytes) limits the
+ * SPLIT; HEAD only to cells where the fixed table holds it, since the
+ * recorder does not time the head side's sort and staging).  `support` (optional, STC_DISPATCH_CELLS bytes) limits the
  * overrides to the cells marked non-zero, normally the cells the model's
  * training data covered, so that the model is not trusted where it would
  * extrapolate; NULL allows them everywhere.  Calls with dispatch

@@ -1235,44 +1235,59 @@ struct HeadArcs {
 // arcs are not staged there).  `range` (a sharded count) keeps only tails
 // in [range[0], range[1]).
 __global__ void __launch_bounds__(256) k_head_keys(Csr g, const uint32_t* __restrict__ asrc,
-                                                   uint64_t m, const uint8_t* __restrict__ gtables,
+                                                   const uint32_t* __restrict__ fdeg, uint64_t m,
+                                                   const uint8_t* __restrict__ gtables,
                                                    const unsigned long long* __restrict__ range,
                                                    uint64_t* __restrict__ keys,
                                                    uint32_t* __restrict__ aend,
                                                    uint8_t* __restrict__ need,
                                                    unsigned long long* __restrict__ ctr) {
+  constexpr int kItems = 4;  // arcs per lane with their gathers in flight together
   __shared__ uint8_t tab[kTableBytes];
   for (uint32_t i = threadIdx.x; i < kTableBytes; i += blockDim.x) tab[i] = gtables[i];
   __syncthreads();
   const uint32_t r0 = range ? (uint32_t)range[0] : 0u;
   const uint32_t r1 = range ? (uint32_t)range[1] : 0xFFFFFFFFu;
   const uint32_t lane = lane_id();
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < m;
-       base += stride) {
-    const uint64_t i = base + lane;
-    bool head = false;
-    uint32_t v = 0, ue32 = 0;
-    if (i < m) {
-      const uint32_t u = asrc[i];
-      v = g.nbr[i];
-      const uint64_t ub = g.off[u], ue = g.off[u + 1];
-      ue32 = (uint32_t)ue;
-      const uint32_t alen = (uint32_t)(ue - i - 1);
-      const uint32_t blen = (uint32_t)(g.off[v + 1] - g.off[v]);
-      if (alen && blen && u >= r0 && u < r1) {
-        head = tab[256 * table_class((uint32_t)(ue - ub)) + 16 * size_bucket(alen) +
-                   size_bucket(blen)] == STC_STRATEGY_HEAD;
-        if (!head) need[u] = 1;  // u keeps an arc for the tail side
-      }
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x * kItems;
+  for (uint64_t base = ((uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u)) * kItems;
+       base < m; base += stride) {
+    uint32_t u[kItems], v[kItems], blen[kItems];
+    uint64_t ub[kItems], ue[kItems];
+#pragma unroll
+    for (int q = 0; q < kItems; q++) {
+      const uint64_t i = base + 32 * q + lane;
+      u[q] = i < m ? asrc[i] : 0u;
+      v[q] = i < m ? g.nbr[i] : 0u;
     }
-    const unsigned hb = __ballot_sync(kFull, head);
-    uint32_t at = 0;
-    if (lane == 0 && hb) at = (uint32_t)atomicAdd(ctr + C_HEAD_NKEYS, (unsigned long long)__popc(hb));
-    at = __shfl_sync(kFull, at, 0);
-    if (head) {
-      keys[at + __popc(hb & lanemask_lt())] = ((uint64_t)v << 32) | i;
-      aend[i] = ue32;
+#pragma unroll
+    for (int q = 0; q < kItems; q++) {
+      const uint64_t i = base + 32 * q + lane;
+      ub[q] = i < m ? g.off[u[q]] : 0;
+      ue[q] = i < m ? g.off[u[q] + 1] : 0;
+      blen[q] = i < m ? fdeg[v[q]] : 0u;
+    }
+#pragma unroll
+    for (int q = 0; q < kItems; q++) {
+      const uint64_t i = base + 32 * q + lane;
+      bool head = false;
+      if (i < m) {
+        const uint32_t alen = (uint32_t)(ue[q] - i - 1);
+        if (alen && blen[q] && u[q] >= r0 && u[q] < r1) {
+          head = tab[256 * table_class((uint32_t)(ue[q] - ub[q])) + 16 * size_bucket(alen) +
+                     size_bucket(blen[q])] == STC_STRATEGY_HEAD;
+          if (!head) need[u[q]] = 1;  // u keeps an arc for the tail side
+        }
+      }
+      const unsigned hb = __ballot_sync(kFull, head);
+      uint32_t at = 0;
+      if (lane == 0 && hb)
+        at = (uint32_t)atomicAdd(ctr + C_HEAD_NKEYS, (unsigned long long)__popc(hb));
+      at = __shfl_sync(kFull, at, 0);
+      if (head) {
+        keys[at + __popc(hb & lanemask_lt())] = ((uint64_t)v[q] << 32) | i;
+        aend[i] = (uint32_t)ue[q];
+      }
     }
   }
 }
@@ -1596,16 +1611,17 @@ void prepare_head(const Tuning& tu) {
 // tails left without arcs), then the sort, runs, plan and the three
 // head-class kernels.  The launch parameters of the block and large classes
 // follow the tuning of the tail side's same classes.
-inline void enqueue_head_keys(cudaStream_t st, const Csr& csr, const uint32_t* asrc, uint64_t m,
-                              const HeadBufs& b, const uint8_t* d_tables,
+inline void enqueue_head_keys(cudaStream_t st, const Csr& csr, const uint32_t* asrc,
+                              const uint32_t* fdeg, uint64_t m, const HeadBufs& b,
+                              const uint8_t* d_tables,
                               const unsigned long long* range, unsigned long long* ctr,
                               int& launches) {
   STC_CUDA(cudaMemsetAsync(ctr + C_HEAD_COUNT, 0, 9 * sizeof(unsigned long long), st));
   STC_CUDA(cudaMemsetAsync(ctr + C_HEAD_NKEYS, 0, sizeof(unsigned long long), st));
   STC_CUDA(cudaMemsetAsync(b.need, 0, csr.n, st));
-  const uint32_t grid = (uint32_t)std::min<uint64_t>((m + 1023) / 1024, kSMs * 16);
-  k_head_keys<<<std::max(1u, grid), 256, 0, st>>>(csr, asrc, m, d_tables, range, b.keys, b.aend,
-                                                  b.need, ctr);
+  const uint32_t grid = (uint32_t)std::min<uint64_t>((m + 1023) / 1024, kSMs * 8);
+  k_head_keys<<<std::max(1u, grid), 256, 0, st>>>(csr, asrc, fdeg, m, d_tables, range, b.keys,
+                                                  b.aend, b.need, ctr);
   launches++;
 }
 
@@ -1741,6 +1757,7 @@ __global__ void __launch_bounds__(256, 4) k_persistent(Csr g, const uint32_t* __
 struct HeadPlan {
   const HeadBufs* bufs = nullptr;  // null: the tables send no arc to the head side
   const uint32_t* asrc = nullptr;
+  const uint32_t* fdeg = nullptr;
   uint64_t m = 0;
   Tuning tuning;
 };
@@ -1753,7 +1770,8 @@ void enqueue_persistent(cudaStream_t st, const Csr& csr, const ClassBounds& cb, 
   const ArcTimes none{nullptr, nullptr};
   const uint8_t* need = nullptr;
   if (hp.bufs) {
-    enqueue_head_keys(st, csr, hp.asrc, hp.m, *hp.bufs, d_tables, nullptr, ctr, launches);
+    enqueue_head_keys(st, csr, hp.asrc, hp.fdeg, hp.m, *hp.bufs, d_tables, nullptr, ctr,
+                      launches);
     need = hp.bufs->need;
   }
   STC_CUDA(cudaMemsetAsync(ctr + C_WORK, 0, 8 * sizeof(uint64_t), st));
@@ -1779,7 +1797,7 @@ void enqueue_persistent(cudaStream_t st, const Csr& csr, const ClassBounds& cb, 
 // Identity of a captured persistent sequence: every pointer and size its
 // kernels were given.
 struct PersistentKey {
-  const void* p[15];
+  const void* p[16];
   uint64_t v[6];
 };
 
@@ -1802,8 +1820,8 @@ void count_persistent(stc_ctx* c, const Csr& csr, const ClassBounds& cb, uint32_
   }
   PersistentKey key{};
   const HeadBufs hb = hp.bufs ? *hp.bufs : HeadBufs{};
-  const void* ptrs[15] = {csr.off, csr.nbr, csr.sgn, csr.verts, lists, plan, ctr, d_tables, s0,
-                          hp.asrc, hb.keys, hb.alt, hb.aend, hb.runs, hb.hl};
+  const void* ptrs[16] = {csr.off, csr.nbr, csr.sgn, csr.verts, lists, plan, ctr, d_tables, s0,
+                          hp.asrc, hb.keys, hb.alt, hb.aend, hb.runs, hb.hl, hp.fdeg};
   memcpy(key.p, ptrs, sizeof(ptrs));
   key.v[0] = csr.n;
   key.v[1] = cb.tiny_max;
@@ -2084,6 +2102,7 @@ void count_triangles(stc_ctx* c, const DeviceGraph& gin, const CountConfig& cfg)
     if (head) {
       hp.bufs = &hb;
       hp.asrc = g.asrc;
+      hp.fdeg = g.fdeg;
       hp.m = g.m_fwd;
       hp.tuning = c->tuning;
     }
@@ -2102,7 +2121,7 @@ void count_triangles(stc_ctx* c, const DeviceGraph& gin, const CountConfig& cfg)
   }
   const uint8_t* need = nullptr;
   if (head) {
-    enqueue_head_keys(st, csr, g.asrc, g.m_fwd, hb, d_table, range, ctr, c->launches);
+    enqueue_head_keys(st, csr, g.asrc, g.fdeg, g.m_fwd, hb, d_table, range, ctr, c->launches);
     need = hb.need;
   }
   k_classify_count<<<kSMs * 4, 256, 0, st>>>(g.off, g.n, cb, ctr, range, need);

@@ -86,8 +86,11 @@ constexpr float kOverrideMargin = 0.0704f;
 // in the model's support and that strategy beats the fixed table's choice by
 // the margin, else the fixed choice.  The giant
 // class stages no hash, so it never takes HASH or SPLIT (its fixed HASH
-// cells run MERGE, and are compared as such); HEAD needs |B| <= 4095, so it
-// is open to cells with b <= 12 only.
+// cells run MERGE, and are compared as such).  HEAD is open only to the
+// cells where the fixed table already holds it: the recorder times a HEAD
+// arc's probes but not its share of the head side's sort and staging, so
+// its costs are too low for the model to add HEAD cells; it may move a HEAD
+// cell to a tail-side strategy.
 __global__ void k_mlp_tables(const float* __restrict__ params, const uint8_t* __restrict__ fixed,
                              const uint8_t* __restrict__ support, uint8_t* __restrict__ tables) {
   __shared__ float p[kMlpParams];
@@ -99,7 +102,7 @@ __global__ void k_mlp_tables(const float* __restrict__ params, const uint8_t* __
   cell_features(cell, f);
   mlp_forward(p, f, h, z);
   const bool giant = (cell >> 8) == kTableGiant;
-  const bool head_ok = (cell & 15) <= 12;
+  const bool head_ok = fixed[cell] == STC_STRATEGY_HEAD;
   auto staged_only = [](int o) { return o == STC_STRATEGY_HASH - 1 || o == STC_STRATEGY_SPLIT - 1; };
   int best = 0;
   for (int o = 1; o < kMlpOut; o++) {

@@ -93,7 +93,31 @@ static __global__ void __launch_bounds__(1024) k_scan_counts(uint32_t* __restric
   }
 }
 
-static __global__ void __launch_bounds__(kSortThreads, 2) k_radix_downsweep(
+// Ranks one tile's keys (stable): r[j] = the key's rank among the keys of
+// its digit in its warp's slice, whist[warp][digit] = the slice's count.
+// kFull: every key of the tile is valid, so digits fit 8 bits and the warp
+// match takes 8 ballots; a partial tile marks invalid keys with the digit
+// kRadix (9 bits).
+template <bool kFull>
+__device__ __forceinline__ void rank_tile(const uint64_t (&k)[kSortItems], uint64_t wbase,
+                                          uint64_t end, int shift, uint32_t dmask,
+                                          uint16_t (*whist)[kRadix + 1], unsigned warp,
+                                          unsigned lt, uint32_t (&r)[kSortItems]) {
+#pragma unroll
+  for (int j = 0; j < kSortItems; j++) {
+    const bool valid = kFull || wbase + (uint64_t)j * 32 < end;
+    const uint32_t dg = valid ? (uint32_t)(k[j] >> shift) & dmask : kRadix;
+    const unsigned peers = kFull ? match_label<8>(dg) : match_label<9>(dg);
+    const uint32_t base = whist[warp][dg];
+    const uint32_t below = __popc(peers & lt);
+    __syncwarp();
+    if (below == 0 && valid) whist[warp][dg] = (uint16_t)(base + __popc(peers));
+    __syncwarp();
+    r[j] = base + below;
+  }
+}
+
+static __global__ void __launch_bounds__(kSortThreads, 3) k_radix_downsweep(
     const uint64_t* __restrict__ in, uint64_t* __restrict__ out, uint64_t m, uint64_t per_cta,
     int shift, uint32_t dmask, const uint32_t* __restrict__ offsets, uint32_t grid,
     const unsigned long long* __restrict__ m_dev) {
@@ -106,59 +130,61 @@ static __global__ void __launch_bounds__(kSortThreads, 2) k_radix_downsweep(
   if (m_dev && *m_dev < m) m = *m_dev;
   const uint64_t begin = (uint64_t)blockIdx.x * per_cta;
   const uint64_t end = begin + per_cta < m ? begin + per_cta : m;
+  // gofs[d]: where digit d's next key goes in the output
   for (unsigned d = tid; d < kRadix; d += kSortThreads) gofs[d] = offsets[(uint64_t)d * grid + blockIdx.x];
   const unsigned lt = lanemask_lt();
   for (uint64_t tile = begin; tile < end; tile += kSortTile) {
     for (unsigned i = tid; i < kSortWarps * (kRadix + 1); i += kSortThreads) (&whist[0][0])[i] = 0;
     __syncthreads();
     uint64_t k[kSortItems];
-    uint32_t dg[kSortItems];
     uint32_t r[kSortItems];
     const uint64_t wbase = tile + (uint64_t)warp * (32 * kSortItems) + lane;
+    const bool full = end - tile >= (uint64_t)kSortTile;
 #pragma unroll
     for (int j = 0; j < kSortItems; j++) {
       const uint64_t idx = wbase + (uint64_t)j * 32;
-      k[j] = idx < end ? __ldcs(in + idx) : 0;
-      dg[j] = idx < end ? (uint32_t)(k[j] >> shift) & dmask : kRadix;
+      k[j] = (full || idx < end) ? __ldcs(in + idx) : 0;
     }
-#pragma unroll
-    for (int j = 0; j < kSortItems; j++) {
-      const unsigned peers = match_label<9>(dg[j]);
-      const uint32_t base = whist[warp][dg[j]];
-      const uint32_t below = __popc(peers & lt);
-      __syncwarp();
-      if (below == 0 && dg[j] != kRadix) whist[warp][dg[j]] = (uint16_t)(base + __popc(peers));
-      __syncwarp();
-      r[j] = base + below;
-    }
+    if (full)
+      rank_tile<true>(k, wbase, end, shift, dmask, whist, warp, lt, r);
+    else
+      rank_tile<false>(k, wbase, end, shift, dmask, whist, warp, lt, r);
     __syncthreads();
+    // Thread d: the tile's count of digit d, then every warp's slot for it
+    // as a tile position (digit start + the warps before).
+    const unsigned d = tid;  // kSortThreads == kRadix
     uint32_t cnt = 0;
+#pragma unroll
+    for (int w = 0; w < kSortWarps; w++) cnt += whist[w][d];
+    uint32_t total;
+    const uint32_t st = block_exclusive_scan<kSortThreads>(cnt, scan_tmp, total);
     {
-      const unsigned d = tid;  // kSortThreads == kRadix
+      uint32_t run = st;
 #pragma unroll
       for (int w = 0; w < kSortWarps; w++) {
         const uint32_t c = whist[w][d];
-        whist[w][d] = (uint16_t)cnt;
-        cnt += c;
+        whist[w][d] = (uint16_t)run;
+        run += c;
       }
     }
-    uint32_t total;
-    const uint32_t st = block_exclusive_scan<kSortThreads>(cnt, scan_tmp, total);
-    tile_start[tid] = st;
+    tile_start[d] = gofs[d] - st;  // output index of tile position p is tile_start[digit] + p
     __syncthreads();
 #pragma unroll
     for (int j = 0; j < kSortItems; j++) {
-      if (dg[j] != kRadix) sbuf[tile_start[dg[j]] + whist[warp][dg[j]] + r[j]] = k[j];
+      if (full || wbase + (uint64_t)j * 32 < end) {
+        const uint32_t dg = (uint32_t)(k[j] >> shift) & dmask;
+        sbuf[whist[warp][dg] + r[j]] = k[j];
+      }
     }
     __syncthreads();
     const uint32_t valid = (uint32_t)(end - tile < (uint64_t)kSortTile ? end - tile : kSortTile);
     for (uint32_t i = tid; i < valid; i += kSortThreads) {
       const uint64_t key = sbuf[i];
-      const uint32_t d = (uint32_t)(key >> shift) & dmask;
-      out[(uint64_t)gofs[d] + (i - tile_start[d])] = key;
+      const uint32_t dk = (uint32_t)(key >> shift) & dmask;
+      out[(uint32_t)(tile_start[dk] + i)] = key;  // indices are below m < 2^32
     }
     __syncthreads();
-    gofs[tid] += cnt;
+    gofs[d] += cnt;
     __syncthreads();
   }
 }
