@@ -229,13 +229,14 @@ __device__ __forceinline__ void arc_bytes(uint64_t i, uint32_t u, uint32_t v,
   probe += 5ull * (alen < dv ? alen : dv) + 30ull;
 }
 
-// Splits sorted arc keys into the neighbour, sign and tail arrays (the tail
-// array only when `asrc` is given) and accumulates the merge-model and
+// Splits sorted arc keys into the neighbour, sign, tail and signed-head
+// arrays (the last two only when given) and accumulates the merge-model and
 // probe-model bytes of every arc (arc_bytes).
 __global__ void k_csr_fill(const uint64_t* __restrict__ akeys, uint64_t ma, uint32_t bits,
                            const uint32_t* __restrict__ fdeg, const uint64_t* __restrict__ off,
                            uint32_t* __restrict__ nbr, int8_t* __restrict__ sgn,
-                           uint32_t* __restrict__ asrc, unsigned long long* __restrict__ ctr) {
+                           uint32_t* __restrict__ asrc, uint32_t* __restrict__ nkey,
+                           unsigned long long* __restrict__ ctr) {
   const uint64_t idmask = (1ull << bits) - 1;
   unsigned long long bytes = 0, probe = 0;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
@@ -245,6 +246,7 @@ __global__ void k_csr_fill(const uint64_t* __restrict__ akeys, uint64_t ma, uint
     nbr[i] = dst;
     sgn[i] = (k >> 63) ? (int8_t)-1 : (int8_t)1;
     if (asrc) asrc[i] = src;
+    if (nkey) nkey[i] = (dst << 1) | (uint32_t)(k >> 63);
     arc_bytes(i, src, dst, off, fdeg, bytes, probe);
   }
   bytes = warp_sum(bytes);
@@ -311,8 +313,10 @@ void finish_csr_from_arc_keys(stc_ctx* c, DeviceGraph& g, uint64_t* akeys, uint6
   g.nbr = buffer<uint32_t>(c, B_NBR, g.m_fwd + 4);  // + 4: the engine reads whole int4 chunks
   g.sgn = buffer<int8_t>(c, B_SGN, g.m_fwd + 4);
   g.asrc = buffer<uint32_t>(c, B_ASRC, g.m_fwd);
+  g.nkey = buffer<uint32_t>(c, B_NKEY, g.m_fwd + 4);
   k_csr_fill<<<grid_for(g.m_fwd, 4), kThreads, 0, c->stream>>>(sorted, g.m_fwd, g.bits, g.fdeg,
                                                                g.off, g.nbr, g.sgn, g.asrc,
+                                                               g.nkey,
                                                                (unsigned long long*)counters(c));
   c->launches += 1;
   STC_CUDA(cudaGetLastError());
@@ -552,20 +556,23 @@ __global__ void k_arc_keys_raw(EdgeIds e, const int8_t* __restrict__ sign, uint6
 }
 
 // The first key of each run of equal (lo, hi) in the sorted arc keys becomes
-// arc `pos` of the CSR: head, sign and tail.
+// arc `pos` of the CSR: head, sign, tail and signed head.
 struct EmitArc {
   const uint64_t* keys;
   uint32_t bits;
   uint32_t* nbr;
   int8_t* sgn;
   uint32_t* asrc;
+  uint32_t* nkey;
   __device__ void operator()(uint64_t i, uint64_t pos, uint32_t flag) const {
     if (!flag) return;
     const uint64_t k = keys[i];
     const uint64_t idmask = (1ull << bits) - 1;
-    nbr[pos] = (uint32_t)(k & idmask);
+    const uint32_t head = (uint32_t)(k & idmask);
+    nbr[pos] = head;
     sgn[pos] = (k >> 63) ? (int8_t)-1 : (int8_t)1;
     asrc[pos] = (uint32_t)((k >> bits) & idmask);
+    nkey[pos] = (head << 1) | (uint32_t)(k >> 63);
   }
 };
 
@@ -672,7 +679,8 @@ void build_totals(stc_ctx* c, const EdgeIds& e, const int8_t* d_sign, uint64_t m
     g.nbr = buffer<uint32_t>(c, B_NBR, g.m_fwd + 4);  // + 4: the engine reads whole int4 chunks
     g.sgn = buffer<int8_t>(c, B_SGN, g.m_fwd + 4);
     g.asrc = buffer<uint32_t>(c, B_ASRC, g.m_fwd);
-    range_apply(flag, EmitArc{sorted, g.bits, g.nbr, g.sgn, g.asrc}, g.m_valid, sums, st,
+    g.nkey = buffer<uint32_t>(c, B_NKEY, g.m_fwd + 4);
+    range_apply(flag, EmitArc{sorted, g.bits, g.nbr, g.sgn, g.asrc, g.nkey}, g.m_valid, sums, st,
                 &c->launches);
     k_fdeg_count<<<grid_for(g.m_fwd, 4), kThreads, 0, st>>>(g.asrc, g.m_fwd, g.fdeg);
     c->launches++;
@@ -966,7 +974,7 @@ void export_forward_csr(stc_ctx* c, const DeviceGraph& g, stc_forward_csr* out) 
   }
   if (mu) {
     k_csr_fill<<<grid_for(mu, 4), kThreads, 0, st>>>(sorted, mu, g.bits, fdeg_id, off_id, edges,
-                                                     signs, nullptr,
+                                                     signs, nullptr, nullptr,
                                                      (unsigned long long*)counters(c));
   }
   STC_CUDA(cudaGetLastError());

@@ -70,6 +70,9 @@ struct Csr {
   // vertex; null unless a count uses STC_STRATEGY_SPLIT.
   const uint32_t* __restrict__ nbr_split = nullptr;
   const uint32_t* __restrict__ psplit = nullptr;
+  // Heads with their signs, id << 1 | negative (same offsets, padded
+  // likewise): what the head side streams, one 16-byte load per chunk.
+  const uint32_t* __restrict__ nkey = nullptr;
 };
 
 // Per-thread type counters indexed by the number of negative edges.
@@ -430,6 +433,44 @@ __device__ __forceinline__ void process_chunk(const StageMem& m, uint32_t d, con
   }
 }
 
+// HASH for one int4 chunk of signed heads (id << 1 | negative, the head
+// side's stream): as process_chunk's HASH path, with each entry's sign taken
+// from its own low bit instead of a separate sign word.
+template <class PC>
+__device__ __forceinline__ void process_keyed_chunk(const StageMem& m, const Geo& geo,
+                                                    const uint4& q, uint32_t vm, uint32_t nuv,
+                                                    PC& pc) {
+  constexpr uint32_t kNoKey = kNoId << 1;
+  uint4 k4 = q;
+  if (vm != 0xFu) {
+    k4.x = (vm & 1u) ? k4.x : kNoKey;
+    k4.y = (vm & 2u) ? k4.y : kNoKey;
+    k4.z = (vm & 4u) ? k4.z : kNoKey;
+    k4.w = (vm & 8u) ? k4.w : kNoKey;
+  }
+  bool again = false;
+#pragma unroll
+  for (uint32_t e = 0; e < 4; e++) {
+    const uint32_t key = pick4(k4, e);
+    const uint32_t k2 = key & ~1u;  // 2 x
+    const uint2 w = *reinterpret_cast<const uint2*>(m.hk + 2 * hash_slot(key >> 1, geo.shift));
+    const uint32_t d0 = w.x - k2, d1 = w.y - k2;
+    const bool hit = d0 < 2 || d1 < 2;
+    again |= !hit && w.y != kEmpty;
+    pc.add_if(hit, nuv + (d0 < 2 ? d0 : d1 & 1u) + (key & 1u));
+  }
+  if (again) {
+#pragma unroll 1
+    for (uint32_t e = 0; e < 4; e++) {
+      const uint32_t key = pick4(k4, e), x = key >> 1;
+      const uint2 w = *reinterpret_cast<const uint2*>(m.hk + 2 * hash_slot(x, geo.shift));
+      if (w.x - (key & ~1u) < 2 || w.y - (key & ~1u) < 2 || w.y == kEmpty) continue;
+      const uint32_t r = probe_rest(m.hk, geo.nb, geo.shift, x);
+      if (r) pc.add(nuv + (r >> 1) + (key & 1u));
+    }
+  }
+}
+
 // The streamed arcs of a staged list as one sequence of aligned int4
 // chunks.  Warp w takes a contiguous 1/warps share of the sequence and its
 // lanes take consecutive chunks (coalesced); each lane keeps the extent of
@@ -445,7 +486,9 @@ __device__ __forceinline__ void process_chunk(const StageMem& m, uint32_t d, con
 // MERGE chunks are merged against the sorted A' instead.
 // kSplit: compiled with the SPLIT path (a split index per arc, a per-chunk
 // choice of source); kernels without it stay as lean as before SPLIT.
-template <int U, bool kSplit>
+// kKeyed (the head side, every arc HASH): chunks come from the signed heads
+// g.nkey, one 16-byte load each.
+template <int U, bool kSplit, bool kKeyed = false>
 __device__ __forceinline__ void stream_pass(const Csr& g, const StageMem& m, uint32_t d,
                                             uint32_t warp, uint32_t warps, uint32_t lane,
                                             const Geo& geo, TypeCounts& tc, uint32_t* next) {
@@ -501,7 +544,12 @@ __device__ __forceinline__ void stream_pass(const Csr& g, const StageMem& m, uin
               enter(k);
             }
             const uint32_t ci = cb + c;
-            load_chunk(g, ci, kSplit ? ast : (uint32_t)STC_STRATEGY_HASH, asp, q[u], sw[u]);
+            if (kKeyed) {
+              q[u] = reinterpret_cast<const uint4*>(g.nkey)[ci];
+              sw[u] = 0;
+            } else {
+              load_chunk(g, ci, kSplit ? ast : (uint32_t)STC_STRATEGY_HASH, asp, q[u], sw[u]);
+            }
             vm[u] = (c == pk ? mf : 0xFu) & (c + 1 == pk1 ? ml : 0xFu);
             sk[u] = k;
             snuv[u] = anuv;
@@ -510,7 +558,10 @@ __device__ __forceinline__ void stream_pass(const Csr& g, const StageMem& m, uin
         }
 #pragma unroll
         for (int u = 0; u < U; u++)
-          if (vm[u]) process_chunk(m, d, geo, q[u], sw[u], vm[u], sk[u], snuv[u], sst[u], p8);
+          if (vm[u]) {
+            if (kKeyed) process_keyed_chunk(m, geo, q[u], vm[u], snuv[u], p8);
+            else process_chunk(m, d, geo, q[u], sw[u], vm[u], sk[u], snuv[u], sst[u], p8);
+          }
         if (++rounds == kDrainRounds) {
           p8.drain(tc);
           rounds = 0;
@@ -1469,7 +1520,7 @@ __global__ void __launch_bounds__(256) k_head_warp(Csr g, HeadArcs h, const uint
         timed_head_pass(g, h, m, tn, d, 0, 1, lane, geo, pc, out, at);
       } else {
         warp_chunk_scan(m, tn, lane);
-        stream_pass<U, false>(g, m, tn, 0, 1, lane, geo, out, nullptr);
+        stream_pass<U, false, true>(g, m, tn, 0, 1, lane, geo, out, nullptr);
       }
       __syncwarp();
     }
@@ -1546,7 +1597,7 @@ __global__ void __launch_bounds__(THREADS) k_head_block(Csr g, HeadArcs h,
         timed_head_pass(g, h, m, tn, d, w, kWarps, lane, geo, pc, out, at);
       } else {
         block_chunk_scan<THREADS>(m, tn, scan_tmp);
-        stream_pass<U, false>(g, m, tn, w, kWarps, lane, geo, out, next);
+        stream_pass<U, false, true>(g, m, tn, w, kWarps, lane, geo, out, next);
       }
       __syncthreads();
     }
@@ -1797,7 +1848,7 @@ void enqueue_persistent(cudaStream_t st, const Csr& csr, const ClassBounds& cb, 
 // Identity of a captured persistent sequence: every pointer and size its
 // kernels were given.
 struct PersistentKey {
-  const void* p[16];
+  const void* p[17];
   uint64_t v[6];
 };
 
@@ -1820,8 +1871,8 @@ void count_persistent(stc_ctx* c, const Csr& csr, const ClassBounds& cb, uint32_
   }
   PersistentKey key{};
   const HeadBufs hb = hp.bufs ? *hp.bufs : HeadBufs{};
-  const void* ptrs[16] = {csr.off, csr.nbr, csr.sgn, csr.verts, lists, plan, ctr, d_tables, s0,
-                          hp.asrc, hb.keys, hb.alt, hb.aend, hb.runs, hb.hl, hp.fdeg};
+  const void* ptrs[17] = {csr.off, csr.nbr, csr.sgn, csr.verts, lists, plan, ctr, d_tables, s0,
+                          hp.asrc, hb.keys, hb.alt, hb.aend, hb.runs, hb.hl, hp.fdeg, csr.nkey};
   memcpy(key.p, ptrs, sizeof(ptrs));
   key.v[0] = csr.n;
   key.v[1] = cb.tiny_max;
@@ -2069,13 +2120,14 @@ void count_triangles(stc_ctx* c, const DeviceGraph& gin, const CountConfig& cfg)
                      (cfg.strategy == STC_STRATEGY_AUTO && cfg.dispatch == STC_DISPATCH_LEARNED &&
                       c->model_loaded && c->learned_uses_split);
   if (split) build_split(c, g);
-  Csr csr{g.off, g.nbr, g.sgn, g.verts, g.n, g.nbr_split, g.psplit};
+  Csr csr{g.off, g.nbr, g.sgn, g.verts, g.n, g.nbr_split, g.psplit, g.nkey};
   unsigned long long* ctr = (unsigned long long*)counters(c);
   bool uses_head = false;
   const uint8_t* d_table = dispatch_tables(c, cfg, &uses_head);
   // The head-side pass runs when the tables send arcs there (never for
   // per-vertex counts, whose tables have no HEAD cells).
-  const bool head = uses_head && (cfg.class_mask & 0x20u) && g.asrc != nullptr && g.n >= 2;
+  const bool head = uses_head && (cfg.class_mask & 0x20u) && g.asrc != nullptr &&
+                    g.nkey != nullptr && g.n >= 2;
   HeadBufs hb;
   if (head) hb = head_buffers(c, g);
   const bool timed = cfg.arc_cycles != nullptr;

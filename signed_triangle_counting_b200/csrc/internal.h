@@ -47,6 +47,7 @@ enum BufId {
   B_HEAD_END,                     // head-side pass: end of each arc's tail list (m)
   B_HEAD_RUNS,                    // head-side pass: in-arc range per head vertex (2 n)
   B_HEAD_LIST,                    // head-side pass: head vertices by class, plan, flags
+  B_NKEY,                         // arcs: head << 1 | negative (m + 4)
   B_COUNT_
 };
 
@@ -181,6 +182,7 @@ struct DeviceGraph {
   int8_t* sgn = nullptr;      // arcs: +1 / -1
   uint32_t* fdeg = nullptr;   // out-degree by rank
   uint32_t* asrc = nullptr;   // arcs: tail vertex (rank)
+  uint32_t* nkey = nullptr;   // arcs: head << 1 | negative, padded by 4 (the head side's stream)
   // Batches: G graphs whose vertices (ids and ranks) are contiguous; graph
   // g owns [gbase[g], gbase[g + 1]).  G == 0 for a single graph.
   uint32_t G = 0;
