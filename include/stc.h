@@ -145,7 +145,7 @@ typedef struct stc_stats {
   double ms_count;        /* intersection engine */
   double ms_total;        /* whole call on the device */
   uint32_t kernel_launches;
-  uint32_t reserved;
+  uint32_t groups_replayed; /* batch groups run as one replayed CUDA graph (persistent engine) */
   uint64_t probe_bytes;   /* probe-model bytes: sum over arcs of 5 min(|A'|, |B|) + 30, the
                              shorter list of each arc streamed once (A' = the part of N+(u)
                              after v, B = N+(v)), the arc's 25 bytes and its entry staged */

@@ -115,6 +115,7 @@ class Stats:
     ms_count: float
     ms_total: float
     kernel_launches: int
+    groups_replayed: int
     probe_bytes: int
 
 
@@ -527,7 +528,7 @@ class Context:
     def last_stats(self) -> Stats:
         s = _capi.stc_stats()
         _check(lib().stc_ctx_last_stats(self._h, C.byref(s)))
-        return Stats(**{f: getattr(s, f) for f, _ in _capi.stc_stats._fields_ if f != "reserved"})
+        return Stats(**{f: getattr(s, f) for f, _ in _capi.stc_stats._fields_})
 
     def synth_rmat_device(self, seed: int, scale: int, n: int, samples: int, a: float, b: float,
                           c: float, p_pos: float, src, dst, sign) -> None:

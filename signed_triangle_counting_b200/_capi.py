@@ -47,7 +47,7 @@ class stc_stats(C.Structure):
                 ("m_forward", C.c_uint64), ("alg_bytes", C.c_uint64), ("triangles", C.c_uint64),
                 ("ms_h2d", C.c_double), ("ms_dedup", C.c_double), ("ms_orient", C.c_double),
                 ("ms_csr", C.c_double), ("ms_count", C.c_double), ("ms_total", C.c_double),
-                ("kernel_launches", C.c_uint32), ("reserved", C.c_uint32),
+                ("kernel_launches", C.c_uint32), ("groups_replayed", C.c_uint32),
                 ("probe_bytes", C.c_uint64)]
 
 

@@ -468,7 +468,7 @@ __device__ __forceinline__ bool sampled_edge(uint32_t a, uint32_t b, uint32_t sh
 }
 
 __global__ void __launch_bounds__(kThreads) k_degree_raw(EdgeIds e, uint64_t m, uint64_t per_cta,
-                                                         uint32_t shift,
+                                                         uint32_t shift, uint32_t n,
                                                          uint32_t* __restrict__ deg) {
   __shared__ uint32_t tkey[kRawSlots], tcnt[kRawSlots], used[kRawSlots];
   __shared__ uint32_t nused;
@@ -490,7 +490,9 @@ __global__ void __launch_bounds__(kThreads) k_degree_raw(EdgeIds e, uint64_t m, 
       uint32_t a = kFree, b = kFree;
       if (i < end) {
         cur.at(e, i, a, b);
-        if (a == b || !sampled_edge(a, b, shift)) a = b = kFree;
+        // Ids at or past n only reach here when a capped build's union
+        // outgrew its capacity (flagged by k_batch_bases).
+        if (a == b || a >= n || b >= n || !sampled_edge(a, b, shift)) a = b = kFree;
       }
 #pragma unroll
       for (int side = 0; side < 2; side++) {
@@ -533,10 +535,13 @@ __global__ void __launch_bounds__(kThreads) k_degree_raw(EdgeIds e, uint64_t m, 
 
 // Arc keys of the input's edge copies in rank space: (rank lo << bits |
 // rank hi), the negative flag in bit 63; a self-loop becomes the all-ones
-// sentinel of the 2 * bits window, which sorts after every real key.
+// sentinel of the 2 * bits window, which sorts after every real key.  An
+// endpoint at or past n (a capped build whose union outgrew its capacity)
+// also becomes the sentinel and sets C_OVERFLOW.
 __global__ void k_arc_keys_raw(EdgeIds e, const int8_t* __restrict__ sign, uint64_t m,
-                               uint64_t per_cta, uint32_t bits, const uint32_t* __restrict__ rank,
-                               uint64_t* __restrict__ akeys) {
+                               uint64_t per_cta, uint32_t bits, uint32_t n,
+                               const uint32_t* __restrict__ rank, uint64_t* __restrict__ akeys,
+                               unsigned long long* __restrict__ ctr) {
   const uint64_t sentinel = (bits * 2 >= 64) ? ~0ull >> 1 : ((1ull << (2 * bits)) - 1);
   const uint64_t begin = (uint64_t)blockIdx.x * per_cta;
   const uint64_t end = begin + per_cta < m ? begin + per_cta : m;
@@ -547,7 +552,11 @@ __global__ void k_arc_keys_raw(EdgeIds e, const int8_t* __restrict__ sign, uint6
     uint32_t a, b;
     cur.at(e, i, a, b);
     uint64_t k = sentinel;
-    if (a != b) {
+    if (a == b) {
+      // self-loop: the sentinel
+    } else if (a >= n || b >= n) {
+      atomicExch(ctr + C_OVERFLOW, 1ull);
+    } else {
       const uint32_t ra = rank[a], rb = rank[b];
       k = ((uint64_t)min(ra, rb) << bits) | max(ra, rb) | ((uint64_t)(sign[i] < 0) << 63);
     }
@@ -577,9 +586,12 @@ struct EmitArc {
 };
 
 // Out-degree of every tail from the sorted arcs: lanes take consecutive
-// arcs, so a warp adds each run of equal tails with one atomic.
+// arcs, so a warp adds each run of equal tails with one atomic.  With m_dev,
+// m is a capacity and *m_dev the arc count.
 __global__ void k_fdeg_count(const uint32_t* __restrict__ asrc, uint64_t m,
+                             const unsigned long long* __restrict__ m_dev,
                              uint32_t* __restrict__ fdeg) {
+  if (m_dev) m = min(m, (uint64_t)*m_dev);
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < m;
        base += stride) {
@@ -590,10 +602,13 @@ __global__ void k_fdeg_count(const uint32_t* __restrict__ asrc, uint64_t m,
   }
 }
 
-// The merge-model and probe-model bytes of every arc (arc_bytes).
+// The merge-model and probe-model bytes of every arc (arc_bytes); m_dev as
+// in k_fdeg_count.
 __global__ void k_alg_bytes(const uint32_t* __restrict__ asrc, const uint32_t* __restrict__ nbr,
-                            uint64_t m, const uint64_t* __restrict__ off,
-                            const uint32_t* __restrict__ fdeg, unsigned long long* __restrict__ ctr) {
+                            uint64_t m, const unsigned long long* __restrict__ m_dev,
+                            const uint64_t* __restrict__ off, const uint32_t* __restrict__ fdeg,
+                            unsigned long long* __restrict__ ctr) {
+  if (m_dev) m = min(m, (uint64_t)*m_dev);
   unsigned long long bytes = 0, probe = 0;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride)
@@ -606,13 +621,109 @@ __global__ void k_alg_bytes(const uint32_t* __restrict__ asrc, const uint32_t* _
   }
 }
 
+// Vertex bases of a capped batch build, on the device: vbase = exclusive
+// prefix of the graphs' id spaces, vbase[G] = vertices of the union (also
+// written to C_BATCH_N); a union larger than the capacity n sets C_OVERFLOW.
+// One CTA of 1,024 threads, 1,024 graphs per step.
+__global__ void __launch_bounds__(1024) k_batch_bases(const unsigned int* __restrict__ space,
+                                                      uint32_t G, uint32_t n,
+                                                      uint64_t* __restrict__ vbase,
+                                                      unsigned long long* __restrict__ ctr) {
+  __shared__ uint64_t warp_incl[32];
+  __shared__ uint64_t carry;
+  const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (uint32_t b0 = 0; b0 < G; b0 += 1024) {
+    const uint32_t i = b0 + threadIdx.x;
+    const uint64_t x = i < G ? space[i] : 0;
+    uint64_t v = x;  // inclusive scan within the warp
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint64_t y = __shfl_up_sync(kFull, v, d);
+      if (lane >= (uint32_t)d) v += y;
+    }
+    if (lane == 31) warp_incl[w] = v;
+    __syncthreads();
+    if (w == 0) {
+      uint64_t t = warp_incl[lane];
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const uint64_t y = __shfl_up_sync(kFull, t, d);
+        if (lane >= (uint32_t)d) t += y;
+      }
+      warp_incl[lane] = t;
+    }
+    __syncthreads();
+    const uint64_t before = carry + (w ? warp_incl[w - 1] : 0) + v - x;
+    if (i < G) vbase[i] = before;
+    __syncthreads();
+    if (threadIdx.x == 1023) carry = before + x;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    vbase[G] = carry;
+    ctr[C_BATCH_N] = carry;
+    if (carry > n) ctr[C_OVERFLOW] = 1;
+  }
+}
+
+// Vertex sort keys of a capped batch build: graph << (32 + dbits) | degree
+// << 32 | id, the keys k_vertex_keys and k_batch_vertex_graph make together;
+// vertices past the union (vbase[G] <= i < n) take all-ones graph and
+// degree bits and so rank last.  A degree wider than dbits sets C_OVERFLOW.
+__global__ void k_batch_vertex_keys(const uint32_t* __restrict__ deg, uint32_t n,
+                                    const uint64_t* __restrict__ vbase, uint32_t G,
+                                    uint64_t per_cta, uint32_t dbits, uint32_t gbits,
+                                    uint64_t* __restrict__ vkeys,
+                                    unsigned long long* __restrict__ ctr) {
+  const uint64_t begin = (uint64_t)blockIdx.x * per_cta;
+  const uint64_t end = begin + per_cta < n ? begin + per_cta : n;
+  if (begin >= end) return;
+  const uint64_t nreal = vbase[G];
+  const uint64_t pad = ((1ull << (dbits + gbits)) - 1) << 32;
+  uint32_t g = begin < nreal ? first_segment(vbase, G, begin) : 0;
+  bool over = false;
+  for (uint64_t i = begin + threadIdx.x; i < end; i += blockDim.x) {
+    if (i >= nreal) {
+      vkeys[i] = pad | i;
+      continue;
+    }
+    while (vbase[g + 1] <= i) g++;
+    uint64_t d = deg[i];
+    if (d >> dbits) {
+      over = true;
+      d = (1ull << dbits) - 1;
+    }
+    vkeys[i] = (gbits ? (uint64_t)g << (32 + dbits) : 0ull) | (d << 32) | i;
+  }
+  if (over) atomicExch(ctr + C_OVERFLOW, 1ull);
+}
+
+// UniqueFlag over all m sorted arc keys, the self-loop sentinels (sorted
+// last, all ones in the 2 * bits window) excluded: a capped build does not
+// know m_valid on the host.
+struct UniqueArcFlag {
+  const uint64_t* keys;
+  uint64_t mask;
+  __device__ uint32_t operator()(uint64_t i) const {
+    const uint64_t k = keys[i] & mask;
+    if (k == mask) return 0u;
+    if (i == 0) return 1u;
+    return k != (keys[i - 1] & mask) ? 1u : 0u;
+  }
+};
+
 // Steps 2-6 of the totals path, after the ids (g.n, g.bits, g.m_valid set):
 // degrees over the edge copies (sampled on dense graphs), (degree, id) rank
-// (graph-major for a batch
-// with vertex bases d_vbase), arc keys of every copy, their sort, the first
-// of each run of equal arcs, offsets.  g.ukeys stays null.
+// (graph-major for a batch with vertex bases d_vbase), arc keys of every
+// copy, their sort, the first of each run of equal arcs, offsets.  g.ukeys
+// stays null.  With `caps` (a batch whose sizes stay on the device) nothing
+// is read back: g.n is the vertex capacity, the degree bits and sample shift
+// come from caps, and g.m_fwd is the arc capacity (m) with the arc count in
+// C_BATCH_MU (g.m_dev).
 void build_totals(stc_ctx* c, const EdgeIds& e, const int8_t* d_sign, uint64_t m, DeviceGraph& g,
-                  const uint64_t* d_vbase, uint32_t G) {
+                  const uint64_t* d_vbase, uint32_t G, const BatchCaps* caps = nullptr) {
   cudaStream_t st = c->stream;
   unsigned long long* ctr = (unsigned long long*)counters(c);
   uint32_t* sort_counts = buffer<uint32_t>(c, B_SORT_COUNTS, (size_t)kRadix * kMaxSortGrid);
@@ -632,8 +743,8 @@ void build_totals(stc_ctx* c, const EdgeIds& e, const int8_t* d_sign, uint64_t m
     // >= 16): shift = bit width of m / n, less 3, at most 3.
     const uint64_t ratio = g.m_valid / std::max<uint64_t>(1, g.n);
     const uint32_t bw = bit_width64(ratio);
-    const uint32_t shift = bw > 3 ? std::min<uint32_t>(3, bw - 3) : 0;
-    k_degree_raw<<<ep.grid, kThreads, 0, st>>>(e, m, ep.per_cta, shift, g.deg);
+    g.shift = caps ? caps->shift : bw > 3 ? std::min<uint32_t>(3, bw - 3) : 0;
+    k_degree_raw<<<ep.grid, kThreads, 0, st>>>(e, m, ep.per_cta, g.shift, g.n, g.deg);
     c->launches++;
   }
   STC_CUDA(cudaGetLastError());
@@ -642,20 +753,32 @@ void build_totals(stc_ctx* c, const EdgeIds& e, const int8_t* d_sign, uint64_t m
   if (g.n) {
     uint64_t* va = buffer<uint64_t>(c, B_VKEYS_A, g.n);
     uint64_t* vb = buffer<uint64_t>(c, B_VKEYS_B, g.n);
-    k_vertex_keys<<<grid_for(g.n, 4), kThreads, 0, st>>>(g.deg, g.n, va, ctr);
-    c->launches++;
-    read_counters(c, C_MAX_DEG, 1);
-    g.max_deg = (uint32_t)c->h_pinned[C_MAX_DEG];
-    const int dbits = (int)bit_width64(g.max_deg);
     const int gbits = d_vbase ? (int)bit_width64(G > 1 ? G - 1 : 0) : 0;
-    if (32 + dbits + gbits > 64) fail(STC_ERR_LIMIT, "batch too large for the vertex sort key");
-    if (gbits) {
+    if (caps) {
+      g.dbits = caps->dbits;
+      if (32 + (int)g.dbits + gbits > 64)
+        fail(STC_ERR_LIMIT, "batch too large for the vertex sort key");
       const RangePartition vp = range_partition(g.n, kSortTile, kMaxSortGrid);
-      k_batch_vertex_graph<<<vp.grid, kThreads, 0, st>>>(va, g.n, d_vbase, G, vp.per_cta,
-                                                         32 + dbits);
+      k_batch_vertex_keys<<<vp.grid, kThreads, 0, st>>>(g.deg, g.n, d_vbase, G, vp.per_cta,
+                                                        g.dbits, (uint32_t)gbits, va, ctr);
       c->launches++;
+    } else {
+      k_vertex_keys<<<grid_for(g.n, 4), kThreads, 0, st>>>(g.deg, g.n, va, ctr);
+      c->launches++;
+      read_counters(c, C_MAX_DEG, 1);
+      g.max_deg = (uint32_t)c->h_pinned[C_MAX_DEG];
+      g.dbits = bit_width64(g.max_deg);
+      if (32 + (int)g.dbits + gbits > 64)
+        fail(STC_ERR_LIMIT, "batch too large for the vertex sort key");
+      if (gbits) {
+        const RangePartition vp = range_partition(g.n, kSortTile, kMaxSortGrid);
+        k_batch_vertex_graph<<<vp.grid, kThreads, 0, st>>>(va, g.n, d_vbase, G, vp.per_cta,
+                                                           32 + g.dbits);
+        c->launches++;
+      }
     }
-    uint64_t* vs = radix_sort(va, vb, g.n, 32, 32 + dbits + gbits, sort_counts, st, &c->launches);
+    uint64_t* vs = radix_sort(va, vb, g.n, 32, 32 + (int)g.dbits + gbits, sort_counts, st,
+                              &c->launches);
     k_rank<<<grid_for(g.n, 4), kThreads, 0, st>>>(vs, g.n, g.verts, g.rank);
     c->launches++;
   }
@@ -666,23 +789,40 @@ void build_totals(stc_ctx* c, const EdgeIds& e, const int8_t* d_sign, uint64_t m
   if (g.m_valid) {
     uint64_t* ka = buffer<uint64_t>(c, B_KEYS_A, m);
     uint64_t* kb = buffer<uint64_t>(c, B_KEYS_B, m);
-    k_arc_keys_raw<<<ep.grid, kThreads, 0, st>>>(e, d_sign, m, ep.per_cta, g.bits, g.rank, ka);
+    k_arc_keys_raw<<<ep.grid, kThreads, 0, st>>>(e, d_sign, m, ep.per_cta, g.bits, g.n, g.rank,
+                                                 ka, ctr);
     c->launches++;
     uint64_t* sorted = radix_sort(ka, kb, m, 0, 2 * (int)g.bits, sort_counts, st, &c->launches);
-    // Self-loops sorted last: the first m_valid keys are the real arcs.
-    const UniqueFlag flag{sorted, (1ull << (2 * g.bits)) - 1};
-    const uint32_t grid = range_reduce_scan(flag, g.m_valid, sums, st, &c->launches);
-    STC_CUDA(cudaMemcpyAsync(c->h_pinned + C_WORK, sums + grid, sizeof(uint64_t),
-                             cudaMemcpyDeviceToHost, st));
-    STC_CUDA(cudaStreamSynchronize(st));
-    g.m_unique = g.m_fwd = c->h_pinned[C_WORK];
-    g.nbr = buffer<uint32_t>(c, B_NBR, g.m_fwd + 4);  // + 4: the engine reads whole int4 chunks
-    g.sgn = buffer<int8_t>(c, B_SGN, g.m_fwd + 4);
-    g.asrc = buffer<uint32_t>(c, B_ASRC, g.m_fwd);
-    g.nkey = buffer<uint32_t>(c, B_NKEY, g.m_fwd + 4);
-    range_apply(flag, EmitArc{sorted, g.bits, g.nbr, g.sgn, g.asrc, g.nkey}, g.m_valid, sums, st,
-                &c->launches);
-    k_fdeg_count<<<grid_for(g.m_fwd, 4), kThreads, 0, st>>>(g.asrc, g.m_fwd, g.fdeg);
+    const uint64_t mask = (1ull << (2 * g.bits)) - 1;
+    if (caps) {
+      const UniqueArcFlag flag{sorted, mask};
+      const uint32_t grid = range_reduce_scan(flag, m, sums, st, &c->launches);
+      STC_CUDA(cudaMemcpyAsync(ctr + C_BATCH_MU, sums + grid, sizeof(uint64_t),
+                               cudaMemcpyDeviceToDevice, st));
+      g.m_unique = g.m_fwd = m;
+      g.m_dev = ctr + C_BATCH_MU;
+      g.nbr = buffer<uint32_t>(c, B_NBR, m + 4);
+      g.sgn = buffer<int8_t>(c, B_SGN, m + 4);
+      g.asrc = buffer<uint32_t>(c, B_ASRC, m);
+      g.nkey = buffer<uint32_t>(c, B_NKEY, m + 4);
+      range_apply(flag, EmitArc{sorted, g.bits, g.nbr, g.sgn, g.asrc, g.nkey}, m, sums, st,
+                  &c->launches);
+    } else {
+      // Self-loops sorted last: the first m_valid keys are the real arcs.
+      const UniqueFlag flag{sorted, mask};
+      const uint32_t grid = range_reduce_scan(flag, g.m_valid, sums, st, &c->launches);
+      STC_CUDA(cudaMemcpyAsync(c->h_pinned + C_WORK, sums + grid, sizeof(uint64_t),
+                               cudaMemcpyDeviceToHost, st));
+      STC_CUDA(cudaStreamSynchronize(st));
+      g.m_unique = g.m_fwd = c->h_pinned[C_WORK];
+      g.nbr = buffer<uint32_t>(c, B_NBR, g.m_fwd + 4);  // + 4: the engine reads whole int4 chunks
+      g.sgn = buffer<int8_t>(c, B_SGN, g.m_fwd + 4);
+      g.asrc = buffer<uint32_t>(c, B_ASRC, g.m_fwd);
+      g.nkey = buffer<uint32_t>(c, B_NKEY, g.m_fwd + 4);
+      range_apply(flag, EmitArc{sorted, g.bits, g.nbr, g.sgn, g.asrc, g.nkey}, g.m_valid, sums,
+                  st, &c->launches);
+    }
+    k_fdeg_count<<<grid_for(g.m_fwd, 4), kThreads, 0, st>>>(g.asrc, g.m_fwd, g.m_dev, g.fdeg);
     c->launches++;
   }
   g.off = buffer<uint64_t>(c, B_OFF, (size_t)g.n + 1);
@@ -694,8 +834,8 @@ void build_totals(stc_ctx* c, const EdgeIds& e, const int8_t* d_sign, uint64_t m
     STC_CUDA(cudaMemsetAsync(g.off, 0, sizeof(uint64_t), st));
   }
   if (g.m_fwd) {
-    k_alg_bytes<<<grid_for(g.m_fwd, 4), kThreads, 0, st>>>(g.asrc, g.nbr, g.m_fwd, g.off, g.fdeg,
-                                                           ctr);
+    k_alg_bytes<<<grid_for(g.m_fwd, 4), kThreads, 0, st>>>(g.asrc, g.nbr, g.m_fwd, g.m_dev, g.off,
+                                                           g.fdeg, ctr);
     c->launches++;
   } else {
     g.nbr = buffer<uint32_t>(c, B_NBR, 4);
@@ -947,6 +1087,42 @@ void build_graph_batch(stc_ctx* c, const uint32_t* d_src, const uint32_t* d_dst,
     g.sgn = buffer<int8_t>(c, B_SGN, 4);
   }
   mark(c, 4);
+}
+
+void build_graph_batch_capped(stc_ctx* c, const uint32_t* d_src, const uint32_t* d_dst,
+                              const int8_t* d_sign, uint64_t m, uint32_t G, const BatchCaps& caps,
+                              DeviceGraph& g) {
+  cudaStream_t st = c->stream;
+  unsigned long long* ctr = (unsigned long long*)counters(c);
+  g = DeviceGraph{};
+  g.m_input = m;
+  g.G = G;
+  if (m >= (1ull << 32)) fail(STC_ERR_LIMIT, "batch has 2^32 or more edges");
+  if (caps.n == 0 || caps.n >= (1u << 31) - 1 || caps.bits != std::max<uint32_t>(1, bit_width64(caps.n - 1)))
+    fail(STC_ERR_INTERNAL, "inconsistent batch capacities");
+  if (!c->h_eoff || c->h_eoff_cap < (size_t)G + 1) fail(STC_ERR_INTERNAL, "edge offsets not staged");
+  uint64_t* d_eoff = buffer<uint64_t>(c, B_BATCH_META, 2ull * (G + 1));
+  uint64_t* d_vbase = d_eoff + (G + 1);
+  unsigned int* d_space = reinterpret_cast<unsigned int*>(buffer<uint32_t>(c, B_BATCH_SPACE, G));
+  STC_CUDA(cudaMemcpyAsync(d_eoff, c->h_eoff, (G + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice,
+                           st));
+  STC_CUDA(cudaMemsetAsync(d_space, 0, G * sizeof(uint32_t), st));
+
+  // 1. id space per graph -> vertex bases of the union, on the device.
+  mark(c, 1);
+  const RangePartition ep = range_partition(m, kSortTile, kMaxSortGrid);
+  if (m) {
+    k_batch_ids<<<ep.grid, kThreads, 0, st>>>(d_src, d_dst, m, d_eoff, G, ep.per_cta, d_space, ctr);
+    c->launches++;
+  }
+  k_batch_bases<<<1, 1024, 0, st>>>(d_space, G, caps.n, d_vbase, ctr);
+  c->launches++;
+  STC_CUDA(cudaGetLastError());
+  g.n = caps.n;
+  g.m_valid = m;
+  g.bits = caps.bits;
+  g.gbase = d_vbase;
+  build_totals(c, EdgeIds{d_src, d_dst, d_eoff, d_vbase, G}, d_sign, m, g, d_vbase, G, &caps);
 }
 
 void export_forward_csr(stc_ctx* c, const DeviceGraph& g, stc_forward_csr* out) {

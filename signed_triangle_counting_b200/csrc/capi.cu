@@ -29,7 +29,22 @@ void cuda_check(cudaError_t e, const char* what) {
 uint64_t* counters(stc_ctx* c) { return buffer<uint64_t>(c, B_COUNTERS, C_SLOTS); }
 
 void mark(stc_ctx* c, int slot) {
-  if (c->timing) STC_CUDA(cudaEventRecord(c->ev[slot], c->stream));
+  if (!c->timing) return;
+  // Inside a capture the event becomes a node of the graph that records it
+  // on every replay (an external record), so stage times stay readable.
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (c->stream != nullptr && c->stream != cudaStreamLegacy && c->stream != cudaStreamPerThread)
+    STC_CUDA(cudaStreamIsCapturing(c->stream, &cs));
+  if (cs == cudaStreamCaptureStatusActive)
+    STC_CUDA(cudaEventRecordWithFlags(c->ev[slot], c->stream, cudaEventRecordExternal));
+  else
+    STC_CUDA(cudaEventRecord(c->ev[slot], c->stream));
+}
+
+void release_pipelines(stc_ctx* c) {
+  for (auto& p : c->pipes)
+    if (p.exec) cudaGraphExecDestroy(p.exec);
+  c->pipes.clear();
 }
 
 namespace {
@@ -133,6 +148,209 @@ DeviceInput stage_input(stc_ctx* c, const uint32_t* src, const uint32_t* dst, co
 // needs to about 45 bytes per edge of a group.
 constexpr uint64_t kBatchGroupEdges = 1536ull << 20;
 
+// ------------------------------------------------- batch group pipeline ----
+// A group of a batch on the persistent engine runs as one captured CUDA
+// graph once it has been seen: counters, offsets upload, the whole totals
+// build and the count, with no host synchronisation between the stages.
+// The build then cannot read sizes back, so it runs at capacities (BatchCaps)
+// taken from an earlier, uncapped build of a group with the same key (input
+// pointers, sizes and count configuration), and the device checks that the
+// new data fits them.  A group that does not fit (C_OVERFLOW) is counted
+// again uncapped and its sizes become the new capacities.  Sequence for one
+// key: uncapped (learns capacities) -> capped, uncaptured (sizes every
+// buffer, so that the capture allocates nothing) -> captured and replayed
+// on every later call while no device buffer has moved (c->buf_gen).
+constexpr size_t kMaxPipelines = 4;
+
+// Capacities from an uncapped build: vertices with 1/16 headroom, as far as
+// the id bits allow.
+bool caps_from(const DeviceGraph& g, BatchCaps& caps) {
+  if (g.n == 0 || g.m_fwd == 0) return false;
+  caps.bits = std::max<uint32_t>(1, bit_width64(g.n - 1));
+  const uint64_t room = std::min<uint64_t>(1ull << caps.bits, (1ull << 31) - 2);
+  caps.n = (uint32_t)std::max<uint64_t>(g.n, std::min<uint64_t>(g.n + g.n / 16 + 64, room));
+  caps.dbits = g.dbits;
+  caps.shift = g.shift;
+  return true;
+}
+
+void stage_offsets(stc_ctx* c, const std::vector<uint64_t>& eoff) {
+  if (c->h_eoff_cap < eoff.size()) {
+    STC_CUDA(cudaStreamSynchronize(c->stream));  // no earlier copy still reads it
+    if (c->h_eoff) STC_CUDA(cudaFreeHost(c->h_eoff));
+    c->h_eoff = nullptr;
+    c->h_eoff_cap = 0;
+    const size_t want = eoff.size() + eoff.size() / 8;
+    STC_CUDA(cudaMallocHost(&c->h_eoff, want * sizeof(uint64_t)));
+    c->h_eoff_cap = want;
+    c->buf_gen++;
+  }
+  memcpy(c->h_eoff, eoff.data(), eoff.size() * sizeof(uint64_t));
+}
+
+// Per-graph counts (4 per graph) into h and the counters into c->h_pinned.
+void finish_group(stc_ctx* c, uint32_t gn, std::vector<uint64_t>& h) {
+  const uint64_t* gc = buffer<uint64_t>(c, B_BATCH_COUNTS, 4ull * gn);
+  STC_CUDA(cudaMemcpyAsync(h.data(), gc, 4ull * gn * sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                           c->stream));
+  STC_CUDA(cudaMemcpyAsync(c->h_pinned, counters(c), C_SLOTS * sizeof(uint64_t),
+                           cudaMemcpyDeviceToHost, c->stream));
+  STC_CUDA(cudaStreamSynchronize(c->stream));
+}
+
+struct GroupOut {
+  uint64_t n = 0, m_unique = 0;
+  bool replayed = false;
+};
+
+GroupOut eager_group(stc_ctx* c, const DeviceInput& in, uint64_t me,
+                     const std::vector<uint64_t>& eoff, uint32_t gn, CountConfig cfg,
+                     std::vector<uint64_t>& h, DeviceGraph& g) {
+  STC_CUDA(cudaMemsetAsync(counters(c), 0, C_SLOTS * sizeof(uint64_t), c->stream));
+  build_graph_batch(c, in.src, in.dst, in.sign, me, eoff.data(), gn, g, /*totals=*/true);
+  uint64_t* gc = buffer<uint64_t>(c, B_BATCH_COUNTS, 4ull * gn);
+  STC_CUDA(cudaMemsetAsync(gc, 0, 4ull * gn * sizeof(uint64_t), c->stream));
+  cfg.graph_counts = gc;
+  count_triangles(c, g, cfg);
+  mark(c, 5);
+  finish_group(c, gn, h);
+  return GroupOut{g.n, g.m_unique, false};
+}
+
+// The capturable sequence of a group at capacities `caps`.
+void enqueue_capped_group(stc_ctx* c, const DeviceInput& in, uint64_t me, uint32_t gn,
+                          const BatchCaps& caps, CountConfig cfg) {
+  STC_CUDA(cudaMemsetAsync(counters(c), 0, C_SLOTS * sizeof(uint64_t), c->stream));
+  uint64_t* gc = buffer<uint64_t>(c, B_BATCH_COUNTS, 4ull * gn);
+  STC_CUDA(cudaMemsetAsync(gc, 0, 4ull * gn * sizeof(uint64_t), c->stream));
+  DeviceGraph g;
+  build_graph_batch_capped(c, in.src, in.dst, in.sign, me, gn, caps, g);
+  cfg.graph_counts = gc;
+  count_triangles(c, g, cfg);
+  mark(c, 5);
+}
+
+enum class Capture { kOk, kRetry, kFailed };
+
+Capture capture_group(stc_ctx* c, GroupPipeline& p, const DeviceInput& in, uint64_t me,
+                      uint32_t gn, const CountConfig& cfg) {
+  if (p.exec) {
+    STC_CUDA(cudaGraphExecDestroy(p.exec));
+    p.exec = nullptr;
+  }
+  const uint64_t gen0 = c->buf_gen;
+  const int l0 = c->launches;
+  cudaGraph_t graph = nullptr;
+  STC_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+  try {
+    enqueue_capped_group(c, in, me, gn, p.caps, cfg);
+  } catch (...) {
+    cudaStreamEndCapture(c->stream, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    (void)cudaGetLastError();
+    c->launches = l0;
+    return Capture::kFailed;
+  }
+  STC_CUDA(cudaStreamEndCapture(c->stream, &graph));
+  const int launches = c->launches - l0;
+  c->launches = l0;
+  if (c->buf_gen != gen0) {  // a buffer grew inside the capture: size it uncaptured first
+    cudaGraphDestroy(graph);
+    return Capture::kRetry;
+  }
+  const cudaError_t e = cudaGraphInstantiate(&p.exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    p.exec = nullptr;
+    return Capture::kFailed;
+  }
+  p.gen = c->buf_gen;
+  p.launches = launches;
+  p.state = 3;
+  return Capture::kOk;
+}
+
+// Counts one group of a batch (see the pipeline notes above); h receives
+// its per-graph counts and c->h_pinned the counters.
+GroupOut count_group(stc_ctx* c, const DeviceInput& in, uint64_t me,
+                     const std::vector<uint64_t>& eoff, uint32_t gn, const CountConfig& cfg,
+                     std::vector<uint64_t>& h) {
+  DeviceGraph g;
+  const bool stream_ok = c->stream != nullptr && c->stream != cudaStreamLegacy &&
+                         c->stream != cudaStreamPerThread;
+  const bool learned_split = cfg.strategy == STC_STRATEGY_AUTO &&
+                             cfg.dispatch == STC_DISPATCH_LEARNED && c->model_loaded &&
+                             c->learned_uses_split;
+  if (!cfg.persistent || me == 0 || !stream_ok || cfg.strategy == STC_STRATEGY_SPLIT ||
+      learned_split)
+    return eager_group(c, in, me, eoff, gn, cfg, h, g);
+
+  uint64_t key[16] = {};
+  key[0] = reinterpret_cast<uint64_t>(in.src);
+  key[1] = reinterpret_cast<uint64_t>(in.dst);
+  key[2] = reinterpret_cast<uint64_t>(in.sign);
+  key[3] = me;
+  key[4] = gn;
+  key[5] = (uint64_t)cfg.strategy | ((uint64_t)cfg.dispatch << 8) |
+           ((uint64_t)c->model_loaded << 16) | ((uint64_t)c->learned_uses_head << 17) |
+           ((uint64_t)c->timing << 18) | ((uint64_t)cfg.class_mask << 24);
+  key[6] = reinterpret_cast<uint64_t>(c->stream);
+  const Tuning& tu = c->tuning;
+  key[7] = (uint64_t)tu.block_threads | ((uint64_t)tu.hash_factor[0] << 16) |
+           ((uint64_t)tu.hash_factor[1] << 24) | ((uint64_t)tu.hash_factor[2] << 32) |
+           ((uint64_t)tu.unroll[0] << 40) | ((uint64_t)tu.unroll[1] << 48) |
+           ((uint64_t)tu.unroll[2] << 56);
+  GroupPipeline* p = nullptr;
+  for (auto& q : c->pipes)
+    if (memcmp(q.key, key, sizeof(key)) == 0) p = &q;
+  if (!p) {
+    const GroupOut o = eager_group(c, in, me, eoff, gn, cfg, h, g);
+    if (c->pipes.size() >= kMaxPipelines) {  // replace the least recently used
+      auto lru = c->pipes.begin();
+      for (auto it = c->pipes.begin(); it != c->pipes.end(); ++it)
+        if (it->last_use < lru->last_use) lru = it;
+      if (lru->exec) STC_CUDA(cudaGraphExecDestroy(lru->exec));
+      c->pipes.erase(lru);
+    }
+    GroupPipeline q;
+    memcpy(q.key, key, sizeof(key));
+    q.state = caps_from(g, q.caps) ? 1 : -1;
+    q.last_use = ++c->pipe_clock;
+    c->pipes.push_back(q);
+    return o;
+  }
+  p->last_use = ++c->pipe_clock;
+  if (p->state < 0) return eager_group(c, in, me, eoff, gn, cfg, h, g);
+  stage_offsets(c, eoff);
+  bool replayed = false;
+  if (p->state >= 2 && (p->state == 2 || !p->exec || p->gen != c->buf_gen)) {
+    const Capture r = capture_group(c, *p, in, me, gn, cfg);
+    if (r == Capture::kFailed) {
+      p->state = -1;
+      return eager_group(c, in, me, eoff, gn, cfg, h, g);
+    }
+    if (r == Capture::kRetry) p->state = 1;
+  }
+  if (p->state == 3) {
+    STC_CUDA(cudaGraphLaunch(p->exec, c->stream));
+    c->launches += p->launches;
+    replayed = true;
+  } else {
+    enqueue_capped_group(c, in, me, gn, p->caps, cfg);
+  }
+  finish_group(c, gn, h);
+  if (c->h_pinned[C_OVERFLOW]) {
+    if (p->exec) STC_CUDA(cudaGraphExecDestroy(p->exec));
+    p->exec = nullptr;
+    const GroupOut o = eager_group(c, in, me, eoff, gn, cfg, h, g);
+    p->state = caps_from(g, p->caps) ? 1 : -1;
+    return o;
+  }
+  if (p->state == 1) p->state = 2;
+  return GroupOut{c->h_pinned[C_BATCH_N], c->h_pinned[C_BATCH_MU], replayed};
+}
+
 CountConfig count_config(const stc_opts* o) {
   CountConfig cfg;
   if (o) {
@@ -220,8 +438,10 @@ void stc_ctx_destroy(stc_ctx* c) {
   cudaSetDevice(c->device);
   if (c->own_stream) cudaStreamSynchronize(c->own_stream);
   if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+  release_pipelines(c);
   for (auto& b : c->bufs)
     if (b.p) cudaFree(b.p);
+  if (c->h_eoff) cudaFreeHost(c->h_eoff);
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
   if (c->h_pinned) cudaFreeHost(c->h_pinned);
@@ -246,6 +466,8 @@ stc_status stc_ctx_trim(stc_ctx* c) {
       STC_CUDA(cudaGraphExecDestroy(c->graph_exec));
       c->graph_exec = nullptr;
     }
+    release_pipelines(c);
+    c->buf_gen++;
     for (int i = 0; i < B_COUNT_; i++) {
       if (i == B_COUNTERS) continue;
       if (c->bufs[i].p) STC_CUDA(cudaFree(c->bufs[i].p));
@@ -490,26 +712,14 @@ stc_status stc_count_batch_packed(stc_ctx* c, const uint32_t* src, const uint32_
       const uint32_t gn = g1 - g0;
       std::vector<uint64_t> eoff(gn + 1);
       for (uint32_t i = 0; i <= gn; i++) eoff[i] = offsets[g0 + i] - e0;
-      STC_CUDA(cudaMemsetAsync(counters(c), 0, C_SLOTS * sizeof(uint64_t), c->stream));
       DeviceInput in;
       if (dev) {
         in = DeviceInput{src + e0, dst + e0, sign + e0};
       } else {
         in = stage_input(c, src + e0, dst + e0, sign + e0, me, o);
       }
-      DeviceGraph g;
-      build_graph_batch(c, in.src, in.dst, in.sign, me, eoff.data(), gn, g, /*totals=*/true);
-      uint64_t* gc = buffer<uint64_t>(c, B_BATCH_COUNTS, 4ull * gn);
-      STC_CUDA(cudaMemsetAsync(gc, 0, 4ull * gn * sizeof(uint64_t), c->stream));
-      cfg.graph_counts = gc;
-      count_triangles(c, g, cfg);
-      mark(c, 5);
       std::vector<uint64_t> h(4ull * gn);
-      STC_CUDA(cudaMemcpyAsync(h.data(), gc, h.size() * sizeof(uint64_t), cudaMemcpyDeviceToHost,
-                               c->stream));
-      STC_CUDA(cudaMemcpyAsync(c->h_pinned, counters(c), C_SLOTS * sizeof(uint64_t),
-                               cudaMemcpyDeviceToHost, c->stream));
-      STC_CUDA(cudaStreamSynchronize(c->stream));
+      const GroupOut go = count_group(c, in, me, eoff, gn, cfg, h);
       if (c->h_pinned[C_ERROR])
         fail(STC_ERR_INTERNAL, "device reported error word " + std::to_string(c->h_pinned[C_ERROR]));
       if (c->timing) {  // stage times summed over the groups
@@ -526,12 +736,13 @@ stc_status stc_count_batch_packed(stc_ctx* c, const uint32_t* src, const uint32_
         r.t3 = h[4ull * i + 3];
         total.triangles += r.t0 + r.t1 + r.t2 + r.t3;
       }
-      total.n += g.n;
-      total.m_input += g.m_input;
-      total.m_unique += g.m_unique;
-      total.m_forward += g.m_fwd;
+      total.n += go.n;
+      total.m_input += me;
+      total.m_unique += go.m_unique;
+      total.m_forward += go.m_unique;
       total.alg_bytes += c->h_pinned[C_ALG_BYTES];
       total.probe_bytes += c->h_pinned[C_PROBE_BYTES];
+      total.groups_replayed += go.replayed ? 1 : 0;
       g0 = g1;
     }
     mark(c, 7);

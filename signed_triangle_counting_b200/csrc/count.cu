@@ -1287,6 +1287,7 @@ struct HeadArcs {
 // in [range[0], range[1]).
 __global__ void __launch_bounds__(256) k_head_keys(Csr g, const uint32_t* __restrict__ asrc,
                                                    const uint32_t* __restrict__ fdeg, uint64_t m,
+                                                   const unsigned long long* __restrict__ m_dev,
                                                    const uint8_t* __restrict__ gtables,
                                                    const unsigned long long* __restrict__ range,
                                                    uint64_t* __restrict__ keys,
@@ -1295,6 +1296,7 @@ __global__ void __launch_bounds__(256) k_head_keys(Csr g, const uint32_t* __rest
                                                    unsigned long long* __restrict__ ctr) {
   constexpr int kItems = 4;  // arcs per lane with their gathers in flight together
   __shared__ uint8_t tab[kTableBytes];
+  if (m_dev) m = min(m, (uint64_t)*m_dev);  // m a capacity, *m_dev the arc count
   for (uint32_t i = threadIdx.x; i < kTableBytes; i += blockDim.x) tab[i] = gtables[i];
   __syncthreads();
   const uint32_t r0 = range ? (uint32_t)range[0] : 0u;
@@ -1663,7 +1665,8 @@ void prepare_head(const Tuning& tu) {
 // head-class kernels.  The launch parameters of the block and large classes
 // follow the tuning of the tail side's same classes.
 inline void enqueue_head_keys(cudaStream_t st, const Csr& csr, const uint32_t* asrc,
-                              const uint32_t* fdeg, uint64_t m, const HeadBufs& b,
+                              const uint32_t* fdeg, uint64_t m,
+                              const unsigned long long* m_dev, const HeadBufs& b,
                               const uint8_t* d_tables,
                               const unsigned long long* range, unsigned long long* ctr,
                               int& launches) {
@@ -1671,8 +1674,8 @@ inline void enqueue_head_keys(cudaStream_t st, const Csr& csr, const uint32_t* a
   STC_CUDA(cudaMemsetAsync(ctr + C_HEAD_NKEYS, 0, sizeof(unsigned long long), st));
   STC_CUDA(cudaMemsetAsync(b.need, 0, csr.n, st));
   const uint32_t grid = (uint32_t)std::min<uint64_t>((m + 1023) / 1024, kSMs * 8);
-  k_head_keys<<<std::max(1u, grid), 256, 0, st>>>(csr, asrc, fdeg, m, d_tables, range, b.keys,
-                                                  b.aend, b.need, ctr);
+  k_head_keys<<<std::max(1u, grid), 256, 0, st>>>(csr, asrc, fdeg, m, m_dev, d_tables, range,
+                                                  b.keys, b.aend, b.need, ctr);
   launches++;
 }
 
@@ -1810,6 +1813,7 @@ struct HeadPlan {
   const uint32_t* asrc = nullptr;
   const uint32_t* fdeg = nullptr;
   uint64_t m = 0;
+  const unsigned long long* m_dev = nullptr;  // arc count on the device when m is a capacity
   Tuning tuning;
 };
 
@@ -1821,7 +1825,7 @@ void enqueue_persistent(cudaStream_t st, const Csr& csr, const ClassBounds& cb, 
   const ArcTimes none{nullptr, nullptr};
   const uint8_t* need = nullptr;
   if (hp.bufs) {
-    enqueue_head_keys(st, csr, hp.asrc, hp.fdeg, hp.m, *hp.bufs, d_tables, nullptr, ctr,
+    enqueue_head_keys(st, csr, hp.asrc, hp.fdeg, hp.m, hp.m_dev, *hp.bufs, d_tables, nullptr, ctr,
                       launches);
     need = hp.bufs->need;
   }
@@ -1865,7 +1869,14 @@ void count_persistent(stc_ctx* c, const Csr& csr, const ClassBounds& cb, uint32_
                                 (int)StageMem::bytes(kLargeCap, 2 * kLargeCap)));
   if (hp.bufs) prepare_head<Sink, false>(hp.tuning);
   // The legacy default stream cannot be captured: launch directly there.
-  if (st == nullptr || st == cudaStreamLegacy || st == cudaStreamPerThread) {
+  // So does a count that is itself being captured (a batch group's whole
+  // pipeline) or that reads its arc count on the device (the one capped
+  // run that sizes such a pipeline's buffers).
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (st != nullptr && st != cudaStreamLegacy && st != cudaStreamPerThread)
+    STC_CUDA(cudaStreamIsCapturing(st, &cs));
+  if (st == nullptr || st == cudaStreamLegacy || st == cudaStreamPerThread ||
+      cs != cudaStreamCaptureStatusNone || hp.m_dev) {
     enqueue_persistent(st, csr, cb, lists, plan, ctr, d_tables, sink, hp, c->launches);
     return;
   }
@@ -2156,6 +2167,7 @@ void count_triangles(stc_ctx* c, const DeviceGraph& gin, const CountConfig& cfg)
       hp.asrc = g.asrc;
       hp.fdeg = g.fdeg;
       hp.m = g.m_fwd;
+      hp.m_dev = g.m_dev;
       hp.tuning = c->tuning;
     }
     if (cfg.vertex_counts) {
@@ -2173,7 +2185,8 @@ void count_triangles(stc_ctx* c, const DeviceGraph& gin, const CountConfig& cfg)
   }
   const uint8_t* need = nullptr;
   if (head) {
-    enqueue_head_keys(st, csr, g.asrc, g.fdeg, g.m_fwd, hb, d_table, range, ctr, c->launches);
+    enqueue_head_keys(st, csr, g.asrc, g.fdeg, g.m_fwd, g.m_dev, hb, d_table, range, ctr,
+                      c->launches);
     need = hb.need;
   }
   k_classify_count<<<kSMs * 4, 256, 0, st>>>(g.off, g.n, cb, ctr, range, need);

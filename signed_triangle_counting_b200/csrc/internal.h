@@ -74,7 +74,10 @@ enum CounterSlot {
   C_HEAD_QUEUE = 27,           // and the classes' work queues (3 slots)
   C_PROBE_BYTES = 30,          // probe-model bytes of the CSR
   C_HEAD_NKEYS = 31,           // head-side pass: keys (HEAD arcs) appended
-  C_SLOTS = 32
+  C_BATCH_N = 32,              // capped batch build: vertices of the union
+  C_BATCH_MU = 33,             // capped batch build: unique edges (= arcs)
+  C_OVERFLOW = 34,             // capped batch build: a capacity was exceeded (results void)
+  C_SLOTS = 40
 };
 
 // Values of the device error word: 1 = malformed forward CSR,
@@ -110,6 +113,32 @@ struct Tuning {
   uint32_t unroll[3] = {2, 2, 2};
 };
 
+// Sizes a batch group's build is launched with when nothing is read back to
+// the host between its stages: vertex capacity of the union, id bits of the
+// arc keys, degree bits of the vertex sort key and the degree sample shift.
+// They come from an earlier build of a group of the same shape; the device
+// checks the new group against them (C_OVERFLOW).
+struct BatchCaps {
+  uint32_t n = 0;
+  uint32_t bits = 1;
+  uint32_t dbits = 0;
+  uint32_t shift = 0;
+};
+
+// A batch group's whole pipeline (counters, build, count) as one captured
+// CUDA graph: the key it was built for, its capacities, and how far it got
+// (1 = capacities known from an uncapped build, 2 = buffers sized by one
+// capped run, 3 = captured; -1 = capture failed, always run uncapped).
+struct GroupPipeline {
+  uint64_t key[16] = {};
+  BatchCaps caps;
+  int state = 0;
+  cudaGraphExec_t exec = nullptr;
+  uint64_t gen = 0;   // buffer generation the graph was captured with
+  int launches = 0;   // kernels per replay
+  uint64_t last_use = 0;
+};
+
 }  // namespace stc
 
 struct stc_ctx {
@@ -133,6 +162,15 @@ struct stc_ctx {
   uint64_t graph_key[24] = {};
   int graph_launches = 0;  // kernels per replay of graph_exec
   stc::Tuning tuning;
+  // Batch groups captured whole (at most four, the least recently used
+  // replaced), the pinned staging of a group's edge offsets they copy from,
+  // and the buffer generation: bumped whenever a device buffer or the
+  // staging moves, which retires every captured graph.
+  std::vector<stc::GroupPipeline> pipes;
+  uint64_t* h_eoff = nullptr;
+  size_t h_eoff_cap = 0;
+  uint64_t buf_gen = 1;
+  uint64_t pipe_clock = 0;
 };
 
 namespace stc {
@@ -143,6 +181,7 @@ T* buffer(stc_ctx* c, BufId id, size_t count) {
   size_t bytes = count * sizeof(T);
   if (bytes == 0) bytes = 16;
   if (b.cap < bytes) {
+    c->buf_gen++;
     if (b.p) STC_CUDA(cudaFree(b.p));
     b.p = nullptr;
     b.cap = 0;
@@ -183,6 +222,12 @@ struct DeviceGraph {
   uint32_t* fdeg = nullptr;   // out-degree by rank
   uint32_t* asrc = nullptr;   // arcs: tail vertex (rank)
   uint32_t* nkey = nullptr;   // arcs: head << 1 | negative, padded by 4 (the head side's stream)
+  // A capped batch build (BatchCaps) leaves n and m_fwd as capacities: the
+  // arc count is then on the device (m_dev), vertices past the union's last
+  // rank have no arcs.
+  const unsigned long long* m_dev = nullptr;
+  uint32_t dbits = 0;  // degree bits of the vertex sort key (totals path)
+  uint32_t shift = 0;  // degree sample shift (totals path)
   // Batches: G graphs whose vertices (ids and ranks) are contiguous; graph
   // g owns [gbase[g], gbase[g + 1]).  G == 0 for a single graph.
   uint32_t G = 0;
@@ -214,6 +259,14 @@ void graph_from_forward_csr(stc_ctx* c, uint32_t n, uint64_t m, const uint64_t* 
 void build_graph_batch(stc_ctx* c, const uint32_t* d_src, const uint32_t* d_dst,
                        const int8_t* d_sign, uint64_t m, const uint64_t* h_eoff, uint32_t G,
                        DeviceGraph& g, bool totals = false);
+// The totals build of a batch at fixed capacities, with no host
+// synchronisation (capturable): edge offsets are copied from the pinned
+// staging c->h_eoff; g.n and g.m_fwd are capacities and g.m_dev the device
+// arc count; C_BATCH_N / C_BATCH_MU receive the real sizes and C_OVERFLOW is
+// set when the group does not fit `caps` (its counts are then void).
+void build_graph_batch_capped(stc_ctx* c, const uint32_t* d_src, const uint32_t* d_dst,
+                              const int8_t* d_sign, uint64_t m, uint32_t G, const BatchCaps& caps,
+                              DeviceGraph& g);
 // GPU text ingest: parses `size` bytes at d_text (device, padded to a
 // multiple of 16 bytes) into the device input arrays; returns the kept edge
 // count, the data line count and n.

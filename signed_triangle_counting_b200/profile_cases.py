@@ -9,6 +9,7 @@ the 126 MB L2 while keeping a few GB on the device.
     python -m signed_triangle_counting_b200.profile_cases text  --scale 20
     python -m signed_triangle_counting_b200.profile_cases batch --graphs 512
     python -m signed_triangle_counting_b200.profile_cases skew  --shrink 2
+    python -m signed_triangle_counting_b200.profile_cases mlp   --scale 16
 
 rmat   the power-law workload at RMAT scale `--scale` (generated on the
        device); dedup, orientation, CSR and count kernels
@@ -17,6 +18,9 @@ text   the same graph at `--scale` as `u v sign` text in host memory,
 batch  the first `--graphs` graphs of the 4,096-graph batch, in one call on
        the persistent engine
 skew   the skewed workload with its sizes divided by 2**`--shrink`
+mlp    the learned dispatcher: records per-cell cycles of every strategy on
+       the power-law graph at `--scale`, then each rep trains the MLP
+       (`k_mlp_train`, `--epochs`) and builds its tables (`k_mlp_tables`)
 """
 from __future__ import annotations
 
@@ -38,12 +42,13 @@ def _edge_text(el) -> bytes:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["rmat", "text", "batch", "skew"])
+    ap.add_argument("case", choices=["rmat", "text", "batch", "skew", "mlp"])
     ap.add_argument("--scale", type=int, default=22)
     ap.add_argument("--graphs", type=int, default=512)
     ap.add_argument("--shrink", type=int, default=2)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--dispatch", default="fixed", choices=["fixed", "learned"])
+    ap.add_argument("--epochs", type=int, default=3000)
     a = ap.parse_args()
 
     import torch
@@ -76,6 +81,13 @@ def main() -> None:
         ctx.set_tuning(autotune.tuning_for(4))
         run = lambda: ctx.count_batch_packed(src, dst, sign, offs, dispatch=a.dispatch,
                                              persistent=True)
+    elif a.case == "mlp":
+        from . import dispatcher
+        el = synth.rmat(synth.workload_seed(3), a.scale, 1 << a.scale, 16 << a.scale, p_pos=0.5)
+        rec = dispatcher.record(ctx, el.src, el.dst, el.sign)
+        params, _ = dispatcher.train(ctx, rec, epochs=a.epochs)
+        info["params"] = int(len(params))
+        run = lambda: dispatcher.train(ctx, rec, epochs=a.epochs)
     else:
         el = synth.workload(5, a.shrink)
         src = torch.from_numpy(el.src.view("int32")).to(dev)
