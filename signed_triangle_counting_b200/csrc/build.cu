@@ -313,7 +313,7 @@ void finish_csr_from_arc_keys(stc_ctx* c, DeviceGraph& g, uint64_t* akeys, uint6
   g.nbr = buffer<uint32_t>(c, B_NBR, g.m_fwd + 4);  // + 4: the engine reads whole int4 chunks
   g.sgn = buffer<int8_t>(c, B_SGN, g.m_fwd + 4);
   g.asrc = buffer<uint32_t>(c, B_ASRC, g.m_fwd);
-  g.nkey = buffer<uint32_t>(c, B_NKEY, g.m_fwd + 4);
+  g.nkey = buffer<uint32_t>(c, B_NKEY, g.m_fwd + 8);
   k_csr_fill<<<grid_for(g.m_fwd, 4), kThreads, 0, c->stream>>>(sorted, g.m_fwd, g.bits, g.fdeg,
                                                                g.off, g.nbr, g.sgn, g.asrc,
                                                                g.nkey,
@@ -804,7 +804,7 @@ void build_totals(stc_ctx* c, const EdgeIds& e, const int8_t* d_sign, uint64_t m
       g.nbr = buffer<uint32_t>(c, B_NBR, m + 4);
       g.sgn = buffer<int8_t>(c, B_SGN, m + 4);
       g.asrc = buffer<uint32_t>(c, B_ASRC, m);
-      g.nkey = buffer<uint32_t>(c, B_NKEY, m + 4);
+      g.nkey = buffer<uint32_t>(c, B_NKEY, m + 8);
       range_apply(flag, EmitArc{sorted, g.bits, g.nbr, g.sgn, g.asrc, g.nkey}, m, sums, st,
                   &c->launches);
     } else {
@@ -818,7 +818,7 @@ void build_totals(stc_ctx* c, const EdgeIds& e, const int8_t* d_sign, uint64_t m
       g.nbr = buffer<uint32_t>(c, B_NBR, g.m_fwd + 4);  // + 4: the engine reads whole int4 chunks
       g.sgn = buffer<int8_t>(c, B_SGN, g.m_fwd + 4);
       g.asrc = buffer<uint32_t>(c, B_ASRC, g.m_fwd);
-      g.nkey = buffer<uint32_t>(c, B_NKEY, g.m_fwd + 4);
+      g.nkey = buffer<uint32_t>(c, B_NKEY, g.m_fwd + 8);
       range_apply(flag, EmitArc{sorted, g.bits, g.nbr, g.sgn, g.asrc, g.nkey}, g.m_valid, sums,
                   st, &c->launches);
     }

@@ -137,9 +137,15 @@ __device__ __forceinline__ uint32_t lower_bound(const uint32_t* a, uint32_t len,
 }
 
 // Multiplicative hash: the top bits of x * an odd constant.
+// It hashes 2x, so that a signed key 2x | sign hashes by clearing its sign
+// bit (hash_slot_k2) without a shift.
 __device__ __forceinline__ uint32_t hash_slot(uint32_t x, uint32_t shift) {
-  return (x * 0x85EBCA77u) >> shift;
+  return ((x << 1) * 0x85EBCA77u) >> shift;
 }
+__device__ __forceinline__ uint32_t hash_slot_k2(uint32_t k2, uint32_t shift) {
+  return (k2 * 0x85EBCA77u) >> shift;
+}
+
 
 // SEARCH for one arc by one warp: each lane holds the pivot B[lane * step];
 // an A' element (a[i], i in [i0, d)) finds its segment with five shuffles and
@@ -310,18 +316,22 @@ __device__ __noinline__ uint32_t probe_rest(const uint32_t* hk, uint32_t nb, uin
   }
 }
 
+// Chunks of arc i's streamed extent: aligned groups of 4 entries (16
+// bytes), or of 8 entries (32 bytes) with kWide (the head side's stream).
+template <bool kWide = false>
 __device__ __forceinline__ uint32_t arc_chunks(const StageMem& m, uint32_t i) {
   const uint8_t st = m.st[i];
   if (st != STC_STRATEGY_HASH && st != STC_STRATEGY_MERGE && st != STC_STRATEGY_SPLIT) return 0;
-  return ((m.hi[i] + 3) >> 2) - (m.lo[i] >> 2);
+  return kWide ? ((m.hi[i] + 7) >> 3) - (m.lo[i] >> 3) : ((m.hi[i] + 3) >> 2) - (m.lo[i] >> 2);
 }
 
-// pre[i] = int4 chunks of the streamed arcs before arc i; pre[d] = total.
+// pre[i] = chunks of the streamed arcs before arc i; pre[d] = total.
+template <bool kWide = false>
 __device__ __forceinline__ void warp_chunk_scan(const StageMem& m, uint32_t d, uint32_t lane) {
   uint32_t carry = 0;
   for (uint32_t r = 0; r < d; r += 32) {
     const uint32_t i = r + lane;
-    const uint32_t c = i < d ? arc_chunks(m, i) : 0;
+    const uint32_t c = i < d ? arc_chunks<kWide>(m, i) : 0;
     const uint32_t inc = warp_inclusive_scan(c);
     if (i < d) m.pre[i] = carry + inc - c;
     carry += __shfl_sync(kFull, inc, 31);
@@ -330,12 +340,12 @@ __device__ __forceinline__ void warp_chunk_scan(const StageMem& m, uint32_t d, u
   __syncwarp();
 }
 
-template <int THREADS>
+template <int THREADS, bool kWide = false>
 __device__ __forceinline__ void block_chunk_scan(const StageMem& m, uint32_t d, uint32_t* tmp) {
   uint32_t carry = 0;
   for (uint32_t r = 0; r < d; r += THREADS) {
     const uint32_t i = r + threadIdx.x;
-    const uint32_t c = i < d ? arc_chunks(m, i) : 0;
+    const uint32_t c = i < d ? arc_chunks<kWide>(m, i) : 0;
     uint32_t total;
     const uint32_t excl = block_exclusive_scan<THREADS>(c, tmp, total);
     if (i < d) m.pre[i] = carry + excl;
@@ -433,27 +443,31 @@ __device__ __forceinline__ void process_chunk(const StageMem& m, uint32_t d, con
   }
 }
 
-// HASH for one int4 chunk of signed heads (id << 1 | negative, the head
-// side's stream): as process_chunk's HASH path, with each entry's sign taken
-// from its own low bit instead of a separate sign word.
+// HASH for an aligned chunk of eight signed heads (id << 1 | negative, the
+// head side's stream; a, then b), vm its 8-bit mask: as process_chunk's HASH
+// path, with each entry's sign taken from its own low bit instead of a
+// separate sign word, one mask test and one overflow test per eight keys.
 template <class PC>
-__device__ __forceinline__ void process_keyed_chunk(const StageMem& m, const Geo& geo,
-                                                    const uint4& q, uint32_t vm, uint32_t nuv,
-                                                    PC& pc) {
+__device__ __forceinline__ void process_keyed_chunk8(const StageMem& m, const Geo& geo, uint4 a,
+                                                     uint4 b, uint32_t vm, uint32_t nuv,
+                                                     PC& pc) {
   constexpr uint32_t kNoKey = kNoId << 1;
-  uint4 k4 = q;
-  if (vm != 0xFu) {
-    k4.x = (vm & 1u) ? k4.x : kNoKey;
-    k4.y = (vm & 2u) ? k4.y : kNoKey;
-    k4.z = (vm & 4u) ? k4.z : kNoKey;
-    k4.w = (vm & 8u) ? k4.w : kNoKey;
+  if (vm != 0xFFu) {
+    a.x = (vm & 1u) ? a.x : kNoKey;
+    a.y = (vm & 2u) ? a.y : kNoKey;
+    a.z = (vm & 4u) ? a.z : kNoKey;
+    a.w = (vm & 8u) ? a.w : kNoKey;
+    b.x = (vm & 16u) ? b.x : kNoKey;
+    b.y = (vm & 32u) ? b.y : kNoKey;
+    b.z = (vm & 64u) ? b.z : kNoKey;
+    b.w = (vm & 128u) ? b.w : kNoKey;
   }
   bool again = false;
 #pragma unroll
-  for (uint32_t e = 0; e < 4; e++) {
-    const uint32_t key = pick4(k4, e);
+  for (uint32_t e = 0; e < 8; e++) {
+    const uint32_t key = e < 4 ? pick4(a, e) : pick4(b, e - 4);
     const uint32_t k2 = key & ~1u;  // 2 x
-    const uint2 w = *reinterpret_cast<const uint2*>(m.hk + 2 * hash_slot(key >> 1, geo.shift));
+    const uint2 w = *reinterpret_cast<const uint2*>(m.hk + 2 * hash_slot_k2(k2, geo.shift));
     const uint32_t d0 = w.x - k2, d1 = w.y - k2;
     const bool hit = d0 < 2 || d1 < 2;
     again |= !hit && w.y != kEmpty;
@@ -461,14 +475,99 @@ __device__ __forceinline__ void process_keyed_chunk(const StageMem& m, const Geo
   }
   if (again) {
 #pragma unroll 1
-    for (uint32_t e = 0; e < 4; e++) {
-      const uint32_t key = pick4(k4, e), x = key >> 1;
+    for (uint32_t e = 0; e < 8; e++) {
+      const uint32_t key = e < 4 ? pick4(a, e) : pick4(b, e - 4), x = key >> 1;
       const uint2 w = *reinterpret_cast<const uint2*>(m.hk + 2 * hash_slot(x, geo.shift));
       if (w.x - (key & ~1u) < 2 || w.y - (key & ~1u) < 2 || w.y == kEmpty) continue;
       const uint32_t r = probe_rest(m.hk, geo.nb, geo.shift, x);
       if (r) pc.add(nuv + (r >> 1) + (key & 1u));
     }
   }
+}
+
+// The head side's stream: the staged in-arcs' A' extents of signed heads
+// (g.nkey) as one sequence of aligned 8-entry (32-byte) chunks, shared out
+// as in stream_pass (warp shares, lanes on consecutive chunks, the last
+// eighth claimed from `next`).  A lane loads a chunk with two 16-byte
+// loads, UK chunks per round, and the cursor, mask and branch work per
+// chunk is spread over eight keys instead of four.  pre[] counts 8-entry
+// chunks (block_chunk_scan / warp_chunk_scan with kWide).
+template <int UK>
+__device__ __forceinline__ void stream_pass_keyed(const Csr& g, const StageMem& m, uint32_t d,
+                                                  uint32_t warp, uint32_t warps, uint32_t lane,
+                                                  const Geo& geo, TypeCounts& tc,
+                                                  uint32_t* next) {
+  const uint32_t total = m.pre[d];
+  const uint32_t fixed = next ? total - total / 8 : total;
+  const uint32_t per = (fixed + warps - 1) / warps;
+  uint32_t seg_begin = min(fixed, warp * per), seg_end = min(fixed, seg_begin + per);
+  uint32_t k = 0, pk, pk1, cb, mf, ml, anuv;
+  auto enter = [&](uint32_t kk) {
+    pk = m.pre[kk];
+    pk1 = m.pre[kk + 1];
+    const uint32_t alo = m.lo[kk], ahi = m.hi[kk];
+    cb = (alo >> 3) - pk;
+    mf = (0xFFu << (alo & 7u)) & 0xFFu;
+    ml = 0xFFu >> (7u - ((ahi - 1u) & 7u));
+    anuv = m.s[kk] < 0;
+  };
+  // 8-bit fields: at most 8 UK adds per field per round.
+  constexpr uint32_t kDrainRounds = 255 / (8 * UK);
+  constexpr uint32_t kClaim = 32 * UK;  // 8-entry chunks a warp claims at a time (one round)
+  const uint4* src = reinterpret_cast<const uint4*>(g.nkey);
+  PackedCounts8 p8;
+  uint32_t rounds = 0;
+  while (true) {
+    if (seg_begin < seg_end) {
+      {
+        uint32_t lo_k = k, hi_k = d;
+        const uint32_t c0 = seg_begin + lane;
+        while (hi_k - lo_k > 1) {
+          const uint32_t mid = (lo_k + hi_k) >> 1;
+          if (m.pre[mid] <= c0) lo_k = mid; else hi_k = mid;
+        }
+        k = lo_k;
+        enter(k);
+      }
+      for (uint32_t base = seg_begin; base < seg_end; base += 32 * UK) {
+        uint4 qa[UK], qb[UK];
+        uint32_t vm[UK], snuv[UK];
+#pragma unroll
+        for (int u = 0; u < UK; u++) {
+          const uint32_t c = base + 32 * u + lane;
+          vm[u] = 0;
+          if (c < seg_end) {
+            if (c >= pk1) {
+              do {
+                k++;
+              } while (m.pre[k + 1] <= c);
+              enter(k);
+            }
+            const uint32_t ci = cb + c;
+            qa[u] = src[2 * ci];
+            qb[u] = src[2 * ci + 1];
+            vm[u] = (c == pk ? mf : 0xFFu) & (c + 1 == pk1 ? ml : 0xFFu);
+            snuv[u] = anuv;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < UK; u++)
+          if (vm[u]) process_keyed_chunk8(m, geo, qa[u], qb[u], vm[u], snuv[u], p8);
+        if (++rounds == kDrainRounds) {
+          p8.drain(tc);
+          rounds = 0;
+        }
+      }
+    }
+    if (!next) break;
+    uint32_t s0 = 0;
+    if (lane == 0) s0 = atomicAdd(next, kClaim);
+    s0 = fixed + __shfl_sync(kFull, s0, 0);
+    if (s0 >= total) break;
+    seg_begin = s0;
+    seg_end = min(total, s0 + kClaim);
+  }
+  p8.drain(tc);
 }
 
 // The streamed arcs of a staged list as one sequence of aligned int4
@@ -486,9 +585,7 @@ __device__ __forceinline__ void process_keyed_chunk(const StageMem& m, const Geo
 // MERGE chunks are merged against the sorted A' instead.
 // kSplit: compiled with the SPLIT path (a split index per arc, a per-chunk
 // choice of source); kernels without it stay as lean as before SPLIT.
-// kKeyed (the head side, every arc HASH): chunks come from the signed heads
-// g.nkey, one 16-byte load each.
-template <int U, bool kSplit, bool kKeyed = false>
+template <int U, bool kSplit>
 __device__ __forceinline__ void stream_pass(const Csr& g, const StageMem& m, uint32_t d,
                                             uint32_t warp, uint32_t warps, uint32_t lane,
                                             const Geo& geo, TypeCounts& tc, uint32_t* next) {
@@ -544,12 +641,7 @@ __device__ __forceinline__ void stream_pass(const Csr& g, const StageMem& m, uin
               enter(k);
             }
             const uint32_t ci = cb + c;
-            if (kKeyed) {
-              q[u] = reinterpret_cast<const uint4*>(g.nkey)[ci];
-              sw[u] = 0;
-            } else {
-              load_chunk(g, ci, kSplit ? ast : (uint32_t)STC_STRATEGY_HASH, asp, q[u], sw[u]);
-            }
+            load_chunk(g, ci, kSplit ? ast : (uint32_t)STC_STRATEGY_HASH, asp, q[u], sw[u]);
             vm[u] = (c == pk ? mf : 0xFu) & (c + 1 == pk1 ? ml : 0xFu);
             sk[u] = k;
             snuv[u] = anuv;
@@ -558,10 +650,7 @@ __device__ __forceinline__ void stream_pass(const Csr& g, const StageMem& m, uin
         }
 #pragma unroll
         for (int u = 0; u < U; u++)
-          if (vm[u]) {
-            if (kKeyed) process_keyed_chunk(m, geo, q[u], vm[u], snuv[u], p8);
-            else process_chunk(m, d, geo, q[u], sw[u], vm[u], sk[u], snuv[u], sst[u], p8);
-          }
+          if (vm[u]) process_chunk(m, d, geo, q[u], sw[u], vm[u], sk[u], snuv[u], sst[u], p8);
         if (++rounds == kDrainRounds) {
           p8.drain(tc);
           rounds = 0;
@@ -1521,8 +1610,11 @@ __global__ void __launch_bounds__(256) k_head_warp(Csr g, HeadArcs h, const uint
       if (kTime) {
         timed_head_pass(g, h, m, tn, d, 0, 1, lane, geo, pc, out, at);
       } else {
-        warp_chunk_scan(m, tn, lane);
-        stream_pass<U, false, true>(g, m, tn, 0, 1, lane, geo, out, nullptr);
+        warp_chunk_scan<true>(m, tn, lane);
+        // U / 2 chunks of 8 entries: U 16-byte loads in flight per lane, as
+        // in the tail side (more raise the registers above 64 and cost
+        // this kernel a CTA per SM).
+        stream_pass_keyed<(U > 1 ? U / 2 : 1)>(g, m, tn, 0, 1, lane, geo, out, nullptr);
       }
       __syncwarp();
     }
@@ -1598,8 +1690,9 @@ __global__ void __launch_bounds__(THREADS) k_head_block(Csr g, HeadArcs h,
       if (kTime) {
         timed_head_pass(g, h, m, tn, d, w, kWarps, lane, geo, pc, out, at);
       } else {
-        block_chunk_scan<THREADS>(m, tn, scan_tmp);
-        stream_pass<U, false, true>(g, m, tn, w, kWarps, lane, geo, out, next);
+        block_chunk_scan<THREADS, true>(m, tn, scan_tmp);
+        // U chunks of 8 entries: 2 U 16-byte loads in flight per lane.
+        stream_pass_keyed<U>(g, m, tn, w, kWarps, lane, geo, out, next);
       }
       __syncthreads();
     }

@@ -47,7 +47,7 @@ enum BufId {
   B_HEAD_END,                     // head-side pass: end of each arc's tail list (m)
   B_HEAD_RUNS,                    // head-side pass: in-arc range per head vertex (2 n)
   B_HEAD_LIST,                    // head-side pass: head vertices by class, plan, flags
-  B_NKEY,                         // arcs: head << 1 | negative (m + 4)
+  B_NKEY,                         // arcs: head << 1 | negative (m + 8)
   B_COUNT_
 };
 
@@ -221,7 +221,7 @@ struct DeviceGraph {
   int8_t* sgn = nullptr;      // arcs: +1 / -1
   uint32_t* fdeg = nullptr;   // out-degree by rank
   uint32_t* asrc = nullptr;   // arcs: tail vertex (rank)
-  uint32_t* nkey = nullptr;   // arcs: head << 1 | negative, padded by 4 (the head side's stream)
+  uint32_t* nkey = nullptr;   // arcs: head << 1 | negative, padded by 8 (the head side's stream)
   // A capped batch build (BatchCaps) leaves n and m_fwd as capacities: the
   // arc count is then on the device (m_dev), vertices past the union's last
   // rank have no arcs.
