@@ -261,32 +261,55 @@ static __global__ void __launch_bounds__(1024) k_scan_small(uint64_t* __restrict
   if (threadIdx.x == 0) a[n] = total;
 }
 
+// Index into a tile buffer with one padding word per 32: the blocked reads
+// (thread t, item j at t * kScanItems + j) then hit 32 distinct banks.
+__device__ __forceinline__ uint32_t tile_pad(uint32_t x) { return x + (x >> 5); }
+
+// Every element's exclusive prefix to `emit`, tile by tile: f is evaluated
+// and emit called in a striped order (consecutive threads on consecutive
+// elements, so that the loads inside f and the stores inside emit
+// coalesce), while the scan itself runs over a blocked copy of the tile's
+// values in shared memory.
 template <class F, class E>
 __global__ void __launch_bounds__(kScanThreads) k_range_apply(F f, E emit, uint64_t n,
                                                               uint64_t per_cta,
                                                               const uint64_t* __restrict__ offs) {
+  constexpr uint32_t kPadded = kScanTile + kScanTile / 32;
   __shared__ uint64_t tmp[kScanThreads / 32 + 1];
+  __shared__ uint32_t sv[kPadded];  // values
+  __shared__ uint64_t sp[kPadded];  // tile-relative exclusive prefixes
   const uint64_t begin = (uint64_t)blockIdx.x * per_cta;
   const uint64_t end = begin + per_cta < n ? begin + per_cta : n;
   uint64_t carry = offs[blockIdx.x];
   for (uint64_t tile = begin; tile < end; tile += kScanTile) {
-    // Blocked arrangement: thread t owns kScanItems consecutive elements.
-    const uint64_t b = tile + (uint64_t)threadIdx.x * kScanItems;
+#pragma unroll
+    for (int j = 0; j < kScanItems; j++) {
+      const uint32_t x = j * kScanThreads + threadIdx.x;
+      sv[tile_pad(x)] = tile + x < end ? f(tile + x) : 0u;
+    }
+    __syncthreads();
     uint32_t v[kScanItems];
     uint64_t s = 0;
 #pragma unroll
     for (int j = 0; j < kScanItems; j++) {
-      v[j] = (b + j < end) ? f(b + j) : 0u;
+      v[j] = sv[tile_pad(threadIdx.x * kScanItems + j)];
       s += v[j];
     }
     uint64_t total;
-    uint64_t run = carry + block_exclusive_scan<kScanThreads>(s, tmp, total);
+    uint64_t run = block_exclusive_scan<kScanThreads>(s, tmp, total);
 #pragma unroll
     for (int j = 0; j < kScanItems; j++) {
-      if (b + j < end) emit(b + j, run, v[j]);
+      sp[tile_pad(threadIdx.x * kScanItems + j)] = run;
       run += v[j];
     }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kScanItems; j++) {
+      const uint32_t x = j * kScanThreads + threadIdx.x;
+      if (tile + x < end) emit(tile + x, carry + sp[tile_pad(x)], sv[tile_pad(x)]);
+    }
     carry += total;
+    __syncthreads();  // the next tile reuses sv and sp
   }
 }
 
