@@ -1374,8 +1374,17 @@ struct HeadArcs {
 // an arc left to the tail side (the array starts at 0; tails without such
 // arcs are not staged there).  `range` (a sharded count) keeps only tails
 // in [range[0], range[1]).
+// Size bucket of every vertex's out-degree, one byte each: the head keys
+// gather it for every arc's head, from an array a quarter the size of the
+// out-degrees (more of it stays in L2).
+__global__ void k_fdeg_bucket(const uint32_t* __restrict__ fdeg, uint32_t n,
+                              uint8_t* __restrict__ out) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = (uint8_t)size_bucket(fdeg[i]);
+}
+
 __global__ void __launch_bounds__(256) k_head_keys(Csr g, const uint32_t* __restrict__ asrc,
-                                                   const uint32_t* __restrict__ fdeg, uint64_t m,
+                                                   const uint8_t* __restrict__ fbkt, uint64_t m,
                                                    const unsigned long long* __restrict__ m_dev,
                                                    const uint8_t* __restrict__ gtables,
                                                    const unsigned long long* __restrict__ range,
@@ -1407,7 +1416,7 @@ __global__ void __launch_bounds__(256) k_head_keys(Csr g, const uint32_t* __rest
       const uint64_t i = base + 32 * q + lane;
       ub[q] = i < m ? g.off[u[q]] : 0;
       ue[q] = i < m ? g.off[u[q] + 1] : 0;
-      blen[q] = i < m ? fdeg[v[q]] : 0u;
+      blen[q] = i < m ? fbkt[v[q]] : 0u;
     }
 #pragma unroll
     for (int q = 0; q < kItems; q++) {
@@ -1417,7 +1426,7 @@ __global__ void __launch_bounds__(256) k_head_keys(Csr g, const uint32_t* __rest
         const uint32_t alen = (uint32_t)(ue[q] - i - 1);
         if (alen && blen[q] && u[q] >= r0 && u[q] < r1) {
           head = tab[256 * table_class((uint32_t)(ue[q] - ub[q])) + 16 * size_bucket(alen) +
-                     size_bucket(blen[q])] == STC_STRATEGY_HEAD;
+                     blen[q]] == STC_STRATEGY_HEAD;
           if (!head) need[u[q]] = 1;  // u keeps an arc for the tail side
         }
       }
@@ -1463,13 +1472,19 @@ __global__ void __launch_bounds__(256) k_head_runs(const uint64_t* __restrict__ 
 #pragma unroll
       for (int k = 0; k < kHeadClasses; k++) cnt[k] += c == (uint32_t)k;
     } else {
-      const unsigned peers = __match_any_sync(kFull, c);
-      const uint32_t leader = __ffs(peers) - 1;
-      uint32_t pos = 0;
-      if (c < kHeadClasses && lane == leader)
-        pos = (uint32_t)atomicAdd(ctr + C_HEAD_CURSOR + c, (unsigned long long)__popc(peers));
-      pos = __shfl_sync(kFull, pos, leader) + __popc(peers & lanemask_lt());
-      if (c < kHeadClasses) hl[kHeadPlanWords + hl[c] + pos] = (uint32_t)j;
+      // Item starts are rare (about one entry in fifty): one ballot per
+      // class, and an atomic only where the warp holds some.
+#pragma unroll
+      for (uint32_t k = 0; k < (uint32_t)kHeadClasses; k++) {
+        const unsigned peers = __ballot_sync(kFull, c == k);
+        if (peers == 0) continue;
+        const uint32_t leader = __ffs(peers) - 1;
+        uint32_t pos = 0;
+        if (lane == leader)
+          pos = (uint32_t)atomicAdd(ctr + C_HEAD_CURSOR + k, (unsigned long long)__popc(peers));
+        pos = __shfl_sync(kFull, pos, leader) + __popc(peers & lanemask_lt());
+        if (c == k) hl[kHeadPlanWords + hl[k] + pos] = (uint32_t)j;
+      }
     }
   }
   if (!kFill) {
@@ -1767,9 +1782,11 @@ inline void enqueue_head_keys(cudaStream_t st, const Csr& csr, const uint32_t* a
   STC_CUDA(cudaMemsetAsync(ctr + C_HEAD_NKEYS, 0, sizeof(unsigned long long), st));
   STC_CUDA(cudaMemsetAsync(b.need, 0, csr.n, st));
   const uint32_t grid = (uint32_t)std::min<uint64_t>((m + 1023) / 1024, kSMs * 8);
-  k_head_keys<<<std::max(1u, grid), 256, 0, st>>>(csr, asrc, fdeg, m, m_dev, d_tables, range,
+  uint8_t* fbkt = reinterpret_cast<uint8_t*>(b.runs);  // free until the runs are found
+  k_fdeg_bucket<<<kSMs * 8, 256, 0, st>>>(fdeg, csr.n, fbkt);
+  k_head_keys<<<std::max(1u, grid), 256, 0, st>>>(csr, asrc, fbkt, m, m_dev, d_tables, range,
                                                   b.keys, b.aend, b.need, ctr);
-  launches++;
+  launches += 2;
 }
 
 template <class Sink, bool kTime>

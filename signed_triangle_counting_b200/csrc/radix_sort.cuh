@@ -78,18 +78,39 @@ static __global__ void __launch_bounds__(kSortThreads) k_radix_upsweep(
 }
 
 // Exclusive scan of `n` 32-bit counts in place by one CTA of 1024 threads.
+// Each warp takes a contiguous run of 32-entry rows, read and written a
+// row at a time (coalesced): a first pass sums its run, the 32 sums are
+// scanned in shared memory, and a second pass scans row by row with the
+// warp's carry.
 static __global__ void __launch_bounds__(1024) k_scan_counts(uint32_t* __restrict__ a, uint32_t n) {
-  __shared__ uint32_t tmp[33];
-  const uint32_t per = (n + 1023) / 1024;
-  const uint32_t b = threadIdx.x * per, e = b + per < n ? b + per : n;
+  __shared__ uint32_t wbase[32];
+  const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+  const uint32_t rows = (n + 31) / 32;
+  const uint32_t per = (rows + 31) / 32;
+  const uint32_t r0 = min(rows, warp * per), r1 = min(rows, r0 + per);
   uint32_t s = 0;
-  for (uint32_t i = b; i < e; i++) s += a[i];
-  uint32_t total;
-  uint32_t run = block_exclusive_scan<1024>(s, tmp, total);
-  for (uint32_t i = b; i < e; i++) {
-    uint32_t x = a[i];
-    a[i] = run;
-    run += x;
+#pragma unroll 4
+  for (uint32_t r = r0; r < r1; r++) {
+    const uint32_t i = r * 32 + lane;
+    s += i < n ? a[i] : 0u;
+  }
+  s = __reduce_add_sync(kFull, s);
+  if (lane == 0) wbase[warp] = s;
+  __syncthreads();
+  if (warp == 0) {
+    const uint32_t t = wbase[lane];
+    const uint32_t inc = warp_inclusive_scan(t);
+    wbase[lane] = inc - t;
+  }
+  __syncthreads();
+  uint32_t carry = wbase[warp];
+#pragma unroll 4
+  for (uint32_t r = r0; r < r1; r++) {
+    const uint32_t i = r * 32 + lane;
+    const uint32_t x = i < n ? a[i] : 0u;
+    const uint32_t inc = warp_inclusive_scan(x);
+    if (i < n) a[i] = carry + inc - x;
+    carry += __shfl_sync(kFull, inc, 31);
   }
 }
 
