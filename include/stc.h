@@ -293,8 +293,15 @@ stc_status stc_count_oriented_csr_noalloc(const uint64_t* d_offsets, const uint3
  * array of G + 1 entries and outs[g] receives graph g's counts.  The graphs
  * are counted together as one disjoint union whose vertex order is
  * graph-major and (degree, id) within each graph, so every graph is oriented
- * exactly as it would be alone.  No counterpart in the reference, which
- * counts one graph per process. */
+ * exactly as it would be alone.  With STC_F_PERSISTENT on a stream other
+ * than the legacy default stream, each group of graphs (at most 1.5 Gi
+ * input edges) is captured whole, build and count, as one CUDA graph on its
+ * third call with the same input pointers, sizes and options, and replayed
+ * on every call after that while the context's buffers stay in place
+ * (stc_stats.groups_replayed); a group whose graphs outgrow the sizes it
+ * was captured at is counted again without the graph, with the same
+ * results.  No counterpart in the reference, which counts one graph per
+ * process. */
 stc_status stc_count_batch_packed(stc_ctx* ctx, const uint32_t* src, const uint32_t* dst,
                                   const int8_t* sign, const uint64_t* offsets, uint32_t G,
                                   const stc_opts* opts, stc_counts* outs);
