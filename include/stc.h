@@ -19,7 +19,13 @@
  *    lower to the higher vertex of that order (MC/graph_io.h:261-330);
  *  - a triangle's type is its number of negative edges: 0 -> T3 (+++),
  *    1 -> T2 (++-), 2 -> T1 (+--), 3 -> T0 (---) (MC/tc_serial.cpp:95-112).
- * Vertex ids must be below 2^31 - 1 and an edge list below 2^32 elements.
+ * Counts of totals (stc_count, stc_count_text, batches of graphs whose ids
+ * stay below 2^31 - 1 in all) take any 32-bit vertex id: a list whose
+ * largest id reaches 2^31 - 1 is relabelled on the device to dense ids in
+ * the same order first, which changes no count.  Calls that report per
+ * vertex or per id (vertex counts, CSR export, shards, the timing recorder
+ * and the autotuner) need ids below 2^31 - 1.  An edge list stays below
+ * 2^32 elements, and a list's distinct ids below 2^31 - 1.
  */
 #ifndef STC_H
 #define STC_H
@@ -39,7 +45,7 @@ typedef enum stc_status {
   STC_ERR_IO = 2,               /* file cannot be opened / read (MC/graph_io.h:40-59) */
   STC_ERR_CUDA = 3,             /* a CUDA call failed; see stc_ctx_last_error */
   STC_ERR_OUT_OF_MEMORY = 4,    /* host or device allocation failed */
-  STC_ERR_LIMIT = 5,            /* id >= 2^31 - 1 or list >= 2^32 elements */
+  STC_ERR_LIMIT = 5,            /* id >= 2^31 - 1 where ids are reported, list >= 2^32 elements */
   STC_ERR_DEVICE_TIMEOUT = 6,   /* a bounded device-side wait expired */
   STC_ERR_NO_DEVICE = 7,        /* no CUDA device, or not an sm_100 part */
   STC_ERR_INTERNAL = 8          /* a self-check failed (e.g. strategies disagree) */

@@ -847,6 +847,81 @@ void build_totals(stc_ctx* c, const EdgeIds& e, const int8_t* d_sign, uint64_t m
   mark(c, 4);
 }
 
+// ---------------------------------------------------- dense relabel ----
+// Counts of totals accept any 32-bit id: an edge list whose largest id
+// reaches 2^31 - 1 (where the engine's signed keys and ranks would not fit)
+// is relabelled to dense ids first, the index of each id among the list's
+// distinct ids.  The relabelling keeps the ids' order, so the graph, its
+// (degree, id) order and its counts are those of the original list.
+
+// Both endpoints of every edge as 64-bit sort keys.
+__global__ void k_endpoint_keys(const uint32_t* __restrict__ u, const uint32_t* __restrict__ v,
+                                uint64_t m, uint64_t* __restrict__ keys) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
+    keys[2 * i] = u[i];
+    keys[2 * i + 1] = v[i];
+  }
+}
+
+struct DistinctEmit {
+  const uint64_t* keys;
+  uint32_t* out;
+  __device__ void operator()(uint64_t i, uint64_t pos, uint32_t flag) const {
+    if (flag) out[pos] = (uint32_t)keys[i];
+  }
+};
+
+__device__ __forceinline__ uint32_t dense_id(const uint32_t* __restrict__ ids, uint32_t nd,
+                                             uint32_t x) {
+  uint32_t lo = 0, hi = nd;  // first index with ids[index] >= x (x is present)
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (ids[mid] < x) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void k_relabel(const uint32_t* __restrict__ u, const uint32_t* __restrict__ v,
+                          uint64_t m, const uint32_t* __restrict__ ids, uint32_t nd,
+                          uint32_t* __restrict__ ou, uint32_t* __restrict__ ov) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
+    ou[i] = dense_id(ids, nd, u[i]);
+    ov[i] = dense_id(ids, nd, v[i]);
+  }
+}
+
+// Relabels the m edges at (*src, *dst) to dense ids in context buffers and
+// points *src / *dst at them; returns the number of distinct ids.
+uint64_t relabel_dense(stc_ctx* c, const uint32_t** src, const uint32_t** dst, uint64_t m) {
+  cudaStream_t st = c->stream;
+  uint32_t* sort_counts = buffer<uint32_t>(c, B_SORT_COUNTS, (size_t)kRadix * kMaxSortGrid);
+  uint64_t* sums = buffer<uint64_t>(c, B_SCAN_SUMS, kMaxSortGrid + 1);
+  uint64_t* ka = buffer<uint64_t>(c, B_KEYS_A, 2 * m);
+  uint64_t* kb = buffer<uint64_t>(c, B_KEYS_B, 2 * m);
+  k_endpoint_keys<<<grid_for(m, 4), kThreads, 0, st>>>(*src, *dst, m, ka);
+  c->launches++;
+  const uint64_t* sorted = radix_sort(ka, kb, 2 * m, 0, 32, sort_counts, st, &c->launches);
+  const UniqueFlag flag{sorted, 0xFFFFFFFFull};
+  const uint32_t grid = range_reduce_scan(flag, 2 * m, sums, st, &c->launches);
+  STC_CUDA(cudaMemcpyAsync(c->h_pinned + C_WORK, sums + grid, sizeof(uint64_t),
+                           cudaMemcpyDeviceToHost, st));
+  STC_CUDA(cudaStreamSynchronize(st));
+  const uint64_t nd = c->h_pinned[C_WORK];
+  if (nd >= (1ull << 31) - 1)
+    fail(STC_ERR_LIMIT, std::to_string(nd) + " distinct vertex ids >= 2^31 - 1");
+  uint32_t* ids = buffer<uint32_t>(c, B_DISTINCT, nd);
+  range_apply(flag, DistinctEmit{sorted, ids}, 2 * m, sums, st, &c->launches);
+  uint32_t* out = buffer<uint32_t>(c, B_RELABEL, 2 * m);
+  k_relabel<<<grid_for(m, 4), kThreads, 0, st>>>(*src, *dst, m, ids, (uint32_t)nd, out, out + m);
+  c->launches++;
+  STC_CUDA(cudaGetLastError());
+  *src = out;
+  *dst = out + m;
+  return nd;
+}
+
 }  // namespace
 
 void build_graph(stc_ctx* c, const uint32_t* d_src, const uint32_t* d_dst, const int8_t* d_sign,
@@ -864,11 +939,15 @@ void build_graph(stc_ctx* c, const uint32_t* d_src, const uint32_t* d_dst, const
     c->launches++;
   }
   read_counters(c, C_MAX_ID, 2);
-  const uint64_t max_id = c->h_pinned[C_MAX_ID];
+  uint64_t max_id = c->h_pinned[C_MAX_ID];
   const uint64_t self = c->h_pinned[C_SELF];
   // Ids (and ranks) stay below 2^31 - 1: the engine keeps a sign in bit 31.
-  if (max_id >= (1ull << 31) - 1)
-    fail(STC_ERR_LIMIT, "vertex id " + std::to_string(max_id) + " >= 2^31 - 1");
+  // Counts of totals relabel larger ids to dense ones; the other paths
+  // report results by id and keep the limit.
+  if (max_id >= (1ull << 31) - 1) {
+    if (!totals) fail(STC_ERR_LIMIT, "vertex id " + std::to_string(max_id) + " >= 2^31 - 1");
+    max_id = relabel_dense(c, &d_src, &d_dst, m) - 1;
+  }
   g.n = m ? (uint32_t)max_id + 1 : 0;
   g.m_valid = m - self;
   g.bits = std::max<uint32_t>(1, bit_width64(max_id));

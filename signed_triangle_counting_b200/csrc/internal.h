@@ -48,6 +48,8 @@ enum BufId {
   B_HEAD_RUNS,                    // head-side pass: in-arc range per head vertex (2 n)
   B_HEAD_LIST,                    // head-side pass: head vertices by class, plan, flags
   B_NKEY,                         // arcs: head << 1 | negative (m + 8)
+  B_RELABEL,                      // ids >= 2^31 - 1: the edges relabelled to dense ids (2 m)
+  B_DISTINCT,                     // ids >= 2^31 - 1: the sorted distinct ids
   B_COUNT_
 };
 

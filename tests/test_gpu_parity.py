@@ -129,10 +129,48 @@ def test_degenerate_inputs(ctx):
     assert t.as_tuple() == (1, 0, 0, 0)
 
 
+def _dense(src, dst):
+    """The list relabelled to dense ids in the same order (the oracle's ids)."""
+    ids, inv = np.unique(np.concatenate([src, dst]), return_inverse=True)
+    return inv[: len(src)].astype(np.uint32), inv[len(src):].astype(np.uint32)
+
+
+def test_large_ids_counted_as_dense(ctx):
+    """Counts of totals take any uint32 id (the reference's parse does): ids
+    at and above 2^31 - 1, up to 2^32 - 1, with duplicates and self-loops,
+    give the counts of the same graph on dense ids."""
+    rng = np.random.default_rng(17)
+    for base in ((1 << 31) - 1, 1 << 31, (1 << 32) - 5000):
+        el = synth.rmat(900 + base % 97, 11, 2000, 24000, p_pos=0.5)
+        table = np.sort(rng.choice(np.arange(base, min(base + 4000, 1 << 32), dtype=np.uint64),
+                                   el.n, replace=False)).astype(np.uint32)
+        table[-1] = np.uint32((1 << 32) - 1)
+        src, dst = table[el.src], table[el.dst]
+        # a duplicate with the other sign, a self-loop on the largest id
+        src = np.concatenate([src, src[:1], table[-1:]])
+        dst = np.concatenate([dst, dst[:1], table[-1:]])
+        sign = np.concatenate([el.sign, -el.sign[:1], np.array([1], np.int8)])
+        ds, dd = _dense(src, dst)
+        want = oracle.count_arrays(ds, dd, sign)
+        assert ctx.count(src, dst, sign).as_tuple() == want, base
+        # small ids mixed in
+        src2 = np.concatenate([src, np.array([3, 4], np.uint32)])
+        dst2 = np.concatenate([dst, np.array([4, int(table[0])], np.uint32)])
+        sign2 = np.concatenate([sign, np.array([-1, 1], np.int8)])
+        ds2, dd2 = _dense(src2, dst2)
+        assert ctx.count(src2, dst2, sign2).as_tuple() == oracle.count_arrays(ds2, dd2, sign2)
+    text = b"4294967295 5 1\n5 2147483647 -1\n2147483647 4294967295 1\n5 7 1\n"
+    got = ctx.count_text(text)[0]
+    assert got.as_tuple() == (0, 0, 1, 0)  # one triangle with one negative edge
+
+
 def test_id_limit(ctx):
+    """Per-vertex results are indexed by id: those calls keep ids below
+    2^31 - 1."""
     for bad in ((1 << 31) - 1, 1 << 31, (1 << 32) - 1):
         with pytest.raises(stc.StcError) as e:
-            ctx.count(np.array([bad], np.uint32), np.array([1], np.uint32), np.array([1], np.int8))
+            ctx.vertex_counts(np.array([bad], np.uint32), np.array([1], np.uint32),
+                              np.array([1], np.int8))
         assert e.value.status == _capi.STC_ERR_LIMIT
 
 
