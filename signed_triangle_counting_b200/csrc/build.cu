@@ -459,6 +459,11 @@ struct EdgeCursor {
 // (an endpoint that finds no free slot within kDegProbes probes is added
 // directly).
 constexpr int kRawTile = 512;
+// Edges of the input are taken in chunks of kEdgeChunk, chunk c by CTA
+// c mod grid: the CTAs of a launch work on neighbouring edges at any time,
+// so for a batch they gather the ranks and degrees of a few neighbouring
+// graphs at once, which stay in L2.
+constexpr uint64_t kEdgeChunk = 4096;
 constexpr int kRawSlots = 2048;  // 2 kRawTile endpoints per tile: load <= 1/2
 
 __device__ __forceinline__ bool sampled_edge(uint32_t a, uint32_t b, uint32_t shift) {
@@ -467,9 +472,8 @@ __device__ __forceinline__ bool sampled_edge(uint32_t a, uint32_t b, uint32_t sh
   return ((lo * 0x9E3779B1u) ^ (hi * 0x7FEB352Du) ^ ((lo ^ hi) >> 15)) >> (32 - shift) == 0;
 }
 
-__global__ void __launch_bounds__(kThreads) k_degree_raw(EdgeIds e, uint64_t m, uint64_t per_cta,
-                                                         uint32_t shift, uint32_t n,
-                                                         uint32_t* __restrict__ deg) {
+__global__ void __launch_bounds__(kThreads) k_degree_raw(EdgeIds e, uint64_t m, uint32_t shift,
+                                                         uint32_t n, uint32_t* __restrict__ deg) {
   __shared__ uint32_t tkey[kRawSlots], tcnt[kRawSlots], used[kRawSlots];
   __shared__ uint32_t nused;
   constexpr uint32_t kFree = 0xFFFFFFFFu;
@@ -479,57 +483,59 @@ __global__ void __launch_bounds__(kThreads) k_degree_raw(EdgeIds e, uint64_t m, 
   }
   if (threadIdx.x == 0) nused = 0;
   __syncthreads();
-  const uint64_t begin = (uint64_t)blockIdx.x * per_cta;
-  const uint64_t end = begin + per_cta < m ? begin + per_cta : m;
-  EdgeCursor cur;
-  if (begin < end) cur.start(e, begin);
-  for (uint64_t t = begin; t < end; t += kRawTile) {
-#pragma unroll
-    for (int r = 0; r < kRawTile / kThreads; r++) {
-      const uint64_t i = t + (uint64_t)r * kThreads + threadIdx.x;
-      uint32_t a = kFree, b = kFree;
-      if (i < end) {
-        cur.at(e, i, a, b);
-        // Ids at or past n only reach here when a capped build's union
-        // outgrew its capacity (flagged by k_batch_bases).
-        if (a == b || a >= n || b >= n || !sampled_edge(a, b, shift)) a = b = kFree;
-      }
-#pragma unroll
-      for (int side = 0; side < 2; side++) {
-        const uint32_t x = side ? b : a;
-        const unsigned px = __match_any_sync(kFull, x);
-        if (x != kFree && (px & lanemask_lt()) == 0) {
-          const uint32_t add = (uint32_t)__popc(px);
-          uint32_t slot = (x * 0x9E3779B1u) >> (32 - 11);
-          bool placed = false;
-          for (int p = 0; p < kDegProbes && !placed; p++) {
-            uint32_t c = tkey[slot];
-            if (c == kFree) {  // claim the slot, or see who claimed it first
-              const uint32_t old = atomicCAS(&tkey[slot], kFree, x);
-              if (old == kFree) used[atomicAdd(&nused, 1u)] = slot;
-              c = old == kFree ? x : old;
+  for (uint64_t chunk = blockIdx.x; chunk * kEdgeChunk < m; chunk += gridDim.x) {
+    const uint64_t begin = chunk * kEdgeChunk;
+    const uint64_t end = begin + kEdgeChunk < m ? begin + kEdgeChunk : m;
+    EdgeCursor cur;
+    cur.start(e, begin);
+    for (uint64_t t = begin; t < end; t += kRawTile) {
+  #pragma unroll
+      for (int r = 0; r < kRawTile / kThreads; r++) {
+        const uint64_t i = t + (uint64_t)r * kThreads + threadIdx.x;
+        uint32_t a = kFree, b = kFree;
+        if (i < end) {
+          cur.at(e, i, a, b);
+          // Ids at or past n only reach here when a capped build's union
+          // outgrew its capacity (flagged by k_batch_bases).
+          if (a == b || a >= n || b >= n || !sampled_edge(a, b, shift)) a = b = kFree;
+        }
+  #pragma unroll
+        for (int side = 0; side < 2; side++) {
+          const uint32_t x = side ? b : a;
+          const unsigned px = __match_any_sync(kFull, x);
+          if (x != kFree && (px & lanemask_lt()) == 0) {
+            const uint32_t add = (uint32_t)__popc(px);
+            uint32_t slot = (x * 0x9E3779B1u) >> (32 - 11);
+            bool placed = false;
+            for (int p = 0; p < kDegProbes && !placed; p++) {
+              uint32_t c = tkey[slot];
+              if (c == kFree) {  // claim the slot, or see who claimed it first
+                const uint32_t old = atomicCAS(&tkey[slot], kFree, x);
+                if (old == kFree) used[atomicAdd(&nused, 1u)] = slot;
+                c = old == kFree ? x : old;
+              }
+              if (c == x) {
+                atomicAdd(&tcnt[slot], add);
+                placed = true;
+              }
+              slot = (slot + 1) & (kRawSlots - 1);
             }
-            if (c == x) {
-              atomicAdd(&tcnt[slot], add);
-              placed = true;
-            }
-            slot = (slot + 1) & (kRawSlots - 1);
+            if (!placed) atomicAdd(deg + x, add);
           }
-          if (!placed) atomicAdd(deg + x, add);
         }
       }
+      __syncthreads();
+      const uint32_t nu = nused;
+      for (uint32_t j = threadIdx.x; j < nu; j += kThreads) {
+        const uint32_t slot = used[j];
+        atomicAdd(deg + tkey[slot], tcnt[slot]);
+        tkey[slot] = kFree;
+        tcnt[slot] = 0;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) nused = 0;
+      __syncthreads();
     }
-    __syncthreads();
-    const uint32_t nu = nused;
-    for (uint32_t j = threadIdx.x; j < nu; j += kThreads) {
-      const uint32_t slot = used[j];
-      atomicAdd(deg + tkey[slot], tcnt[slot]);
-      tkey[slot] = kFree;
-      tcnt[slot] = 0;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) nused = 0;
-    __syncthreads();
   }
 }
 
@@ -539,28 +545,28 @@ __global__ void __launch_bounds__(kThreads) k_degree_raw(EdgeIds e, uint64_t m, 
 // endpoint at or past n (a capped build whose union outgrew its capacity)
 // also becomes the sentinel and sets C_OVERFLOW.
 __global__ void k_arc_keys_raw(EdgeIds e, const int8_t* __restrict__ sign, uint64_t m,
-                               uint64_t per_cta, uint32_t bits, uint32_t n,
-                               const uint32_t* __restrict__ rank, uint64_t* __restrict__ akeys,
-                               unsigned long long* __restrict__ ctr) {
+                               uint32_t bits, uint32_t n, const uint32_t* __restrict__ rank,
+                               uint64_t* __restrict__ akeys, unsigned long long* __restrict__ ctr) {
   const uint64_t sentinel = (bits * 2 >= 64) ? ~0ull >> 1 : ((1ull << (2 * bits)) - 1);
-  const uint64_t begin = (uint64_t)blockIdx.x * per_cta;
-  const uint64_t end = begin + per_cta < m ? begin + per_cta : m;
-  if (begin >= end) return;
-  EdgeCursor cur;
-  cur.start(e, begin);
-  for (uint64_t i = begin + threadIdx.x; i < end; i += blockDim.x) {
-    uint32_t a, b;
-    cur.at(e, i, a, b);
-    uint64_t k = sentinel;
-    if (a == b) {
-      // self-loop: the sentinel
-    } else if (a >= n || b >= n) {
-      atomicExch(ctr + C_OVERFLOW, 1ull);
-    } else {
-      const uint32_t ra = rank[a], rb = rank[b];
-      k = ((uint64_t)min(ra, rb) << bits) | max(ra, rb) | ((uint64_t)(sign[i] < 0) << 63);
+  for (uint64_t chunk = blockIdx.x; chunk * kEdgeChunk < m; chunk += gridDim.x) {
+    const uint64_t begin = chunk * kEdgeChunk;
+    const uint64_t end = begin + kEdgeChunk < m ? begin + kEdgeChunk : m;
+    EdgeCursor cur;
+    cur.start(e, begin);
+    for (uint64_t i = begin + threadIdx.x; i < end; i += blockDim.x) {
+      uint32_t a, b;
+      cur.at(e, i, a, b);
+      uint64_t k = sentinel;
+      if (a == b) {
+        // self-loop: the sentinel
+      } else if (a >= n || b >= n) {
+        atomicExch(ctr + C_OVERFLOW, 1ull);
+      } else {
+        const uint32_t ra = rank[a], rb = rank[b];
+        k = ((uint64_t)min(ra, rb) << bits) | max(ra, rb) | ((uint64_t)(sign[i] < 0) << 63);
+      }
+      akeys[i] = k;
     }
-    akeys[i] = k;
   }
 }
 
@@ -746,7 +752,7 @@ void build_totals(stc_ctx* c, const EdgeIds& e, const int8_t* d_sign, uint64_t m
     const uint64_t ratio = g.m_valid / std::max<uint64_t>(1, g.n);
     const uint32_t bw = bit_width64(ratio);
     g.shift = caps ? caps->shift : bw > 2 ? std::min<uint32_t>(3, bw - 2) : 0;
-    k_degree_raw<<<ep.grid, kThreads, 0, st>>>(e, m, ep.per_cta, g.shift, g.n, g.deg);
+    k_degree_raw<<<ep.grid, kThreads, 0, st>>>(e, m, g.shift, g.n, g.deg);
     c->launches++;
   }
   STC_CUDA(cudaGetLastError());
@@ -791,8 +797,7 @@ void build_totals(stc_ctx* c, const EdgeIds& e, const int8_t* d_sign, uint64_t m
   if (g.m_valid) {
     uint64_t* ka = buffer<uint64_t>(c, B_KEYS_A, m);
     uint64_t* kb = buffer<uint64_t>(c, B_KEYS_B, m);
-    k_arc_keys_raw<<<ep.grid, kThreads, 0, st>>>(e, d_sign, m, ep.per_cta, g.bits, g.n, g.rank,
-                                                 ka, ctr);
+    k_arc_keys_raw<<<ep.grid, kThreads, 0, st>>>(e, d_sign, m, g.bits, g.n, g.rank, ka, ctr);
     c->launches++;
     uint64_t* sorted = radix_sort(ka, kb, m, 0, 2 * (int)g.bits, sort_counts, st, &c->launches);
     const uint64_t mask = (1ull << (2 * g.bits)) - 1;
