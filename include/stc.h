@@ -400,9 +400,11 @@ typedef struct stc_tuning {
 stc_status stc_ctx_set_tuning(stc_ctx* ctx, const stc_tuning* tuning);
 stc_status stc_ctx_get_tuning(const stc_ctx* ctx, stc_tuning* out);
 
-/* Autotuner: builds the graph of (src, dst, sign) once, then, class by class
- * (warp, block, large), counts that class alone under every candidate
- * setting (hash factor x unroll, and for the block class x block threads),
+/* Autotuner: builds the graph of (src, dst, sign) once, in the order counts
+ * of totals use, then, class by class (warp, block, large), counts that
+ * class alone, on both sides of the engine (the tail side's lists and the
+ * head side's heads of that class), under every candidate setting (hash
+ * factor x unroll, and for the block class x block threads),
  * `reps` times each, timed with CUDA events, and keeps the fastest.  Every
  * candidate must give the same counts (else STC_ERR_INTERNAL).  The result
  * is set on the context and copied to `out`. */

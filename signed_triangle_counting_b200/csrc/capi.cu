@@ -910,7 +910,9 @@ stc_status stc_autotune(stc_ctx* c, const uint32_t* src, const uint32_t* dst, co
     begin_call(c, o);
     DeviceInput in = stage_input(c, src, dst, sign, m, o);
     DeviceGraph g;
-    build_graph(c, in.src, in.dst, in.sign, m, g);
+    // The order counts of totals use (stc_count), whose head side takes
+    // most of the count on power-law graphs.
+    build_graph(c, in.src, in.dst, in.sign, m, g, /*totals=*/true);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     STC_CUDA(cudaEventCreate(&e0));
     STC_CUDA(cudaEventCreate(&e1));
@@ -932,7 +934,10 @@ stc_status stc_autotune(stc_ctx* c, const uint32_t* src, const uint32_t* dst, co
               if (k == 1) t.block_threads = ts[ti];
               cands.push_back(t);
             }
-        cfg.class_mask = 1u << (k + 1);
+        // The class on both sides: the tail side's class k and the head
+        // side's (bit 5 runs the head pass: its keys, sort and runs are the
+        // same for every candidate, its class-k kernel is not).
+        cfg.class_mask = (1u << (k + 1)) | 0x20u;
         float best_ms = 0.f;
         bool first = true;
         uint64_t want[4] = {0, 0, 0, 0};

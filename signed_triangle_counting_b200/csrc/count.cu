@@ -1792,7 +1792,8 @@ inline void enqueue_head_keys(cudaStream_t st, const Csr& csr, const uint32_t* a
 template <class Sink, bool kTime>
 void enqueue_head(cudaStream_t st, const Csr& csr, const uint32_t* asrc, uint64_t m,
                   const HeadBufs& b, unsigned long long* ctr, const Sink& sink,
-                  const ArcTimes& at, const Tuning& tu, int& launches) {
+                  const ArcTimes& at, const Tuning& tu, int& launches,
+                  uint32_t class_mask = 0x3F) {
   const uint32_t n = csr.n;
   const uint32_t vbits = std::max<uint32_t>(1, bit_width64(n - 1));
   int sort_launches = 0;
@@ -1804,13 +1805,16 @@ void enqueue_head(cudaStream_t st, const Csr& csr, const uint32_t* asrc, uint64_
   k_head_runs<true><<<kSMs * 4, 256, 0, st>>>(sorted, csr.off, ctr, b.hl, end);
   const HeadArcs h{sorted, b.aend, end, asrc};
   launches += 3 + sort_launches;
+  // Head class c runs with class_mask bit c + 1, as the tail side's class of
+  // the same tuning (the autotuner times one class at a time).
   with_unroll(kTime ? kStreamUnroll : tu.unroll[0], [&](auto U) {
     constexpr int kU = decltype(U)::value;
     if constexpr (!kTime || kU == kStreamUnroll)
-      k_head_warp<Sink, kTime, kU><<<kSMs * 4, 256, 0, st>>>(csr, h, b.hl, ctr, sink, at,
-                                                             tu.hash_factor[0]);
+      if (class_mask & 2u)
+        k_head_warp<Sink, kTime, kU><<<kSMs * 4, 256, 0, st>>>(csr, h, b.hl, ctr, sink, at,
+                                                               tu.hash_factor[0]);
   });
-  {
+  if (class_mask & 4u) {
     const uint32_t cap = kBlockCap;
     const uint32_t hf = fit_hash_factor(tu.hash_factor[1], cap);
     const uint32_t nb = hf * cap;
@@ -1826,7 +1830,7 @@ void enqueue_head(cudaStream_t st, const Csr& csr, const uint32_t* asrc, uint64_
       });
     });
   }
-  {
+  if (class_mask & 8u) {
     const uint32_t cap = kLargeCap;
     const uint32_t hf = fit_hash_factor(tu.hash_factor[2], cap);
     const uint32_t nb = hf * cap;
@@ -2328,7 +2332,7 @@ void count_triangles(stc_ctx* c, const DeviceGraph& gin, const CountConfig& cfg)
     if (head) {
       prepare_head<Sink, kT>(c->tuning);
       enqueue_head<Sink, kT>(st, csr, g.asrc, g.m_fwd, hb, ctr, sink, at, c->tuning,
-                             c->launches);
+                             c->launches, cfg.class_mask);
     }
   };
   if (timed) {
