@@ -686,7 +686,7 @@ __device__ __forceinline__ void search_pass(const Csr& g, const StageMem& m, uin
 // number of arcs.  In this mode every arc is processed alone by one warp,
 // timed from the first load of its B to the last count it adds, so three runs
 // with the strategy forced give every cell's cost under every strategy: the
-// training data of the learned dispatcher and the judge of a dispatch
+// training data of the learned dispatcher and the measure of a dispatch
 // table's regret.  The counting kernels proper pack the int4 chunks of all
 // HASH and MERGE arcs of a list into one stream that keeps every lane busy,
 // so such an arc of c chunks is charged its share of the lanes it would

@@ -16,7 +16,7 @@ changes only speed.
   measured log2 cycles per arc of each strategy as targets, and a weight that
   grows with the cell's number of arcs.
 * ``train`` fits the perceptron on the device (``stc_dispatcher_train``).
-* ``regret`` judges any table against a recording: the time it would spend
+* ``regret`` scores any table against a recording: the time it would spend
   divided by the time of the per-cell best choice (1.0 = no regret).
 
     python -m signed_triangle_counting_b200.dispatcher train [--out PATH]
