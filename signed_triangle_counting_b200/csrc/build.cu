@@ -797,6 +797,7 @@ void build_totals(stc_ctx* c, const EdgeIds& e, const int8_t* d_sign, uint64_t m
   if (g.m_valid) {
     uint64_t* ka = buffer<uint64_t>(c, B_KEYS_A, m);
     uint64_t* kb = buffer<uint64_t>(c, B_KEYS_B, m);
+    wait_sign(c);  // a host sign array may still be on its way (stc_count)
     k_arc_keys_raw<<<ep.grid, kThreads, 0, st>>>(e, d_sign, m, g.bits, g.n, g.rank, ka, ctr);
     c->launches++;
     uint64_t* sorted = radix_sort(ka, kb, m, 0, 2 * (int)g.bits, sort_counts, st, &c->launches);
@@ -968,6 +969,7 @@ void build_graph(stc_ctx* c, const uint32_t* d_src, const uint32_t* d_dst, const
   uint64_t* kb = buffer<uint64_t>(c, B_KEYS_B, m);
   g.ukeys = buffer<uint64_t>(c, B_UKEYS, g.m_valid);
   if (g.m_valid) {
+    wait_sign(c);
     k_pack_dedup<<<grid_for(m, 4), kThreads, 0, st>>>(d_src, d_dst, d_sign, m, g.bits, ka);
     c->launches++;
     uint64_t* sorted = radix_sort(ka, kb, m, 0, 2 * (int)g.bits, sort_counts, st, &c->launches);

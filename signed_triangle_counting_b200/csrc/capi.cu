@@ -41,6 +41,12 @@ void mark(stc_ctx* c, int slot) {
     STC_CUDA(cudaEventRecord(c->ev[slot], c->stream));
 }
 
+void wait_sign(stc_ctx* c) {
+  if (!c->sign_pending) return;
+  c->sign_pending = false;
+  STC_CUDA(cudaStreamWaitEvent(c->stream, c->ev_sign, 0));
+}
+
 void release_pipelines(stc_ctx* c) {
   for (auto& p : c->pipes)
     if (p.exec) cudaGraphExecDestroy(p.exec);
@@ -61,6 +67,11 @@ stc_status guarded(stc_ctx* c, F body) {
     return STC_OK;
   } catch (const Error& e) {
     if (c) c->last_error = e.msg;
+    if (c && c->sign_pending) {  // the caller's sign array stays in use until the copy ends
+      c->sign_pending = false;
+      cudaStreamSynchronize(c->aux_stream);
+      (void)cudaGetLastError();
+    }
     return e.status;
   } catch (const std::bad_alloc&) {
     if (c) c->last_error = "host allocation failed";
@@ -128,8 +139,12 @@ struct DeviceInput {
   const int8_t* sign;
 };
 
+// Device copies of host input (device input as it is).  With defer_sign
+// the sign array is copied on the auxiliary stream after the ids, so that
+// it overlaps the id scan, degrees and ranking; the build waits for it
+// (wait_sign) before its first read of the signs.
 DeviceInput stage_input(stc_ctx* c, const uint32_t* src, const uint32_t* dst, const int8_t* sign,
-                        uint64_t m, const stc_opts* o) {
+                        uint64_t m, const stc_opts* o, bool defer_sign = false) {
   if (m && (!src || !dst || !sign)) fail(STC_ERR_INVALID_ARGUMENT, "null edge array");
   if (o && (o->flags & STC_F_DEVICE_INPUT)) return DeviceInput{src, dst, sign};
   uint32_t* ds = buffer<uint32_t>(c, B_IN_SRC, m);
@@ -138,7 +153,15 @@ DeviceInput stage_input(stc_ctx* c, const uint32_t* src, const uint32_t* dst, co
   if (m) {
     STC_CUDA(cudaMemcpyAsync(ds, src, m * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
     STC_CUDA(cudaMemcpyAsync(dd, dst, m * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
-    STC_CUDA(cudaMemcpyAsync(dg, sign, m, cudaMemcpyHostToDevice, c->stream));
+    if (defer_sign) {
+      STC_CUDA(cudaEventRecord(c->ev_ids, c->stream));
+      STC_CUDA(cudaStreamWaitEvent(c->aux_stream, c->ev_ids, 0));
+      STC_CUDA(cudaMemcpyAsync(dg, sign, m, cudaMemcpyHostToDevice, c->aux_stream));
+      STC_CUDA(cudaEventRecord(c->ev_sign, c->aux_stream));
+      c->sign_pending = true;
+    } else {
+      STC_CUDA(cudaMemcpyAsync(dg, sign, m, cudaMemcpyHostToDevice, c->stream));
+    }
   }
   return DeviceInput{ds, dd, dg};
 }
@@ -420,6 +443,9 @@ stc_status stc_ctx_create(int device, stc_ctx** out) {
   c->device = device;
   stc_status s = guarded(c, [&] {
     STC_CUDA(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
+    STC_CUDA(cudaStreamCreateWithFlags(&c->aux_stream, cudaStreamNonBlocking));
+    STC_CUDA(cudaEventCreateWithFlags(&c->ev_ids, cudaEventDisableTiming));
+    STC_CUDA(cudaEventCreateWithFlags(&c->ev_sign, cudaEventDisableTiming));
     c->stream = c->own_stream;
     STC_CUDA(cudaMallocHost(&c->h_pinned, C_SLOTS * sizeof(uint64_t)));
     for (auto& e : c->ev) STC_CUDA(cudaEventCreate(&e));
@@ -445,6 +471,12 @@ void stc_ctx_destroy(stc_ctx* c) {
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
   if (c->h_pinned) cudaFreeHost(c->h_pinned);
+  if (c->aux_stream) {
+    cudaStreamSynchronize(c->aux_stream);
+    cudaStreamDestroy(c->aux_stream);
+  }
+  if (c->ev_ids) cudaEventDestroy(c->ev_ids);
+  if (c->ev_sign) cudaEventDestroy(c->ev_sign);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   (void)cudaGetLastError();
   delete c;
@@ -482,9 +514,10 @@ stc_status stc_count(stc_ctx* c, const uint32_t* src, const uint32_t* dst, const
   return guarded(c, [&] {
     CountConfig cfg = count_config(o);
     begin_call(c, o);
-    DeviceInput in = stage_input(c, src, dst, sign, m, o);
+    DeviceInput in = stage_input(c, src, dst, sign, m, o, /*defer_sign=*/true);
     DeviceGraph g;
     build_graph(c, in.src, in.dst, in.sign, m, g, /*totals=*/true);
+    wait_sign(c);
     count_triangles(c, g, cfg);
     mark(c, 5);
     end_call(c, g, out);

@@ -152,6 +152,12 @@ struct stc_ctx {
   std::string last_error;
   stc_stats stats{};
   cudaEvent_t ev[8] = {};
+  // A sign array copied from host memory on aux_stream while the ids are
+  // scanned and ranked (stc_count): ev_sign marks its end, and sign_pending
+  // says the call's stream has not waited for it yet (wait_sign).
+  cudaStream_t aux_stream = nullptr;
+  cudaEvent_t ev_ids = nullptr, ev_sign = nullptr;
+  bool sign_pending = false;
   bool timing = false;
   int launches = 0;
   bool fixed_ready = false;   // B_DISPATCH_FIXED holds the fixed tables
@@ -243,6 +249,9 @@ struct DeviceGraph {
 
 // Stage timing helper: records an event when the context is timing.
 void mark(stc_ctx* c, int slot);
+// Makes the call's stream wait for a sign array still being copied on the
+// auxiliary stream (no-op when none is).
+void wait_sign(stc_ctx* c);
 
 // Graph build: input device arrays -> DeviceGraph (all fields).  With
 // `totals`, for counts of totals only: the vertex order is (degree over the
